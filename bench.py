@@ -1,0 +1,328 @@
+#!/usr/bin/env python
+"""Throughput of the line-by-line engine: Voigt line-evaluations/s and spectra/s.
+
+Workload: 200,000 synthetic lines (H2O-, CO2-, O3-like, 50/30/20) over
+600-2500 cm^-1, a 60-layer profile (61 levels uniform in ln p), grid
+600-2500 cm^-1 at 0.001 cm^-1 (1,900,001 points), 25 cm^-1 cut-off, 2 cm^-1
+reference tiles, mu = 0.8. A step is one full spectrum: every device stage from
+levels and line parameters resident in HBM to the transmittance in HBM.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--precision fp32|fp64]
+    python bench.py --impl reference     # the reference's CPU path on this host
+
+Under torchrun each rank computes its own spectrum (rank r uses a profile with
+seeded temperature/H2O perturbations), so per-GPU work is fixed (weak scaling)
+and there is no data-path collective; `value` is all ranks' evaluations divided
+by the slowest rank's time.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "Voigt line-evals/s"
+UNIT = "line-evals/s"
+WORKLOAD = "three_gas_200k_lines_60_layers_600-2500cm-1_step0.001_cutoff25_tile2_mu0.8"
+FLOPS_PER_EVAL_FAR = 12      # far-wing branch of tau_f32_kernel: 5 FFMA + 1 FMUL + 1 RCP
+CPU_SAMPLE = (1000.0, 1000.5)  # sub-window timed on the host (all 60 layers)
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--precision", default="fp32", choices=["fp32", "fp64"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    return ap.parse_args()
+
+
+def workload(rank: int):
+    from pylblrtm_b200 import synthetic
+    sd = synthetic.three_gas_lines()
+    if rank == 0:
+        prof = synthetic.logp_profile()
+    else:
+        lv = synthetic.perturbed_levels(synthetic.logp_levels(), 1, seed=1000 + rank)
+        prof = synthetic.profile_from_levels(lv, 0)
+    return sd, prof
+
+
+# ---------------------------------------------------------------------------- CPU side
+_CPU_CACHE = {}
+
+
+def _cpu_inputs(lo, hi):
+    """Workload lines near the sub-window and the layers (cached per process, untimed)."""
+    key = (lo, hi)
+    if key not in _CPU_CACHE:
+        from oracle import restate
+        from pylblrtm_b200 import synthetic
+        sd = synthetic.restrict(synthetic.three_gas_lines(), lo - 26.0, hi + 26.0)
+        prof = synthetic.logp_profile()
+        _CPU_CACHE[key] = (sd, restate.build_layers(prof.pressure_hpa, prof.temperature_k, prof.vmr))
+    return _CPU_CACHE[key]
+
+
+def _oracle_layer(args):
+    """One layer of the oracle on a sub-window (runs in a worker process)."""
+    k, lo, hi = args
+    sys.path.insert(0, ROOT)
+    from oracle import restate
+    sd, (p, t, v, c) = _cpu_inputs(lo, hi)
+    sl = slice(k, k + 1)
+    nu = restate.grid(lo, hi, 0.001)
+    od = restate.optical_depth(nu, sd.lines, sd.tips, sd.molar_masses, p[sl], t[sl],
+                               {g: a[sl] for g, a in v.items()}, {g: a[sl] for g, a in c.items()}, 25.0, 2.0)
+    n = restate.count_evals(nu, sd.lines, sd.tips, sd.molar_masses, p[sl], t[sl],
+                            {g: a[sl] for g, a in v.items()}, {g: a[sl] for g, a in c.items()}, 25.0, 2.0)
+    return n, od
+
+
+def cpu_reference_sample(workers: int):
+    """Times the oracle port of the reference path on the sub-window, all 60 layers."""
+    lo, hi = CPU_SAMPLE
+    jobs = [(k, lo, hi) for k in range(60)]
+    if workers <= 1:
+        _cpu_inputs(lo, hi)
+        t0 = time.perf_counter()
+        out = [_oracle_layer(j) for j in jobs]
+        dt = time.perf_counter() - t0
+    else:
+        import multiprocessing as mp
+        with mp.get_context("spawn").Pool(workers, initializer=_cpu_inputs, initargs=(lo, hi)) as pool:
+            pool.map(_oracle_layer, [(0, lo, hi)] * workers)      # start-up and input generation, untimed
+            t0 = time.perf_counter()
+            out = pool.map(_oracle_layer, jobs, chunksize=1)
+            dt = time.perf_counter() - t0
+    evals = sum(n for n, _ in out)
+    return evals, dt
+
+
+def cpu_info():
+    model = "unknown"
+    try:
+        for line in open("/proc/cpuinfo"):
+            if line.startswith("model name"):
+                model = line.split(":", 1)[1].strip()
+                break
+    except OSError:
+        pass
+    return model, os.cpu_count(), len(os.sched_getaffinity(0))
+
+
+def run_reference(a):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    model, n_cpu, n_aff = cpu_info()
+    workers = n_aff
+    for _ in range(a.warmup):
+        pass  # the oracle has no warm-up state; the first timed step includes process start-up
+    times, evals = [], 0
+    for _ in range(a.steps):
+        n, dt = cpu_reference_sample(workers)
+        times.append(dt)
+        evals = n
+    t = sum(times)
+    value = evals * a.steps / t
+    sample = (f"oracle port of pylblrtm/forward.py:157-317, grid {CPU_SAMPLE[0]}-{CPU_SAMPLE[1]} cm^-1 "
+              f"(501 points) x 60 layers of the workload, {evals:.3e} evals/step, layer-parallel over "
+              f"{workers} spawn workers; CPU {model}")
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": a.gpus,
+            "steps": a.steps, "warmup": a.warmup, "ms_per_step": 1e3 * t / a.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "sample": f"{CPU_SAMPLE[0]}-{CPU_SAMPLE[1]} cm^-1 x 60 layers"},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": workers, "kind": "port", "sample": sample},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------------------- GPU side
+class ClockSampler:
+    """nvidia-smi clock/throttle samples during the timed region."""
+
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu: int):
+        self.gpu, self.rows, self.proc = gpu, [], None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            threading.Thread(target=self._read, daemon=True).start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([c.strip() for c in line.split(",")])
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            time.sleep(0.25)
+            self.proc.terminate()
+            self.proc.wait()
+
+    def summary(self):
+        sm = [float(r[0]) for r in self.rows if len(r) >= 7 and r[0].replace(".", "").isdigit()]
+        mx = [float(r[1]) for r in self.rows if len(r) >= 7 and r[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in self.rows if len(r) >= 7 for i in range(4) if r[3 + i] == "Active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(sm)}
+
+
+def fp32_peak(torch):
+    """Measured float32 FMA throughput (TFLOP/s) of this GPU with lbl_probe_fma_f32."""
+    from pylblrtm_b200 import _lib
+    sms = torch.cuda.get_device_properties(0).multi_processor_count
+    blocks, iters = sms * 8 * 4, 20000
+    out = torch.zeros(1, device="cuda")
+    s = torch.cuda.current_stream().cuda_stream
+    best = None
+    for _ in range(4):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        _lib.call("lbl_probe_fma_f32", out.data_ptr(), iters, blocks, s)
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1)
+        best = ms if best is None else min(best, ms)
+    return blocks * 256 * 8 * iters * 2 / (best * 1e-3) / 1e12
+
+
+def main():
+    a = parse()
+    if a.impl == "reference":
+        run_reference(a)
+        return
+    import torch
+    import torch.distributed as dist
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+
+    import pylblrtm_b200 as lbl
+    from pylblrtm_b200 import engine
+
+    sd, prof = workload(rank)
+    grid = engine.make_grid(600.0, 2500.0, 0.001, 2.0)
+    job = engine.Job(sd, engine.layer_input_from_profile(prof), grid, 25.0)
+    # evaluation count of one spectrum (the reference tile rule), from the kernel's own counter
+    r0 = job.run(a.precision, mu=[0.8], want_od=False, want_trans=True, count_evals=True)
+    evals_per_step = r0.evals
+    launches_per_step = job.launches
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    for _ in range(a.warmup):
+        job.run(a.precision, mu=[0.8], want_od=False, want_trans=True)
+    timer = {}
+    barrier()
+    with ClockSampler(local) as clocks:
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(a.steps):
+            job.run(a.precision, mu=[0.8], want_od=False, want_trans=True, timer=timer)
+        e1.record()
+        barrier()
+    ms = e0.elapsed_time(e1)
+    tau_ms = [b.elapsed_time(c) for b, c in timer["tau_events"]]
+    if world > 1:
+        t = torch.tensor([ms], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    total_evals = evals_per_step * a.steps * world
+    value = total_evals / (ms * 1e-3)
+
+    # end to end through the public API: host arrays in pinned memory, copies and the
+    # device->host transmittance read inside the timed region
+    e2e = None
+    if not a.no_e2e:
+        pin = {k: torch.from_numpy(np.ascontiguousarray(v)).pin_memory().numpy() for k, v in sd.lines.items()}
+        sd_pin = lbl.SpectralData(pin, sd.tips, sd.molar_masses, sd.molecule)
+        lbl.compute_transmittance(sd_pin, prof, 600.0, 2500.0, mu_view=0.8)
+        barrier()
+        t0 = time.perf_counter()
+        for _ in range(a.steps):
+            nu, T = lbl.compute_transmittance(sd_pin, prof, 600.0, 2500.0, mu_view=0.8)
+        barrier()
+        e2e_s = time.perf_counter() - t0
+        if world > 1:
+            t = torch.tensor([e2e_s], device="cuda", dtype=torch.float64)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            e2e_s = float(t.item())
+        h2d = sum(v.nbytes for v in pin.values()) + prof.pressure_hpa.nbytes * (2 + len(prof.vmr))
+        e2e = {"value": evals_per_step * a.steps * world / e2e_s, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
+               "d2h_bytes_per_step": int(T.nbytes + 8), "spectra_per_s": a.steps * world / e2e_s,
+               "api": "pylblrtm_b200.compute_transmittance"}
+
+    if rank != 0:
+        if world > 1:
+            dist.destroy_process_group()
+        return
+    peak = fp32_peak(torch)
+    tau_avg = sum(tau_ms) / len(tau_ms)
+    achieved = evals_per_step * FLOPS_PER_EVAL_FAR / (tau_avg * 1e-3) / 1e12
+    cpu = None
+    if world == 1 and not a.no_cpu_baseline:
+        n, dt = cpu_reference_sample(1)
+        model, _, _ = cpu_info()
+        cpu = {"value": n / dt, "unit": UNIT, "cores": 1, "kind": "port",
+               "sample": f"oracle port, {CPU_SAMPLE[0]}-{CPU_SAMPLE[1]} cm^-1 x 60 layers ({n:.3e} evals, "
+                         f"{dt:.1f} s), 1 process; CPU {model}"}
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": a.steps, "warmup": a.warmup,
+        "ms_per_step": ms / a.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32" if a.precision == "fp32" else "f64", "data": "synthetic",
+        "spectra_per_s": a.steps * world / (ms * 1e-3),
+        "evals_per_spectrum": evals_per_step,
+        "config": {"workload": WORKLOAD, "precision": a.precision, "lines": 200000, "layers": 60,
+                   "grid_points": grid.n_nu, "parallelism": f"replicas{world}" if world > 1 else "single",
+                   "l2": "inputs and outputs larger than L2 (line records 384 MB, od 456 MB)"},
+        "roofline": {"bound": "fp32", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                     "frac": achieved / peak, "traffic": None,
+                     "kernel": "tau_f32_kernel" if a.precision == "fp32" else "tau_f64_kernel",
+                     "kernel_ms": tau_avg,
+                     "peak_source": "measured live: lbl_probe_fma_f32 (MEASURED_PEAKS.json has no fp32 entry)",
+                     "flops_per_eval": FLOPS_PER_EVAL_FAR},
+        "gpu_launches": launches_per_step * a.steps,
+        "clocks": clocks.summary(),
+        "e2e": e2e,
+        "cpu_baseline": cpu,
+    }
+    print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

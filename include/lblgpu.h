@@ -1,0 +1,153 @@
+/*
+ * lblgpu.h — C ABI of the B200 line-by-line transmittance engine (liblblgpu.so).
+ *
+ * Every entry point takes DEVICE pointers (except where noted), sizes, scalars
+ * and a cudaStream_t passed as void*, enqueues its kernels on that stream and
+ * returns a status code; nothing allocates and nothing synchronises. Buffers
+ * written by one call are read by the next on the same stream. Errors found by
+ * kernels (non-finite or negative line strengths, non-finite optical depth) are
+ * reported through an int error word in device memory that the caller
+ * initialises to INT_MAX and reads after synchronising: it receives the
+ * smallest key  row * (n_grp + 1) + g  (g = group index, g = n_grp for the
+ * optical-depth check), i.e. the first failure in the reference's loop order.
+ *
+ * The reference (PyLBLRTM 0.1.2) is pure Python; each entry point names the
+ * reference code it replaces. The Python host layer (pylblrtm_b200) binds these
+ * symbols with ctypes and keeps the reference's public API on top.
+ */
+#ifndef LBLGPU_H
+#define LBLGPU_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* status codes */
+#define LBL_OK 0
+#define LBL_EINVAL 1    /* bad argument (message in lbl_last_error) */
+#define LBL_ECUDA 2     /* CUDA launch / runtime error */
+
+/* ---- records exchanged between the stages (layouts fixed, 8-byte aligned) ---- */
+
+/* Per (profile-layer, line group): forward.py:236-259, 292. */
+typedef struct {
+  double T, p_self, p_air, col, q_ratio, dop; /* dop = sqrt(T / molar_mass) */
+} LayerGroup;
+
+/* One line after the candidate sort (input parameters + group + input index). */
+typedef struct {
+  double nu0, sref, g_air, g_self, elow, n_air, shift;
+  int gid, src;
+} LineIn;
+
+/* Prepared line for the float64 summation. nuc = NaN marks an inactive line. */
+typedef struct {
+  double nuc, inv_ad, y, amp;
+} LineF64;
+
+/* Prepared line for the float32 summation (integer grid index + remainder). */
+typedef struct {
+  double nuc;
+  int j0;
+  float b, a, y, amp, amp_far;
+} LineF32;
+
+/* Last error message of the calling thread ("" if none). */
+const char* lbl_last_error(void);
+/* ABI version of this library. */
+int lbl_abi_version(void);
+
+/* Layers from levels; replaces pylblrtm/atmosphere.py:110-141
+ * (AtmosphericProfile.build_layers) for a batch of profiles.
+ * p_hpa, t_k: [n_prof, n_lev]; vmr: [n_prof, n_gas, n_lev];
+ * p_atm, t_layer: [n_prof, n_lev-1]; vmr_layer, col: [n_prof, n_gas, n_lev-1].
+ * col_factor = AVOGADRO / (GRAVITY * M_DRY_AIR) (atmosphere.py:134). */
+int lbl_build_layers(const double* p_hpa, const double* t_k, const double* vmr, int n_prof, int n_lev,
+                     int n_gas, double col_factor, double* p_atm, double* t_layer, double* vmr_layer,
+                     double* col, void* stream);
+
+/* Per (profile, layer, group) quantities with Q(296)/Q(T) interpolated from the
+ * TIPS tables; replaces pylblrtm/forward.py:236-240 (with SpectralData.Q,
+ * spectral_data.py:43-52) and forward.py:249-259. out: [n_prof*n_lay, n_grp].
+ * grp_gas[g] indexes the gas axis of vmr_layer/col; tips_t/tips_q hold every
+ * group's table back to back at tips_off[g], length tips_len[g]. */
+int lbl_layer_groups(const double* t_layer, const double* p_atm, const double* vmr_layer, const double* col,
+                     int n_prof, int n_lay, int n_gas, int n_grp, const int* grp_gas, const double* grp_mass,
+                     const int* tips_off, const int* tips_len, const double* tips_t, const double* tips_q,
+                     LayerGroup* out, void* stream);
+
+/* Workspace bytes for lbl_sort_lines. */
+size_t lbl_sort_workspace_bytes(int n_lines);
+
+/* Selects the lines the reference masks in (forward.py:189-220: valid group,
+ * nu0 in [mask_lo - |shift| p_max, mask_hi + |shift| p_max] with
+ * mask_lo = nu[0] - cutoff, mask_hi = nu[-1] + cutoff) and sorts them by nu0
+ * (ties by input index). gid[i] < 0 drops line i. Writes the input indices in
+ * sorted order to order[0 .. *n_kept), the count to *n_kept and the largest
+ * |shift| p_max of a kept line to *max_shift_bound (all device memory). */
+int lbl_sort_lines(const double* nu0, const double* shift, const int* gid, int n_lines, double mask_lo,
+                   double mask_hi, double p_max, void* workspace, size_t workspace_bytes, int* order,
+                   int* n_kept, double* max_shift_bound, void* stream);
+
+/* Gathers the sorted lines into LineIn records (out[0 .. *n_kept)). */
+int lbl_gather_lines(const double* nu0, const double* sref, const double* g_air, const double* g_self,
+                     const double* elow, const double* n_air, const double* shift, const int* gid,
+                     const int* order, const int* n_kept, int n_lines, LineIn* out, void* stream);
+
+/* Candidate line range [ranges[2t], ranges[2t+1]) of each reference tile of
+ * tile_samples grid points: lines whose unshifted centre is within
+ * cutoff + pad of the tile (pad >= the largest pressure shift). The exact
+ * window test of forward.py:295-301 runs inside the summation kernels. */
+int lbl_tile_ranges(const LineIn* lines, const int* n_kept, double nu_min, double step, long long n_nu,
+                    int tile_samples, double cutoff, double pad, int n_tiles, int* ranges, void* stream);
+
+/* Per (row = profile-layer, sorted line) HITRAN scaling; replaces
+ * pylblrtm/forward.py:257-292 (strength with column and 1/R(nuc), Lorentz and
+ * Doppler widths, pressure shift). out: [n_rows, n_lines]. */
+int lbl_line_prep_f64(const LineIn* lines, const int* n_kept, int n_lines, const LayerGroup* lg, int n_rows,
+                      int n_grp, LineF64* out, int* err, void* stream);
+int lbl_line_prep_f32(const LineIn* lines, const int* n_kept, int n_lines, const LayerGroup* lg, int n_rows,
+                      int n_grp, double nu_min, double step, LineF32* out, int* err, void* stream);
+
+/* Optical depth of every (row, grid point): the Voigt sum over the lines of
+ * the point's reference tile window, times R(nu, T_row); replaces
+ * pylblrtm/forward.py:295-315 (tile loop, _voigt, phi @ S, radiation term and
+ * its finiteness check). od: [n_rows, n_nu]. evals (nullable, u64) receives
+ * the number of (row, point, line) evaluations admitted by the tile rule.
+ * _f64: float64 throughout (Gautschi-type Faddeeva). _f32: float32 Faddeeva
+ * with the asymptotic far-wing branch and compensated sums. */
+int lbl_tau_tiles_f64(const LineF64* prep, int n_lines, const int* ranges, const double* t_layer, int n_rows,
+                      double nu_min, double step, long long n_nu, int tile_samples, double cutoff, int n_grp,
+                      double* od, int* err, unsigned long long* evals, void* stream);
+int lbl_tau_tiles_f32(const LineF32* prep, int n_lines, const int* ranges, const double* t_layer, int n_rows,
+                      double nu_min, double step, long long n_nu, int tile_samples, double cutoff, int n_grp,
+                      float* od, int* err, unsigned long long* evals, void* stream);
+
+/* Column sums over layers and transmittance exp(-tau / mu); replaces
+ * pylblrtm/forward.py:151 and config.py:266-270. od: [n_prof, n_lay, n_nu]
+ * (float32 or float64); trans, tau (each nullable): [n_prof, n_nu] float64;
+ * mu: [n_prof] device array of view cosines (mu_view). */
+int lbl_layer_sum_exp_f32(const float* od, int n_prof, int n_lay, long long n_nu, const double* mu,
+                          double* trans, double* tau, void* stream);
+int lbl_layer_sum_exp_f64(const double* od, int n_prof, int n_lay, long long n_nu, const double* mu,
+                          double* trans, double* tau, void* stream);
+
+/* Faddeeva function on arrays (diagnostics; replaces the scipy.special.wofz call
+ * at forward.py:62). mode 0: general algorithm; mode 1 (f32 only): the
+ * engine's real part with the far-wing branch (im not written). */
+int lbl_faddeeva_f64(const double* x, const double* y, long long n, double* re, double* im, void* stream);
+int lbl_faddeeva_f32(const float* x, const float* y, long long n, float* re, float* im, int mode,
+                     void* stream);
+
+/* Measurement probe (no reference counterpart): `blocks` CTAs of 256 threads
+ * each run 8 chains of `iters` dependent float32 FMAs, i.e.
+ * blocks * 256 * 8 * iters * 2 flops; the caller times the launch. */
+int lbl_probe_fma_f32(float* out, int iters, int blocks, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* LBLGPU_H */

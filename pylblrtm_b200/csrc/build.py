@@ -1,0 +1,73 @@
+"""Build liblblgpu.so (sm_100a) in-tree with nvcc.
+
+    python -m pylblrtm_b200.csrc.build          # or pylblrtm_b200.csrc.build.build()
+
+The library lands next to the package (pylblrtm_b200/liblblgpu.so) so that it
+travels with the source tree; nothing is installed into site-packages.
+"""
+
+from __future__ import annotations
+
+import os
+import shutil
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+PKG = os.path.dirname(HERE)
+ROOT = os.path.dirname(PKG)
+SOURCES = ["capi.cu", "prep.cu", "voigt.cu"]
+HEADERS = ["lbl_common.cuh", "faddeeva.cuh", os.path.join("..", "..", "include", "lblgpu.h")]
+LIB = os.path.join(PKG, "liblblgpu.so")
+HOST_LIB = os.path.join(PKG, "libfaddeeva_host.so")
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+
+
+def nvcc() -> str:
+    path = shutil.which("nvcc") or "/usr/local/cuda/bin/nvcc"
+    if not os.path.exists(path):
+        raise RuntimeError("nvcc not found: the CUDA toolkit is required to build liblblgpu.so")
+    return path
+
+
+def _stale(target: str, deps) -> bool:
+    if not os.path.exists(target):
+        return True
+    t = os.path.getmtime(target)
+    return any(os.path.getmtime(os.path.join(HERE, d)) > t for d in deps)
+
+
+def build(force: bool = False, verbose: bool = False) -> str:
+    """Compile every .cu source for sm_100a and link liblblgpu.so; returns its path."""
+    deps = SOURCES + HEADERS + ["build.py", "faddeeva_host.cpp"]
+    if not force and not _stale(LIB, deps):
+        return LIB
+    objdir = os.path.join(ROOT, "_build")
+    os.makedirs(objdir, exist_ok=True)
+    objs = []
+    for src in SOURCES:
+        obj = os.path.join(objdir, src.replace(".cu", ".o"))
+        cmd = [nvcc(), *ARCH, "-O3", "-lineinfo", "-std=c++17", "--extended-lambda", "-Xcompiler", "-fPIC",
+               "-rdc=false", "-c", os.path.join(HERE, src), "-o", obj]
+        if verbose:
+            cmd.insert(1, "-Xptxas=-v")
+        subprocess.run(cmd, check=True)
+        objs.append(obj)
+    tmp = LIB + ".tmp"
+    subprocess.run([nvcc(), *ARCH, "-shared", "-o", tmp, *objs, "-lcudart"], check=True)
+    os.replace(tmp, LIB)
+    build_host_check()
+    return LIB
+
+
+def build_host_check() -> str:
+    """Host (g++) build of faddeeva.cuh used by the CPU accuracy tests."""
+    tmp = HOST_LIB + ".tmp"
+    subprocess.run(["g++", "-O2", "-std=c++17", "-ffp-contract=off", "-fPIC", "-shared",
+                    os.path.join(HERE, "faddeeva_host.cpp"), "-o", tmp], check=True)
+    os.replace(tmp, HOST_LIB)
+    return HOST_LIB
+
+
+if __name__ == "__main__":
+    print(build(force="--force" in sys.argv, verbose="-v" in sys.argv))

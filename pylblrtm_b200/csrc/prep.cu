@@ -1,0 +1,407 @@
+// Preparation kernels: hydrostatic layers, per-(layer, group) quantities with the
+// partition-sum interpolation, candidate-line sort, tile windows and the per
+// (layer, line) HITRAN scaling ("line prep").
+#include <float.h>
+#include <limits.h>
+#include <math.h>
+
+#include "faddeeva.cuh"
+#include "lbl_common.cuh"
+
+namespace lbl {
+
+// ---------------------------------------------------------------------------
+// Layers from levels (pylblrtm/atmosphere.py:117-141), same operation order so
+// the result matches the host NumPy version bit for bit.
+__global__ void build_layers_kernel(const double* __restrict__ p_hpa, const double* __restrict__ t_k,
+                                    const double* __restrict__ vmr, int n_prof, int n_lev, int n_gas,
+                                    double col_factor, double* __restrict__ p_atm,
+                                    double* __restrict__ t_layer, double* __restrict__ vmr_layer,
+                                    double* __restrict__ col) {
+  const int n_lay = n_lev - 1;
+  const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= (long long)n_prof * n_lay) return;
+  const int b = (int)(idx / n_lay), k = (int)(idx % n_lay);
+  const double p0 = p_hpa[(long long)b * n_lev + k], p1 = p_hpa[(long long)b * n_lev + k + 1];
+  p_atm[idx] = __ddiv_rn(__dsqrt_rn(__dmul_rn(p0, p1)), P_STD_HPA);
+  const double t0 = t_k[(long long)b * n_lev + k], t1 = t_k[(long long)b * n_lev + k + 1];
+  t_layer[idx] = __dmul_rn(0.5, __dadd_rn(t0, t1));
+  const double dp_pa = __dmul_rn(fabs(__dsub_rn(p1, p0)), 100.0);
+  const double air = __ddiv_rn(__dmul_rn(col_factor, dp_pa), 1e4);
+  for (int g = 0; g < n_gas; ++g) {
+    const double* v = vmr + ((long long)b * n_gas + g) * n_lev;
+    const double vl = __dmul_rn(0.5, __dadd_rn(v[k], v[k + 1]));
+    const long long o = ((long long)b * n_gas + g) * n_lay + k;
+    vmr_layer[o] = vl;
+    col[o] = __dmul_rn(vl, air);
+  }
+}
+
+// np.interp(x, xp, fp) for increasing xp, clamped at both ends
+// (pylblrtm/spectral_data.py:52 calls np.interp).
+__device__ double interp_clamped(double x, const double* __restrict__ xp, const double* __restrict__ fp,
+                                 int n) {
+  if (isnan(x)) return x;
+  if (x >= xp[n - 1]) return fp[n - 1];
+  if (x < xp[0]) return fp[0];
+  int lo = 0, hi = n - 1;            // invariant xp[lo] <= x < xp[hi]
+  while (hi - lo > 1) {
+    const int mid = (lo + hi) >> 1;
+    if (xp[mid] <= x) lo = mid; else hi = mid;
+  }
+  if (x == xp[lo]) return fp[lo];
+  const double slope = __ddiv_rn(__dsub_rn(fp[lo + 1], fp[lo]), __dsub_rn(xp[lo + 1], xp[lo]));
+  double r = __dadd_rn(__dmul_rn(slope, __dsub_rn(x, xp[lo])), fp[lo]);
+  if (isnan(r)) {
+    r = __dadd_rn(__dmul_rn(slope, __dsub_rn(x, xp[lo + 1])), fp[lo + 1]);
+    if (isnan(r) && fp[lo] == fp[lo + 1]) r = fp[lo];
+  }
+  return r;
+}
+
+// Per (profile, layer, group): partial pressures, column, Q(296)/Q(T) and
+// sqrt(T/M) (pylblrtm/forward.py:236-240, 249-259, 292).
+__global__ void layer_groups_kernel(const double* __restrict__ t_layer, const double* __restrict__ p_atm,
+                                    const double* __restrict__ vmr_layer, const double* __restrict__ col,
+                                    int n_rows, int n_lay, int n_gas, int n_grp,
+                                    const int* __restrict__ grp_gas, const double* __restrict__ grp_mass,
+                                    const int* __restrict__ tips_off, const int* __restrict__ tips_len,
+                                    const double* __restrict__ tips_t, const double* __restrict__ tips_q,
+                                    LayerGroup* __restrict__ out) {
+  const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= (long long)n_rows * n_grp) return;
+  const int row = (int)(idx / n_grp), g = (int)(idx % n_grp);
+  const int b = row / n_lay, k = row % n_lay;
+  const int gas = grp_gas[g];
+  const double T = t_layer[row], P = p_atm[row];
+  const long long gi = ((long long)b * n_gas + gas) * n_lay + k;
+  const double v = vmr_layer[gi];
+  LayerGroup lg;
+  lg.T = T;
+  lg.p_self = __dmul_rn(v, P);
+  lg.p_air = __dsub_rn(P, lg.p_self);
+  lg.col = col[gi];
+  const double* xt = tips_t + tips_off[g];
+  const double* xq = tips_q + tips_off[g];
+  const int n = tips_len[g];
+  const double q_ref = interp_clamped(T_REF, xt, xq, n);
+  lg.q_ratio = __ddiv_rn(q_ref, interp_clamped(T, xt, xq, n));
+  lg.dop = __dsqrt_rn(__ddiv_rn(T, grp_mass[g]));
+  out[idx] = lg;
+}
+
+// ---------------------------------------------------------------------------
+// Candidate-line sort. Keys are nu0 of the lines the reference masks in
+// (pylblrtm/forward.py:215-220) and +inf otherwise; ties break on the input
+// index so the order, and every sum built on it, is deterministic.
+constexpr int SORT_BLOCK = 2048;   // elements sorted per CTA in shared memory
+
+__global__ void sort_keys_kernel(const double* __restrict__ nu0, const double* __restrict__ shift,
+                                 const int* __restrict__ gid, int n_lines, int n_pad, double mask_lo,
+                                 double mask_hi, double p_max, double* __restrict__ keys,
+                                 int* __restrict__ vals, int* __restrict__ n_kept, double* __restrict__ max_sb) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n_pad) return;
+  double key = CUDART_INF;
+  if (i < n_lines && gid[i] >= 0) {
+    const double sb = __dmul_rn(fabs(shift[i]), p_max);      // forward.py:191
+    const double v = nu0[i];
+    // a non-finite centre never lies in a tile window, so it can be dropped here
+    if (isfinite(v) && v >= __dsub_rn(mask_lo, sb) && v <= __dadd_rn(mask_hi, sb)) {
+      key = v;
+      atomicAdd(n_kept, 1);
+      // shift bound of a kept line (non-negative doubles order like their bits)
+      atomicMax((unsigned long long*)max_sb, (unsigned long long)__double_as_longlong(sb));
+    }
+  }
+  keys[i] = key;
+  vals[i] = i;
+}
+
+__device__ __forceinline__ bool key_greater(double ka, int va, double kb, int vb) {
+  return ka > kb || (ka == kb && va > vb);
+}
+
+// Sort stages whose stride is below SORT_BLOCK, in shared memory. With
+// k_first = 2 the kernel sorts every block fully; otherwise it finishes the
+// merge of bitonic size k (strides SORT_BLOCK/2 .. 1).
+__global__ void __launch_bounds__(SORT_BLOCK / 2)
+bitonic_smem_kernel(double* __restrict__ keys, int* __restrict__ vals, int k_first, int k_last) {
+  __shared__ double sk[SORT_BLOCK];
+  __shared__ int sv[SORT_BLOCK];
+  const int base = blockIdx.x * SORT_BLOCK;
+  for (int i = threadIdx.x; i < SORT_BLOCK; i += blockDim.x) {
+    sk[i] = keys[base + i];
+    sv[i] = vals[base + i];
+  }
+  __syncthreads();
+  for (int k = k_first; k <= k_last; k <<= 1) {
+    for (int j = (k == k_first && k_first > SORT_BLOCK) ? SORT_BLOCK / 2 : k >> 1; j > 0; j >>= 1) {
+      const int t = threadIdx.x;
+      const int i = 2 * t - (t & (j - 1));
+      const int p = i + j;
+      const bool asc = (((base + i) & k) == 0);
+      const double ka = sk[i], kb = sk[p];
+      const int va = sv[i], vb = sv[p];
+      if (key_greater(ka, va, kb, vb) == asc) {
+        sk[i] = kb; sk[p] = ka; sv[i] = vb; sv[p] = va;
+      }
+      __syncthreads();
+    }
+  }
+  for (int i = threadIdx.x; i < SORT_BLOCK; i += blockDim.x) {
+    keys[base + i] = sk[i];
+    vals[base + i] = sv[i];
+  }
+}
+
+__global__ void bitonic_global_kernel(double* __restrict__ keys, int* __restrict__ vals, int n_pad, int k,
+                                      int j) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= n_pad / 2) return;
+  const int i = 2 * t - (t & (j - 1));
+  const int p = i + j;
+  const bool asc = ((i & k) == 0);
+  const double ka = keys[i], kb = keys[p];
+  const int va = vals[i], vb = vals[p];
+  if (key_greater(ka, va, kb, vb) == asc) {
+    keys[i] = kb; keys[p] = ka; vals[i] = vb; vals[p] = va;
+  }
+}
+
+// Sorted structure-of-records copy of the kept lines.
+__global__ void gather_lines_kernel(const double* __restrict__ nu0, const double* __restrict__ sref,
+                                    const double* __restrict__ g_air, const double* __restrict__ g_self,
+                                    const double* __restrict__ elow, const double* __restrict__ n_air,
+                                    const double* __restrict__ shift, const int* __restrict__ gid,
+                                    const int* __restrict__ order, const int* __restrict__ n_kept,
+                                    int n_lines, LineIn* __restrict__ out) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= n_lines || j >= *n_kept) return;
+  const int i = order[j];
+  LineIn r;
+  r.nu0 = nu0[i]; r.sref = sref[i]; r.g_air = g_air[i]; r.g_self = g_self[i];
+  r.elow = elow[i]; r.n_air = n_air[i]; r.shift = shift[i]; r.gid = gid[i]; r.src = i;
+  out[j] = r;
+}
+
+// Candidate range of each reference tile (pylblrtm/forward.py:295-301): the
+// sorted lines whose unshifted centre lies within the tile window widened by
+// the largest pressure shift. The exact test on the shifted centre is applied
+// per layer inside the summation kernels.
+__global__ void tile_ranges_kernel(const LineIn* __restrict__ lines, const int* __restrict__ n_kept,
+                                   double nu_min, double step, long long n_nu, int tile_samples,
+                                   double cutoff, double pad, int n_tiles, int2* __restrict__ ranges) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= n_tiles) return;
+  const long long i0 = (long long)t * tile_samples;
+  const long long i1 = min(i0 + tile_samples, n_nu) - 1;
+  const double lo_nu = __dsub_rn(__dsub_rn(grid_nu(nu_min, step, i0), cutoff), pad);
+  const double hi_nu = __dadd_rn(__dadd_rn(grid_nu(nu_min, step, i1), cutoff), pad);
+  const int n = *n_kept;
+  int a = 0, b = n;               // first index with nu0 >= lo_nu
+  while (a < b) { const int m = (a + b) >> 1; if (lines[m].nu0 < lo_nu) a = m + 1; else b = m; }
+  int c = a, d = n;               // first index with nu0 > hi_nu
+  while (c < d) { const int m = (c + d) >> 1; if (lines[m].nu0 <= hi_nu) c = m + 1; else d = m; }
+  ranges[t] = make_int2(a, c);
+}
+
+// ---------------------------------------------------------------------------
+// Line prep (pylblrtm/forward.py:257-292): shifted centre, temperature-scaled
+// strength with column and 1/R(nuc, T), Lorentz and Doppler widths.
+struct ScaledLine {
+  double nuc, S, gamma, alpha;
+  bool active;
+};
+
+__device__ __forceinline__ double radiation_term(double nu, double T) {
+  // nu * tanh(c2 nu / 2T), evaluated as ((0.5 c2) nu) / T like forward.py:48
+  return __dmul_rn(nu, tanh(__ddiv_rn(__dmul_rn(0.5 * C2, nu), T)));
+}
+
+__device__ __forceinline__ ScaledLine scale_line(const LineIn& L, const LayerGroup& G, int* err,
+                                                 int err_key) {
+  ScaledLine s;
+  s.active = G.col != 0.0;                                      // forward.py:253-255
+  if (!s.active) return s;
+  const double T = G.T;
+  s.nuc = __dadd_rn(L.nu0, __dmul_rn(L.shift, G.p_air));        // forward.py:263
+  double S = __dmul_rn(L.sref, G.q_ratio);
+  S = __dmul_rn(S, exp(__dmul_rn(__dmul_rn(-C2, L.elow), __dsub_rn(__ddiv_rn(1.0, T), 1.0 / T_REF))));
+  S = __dmul_rn(S, -expm1(__ddiv_rn(__dmul_rn(-C2, L.nu0), T)));
+  S = __ddiv_rn(S, -expm1(__ddiv_rn(__dmul_rn(-C2, L.nu0), T_REF)));
+  S = __dmul_rn(S, G.col);
+  S = __ddiv_rn(S, radiation_term(s.nuc, T));                   // forward.py:270-278
+  if (!isfinite(S) || S < 0.0) flag_error(err, err_key);        // forward.py:280-283
+  s.S = S;
+  s.gamma = __dmul_rn(pow(__ddiv_rn(T_REF, T), L.n_air),
+                      __dadd_rn(__dmul_rn(L.g_air, G.p_air), __dmul_rn(L.g_self, G.p_self)));
+  s.alpha = __dmul_rn(__dmul_rn(L.nu0, DOPPLER), G.dop);        // forward.py:292
+  return s;
+}
+
+__global__ void line_prep_f64_kernel(const LineIn* __restrict__ lines, const int* __restrict__ n_kept,
+                                     int n_lines, const LayerGroup* __restrict__ lg, int n_rows, int n_grp,
+                                     LineF64* __restrict__ out, int* err) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  const int row = blockIdx.y;
+  if (j >= n_lines || row >= n_rows) return;
+  LineF64 r;
+  r.nuc = CUDART_NAN; r.inv_ad = 0.0; r.y = 0.0; r.amp = 0.0;
+  if (j < *n_kept) {
+    const LineIn L = lines[j];
+    const ScaledLine s = scale_line(L, lg[(long long)row * n_grp + L.gid], err, row * (n_grp + 1) + L.gid);
+    if (s.active) {
+      r.nuc = s.nuc;
+      r.inv_ad = __ddiv_rn(SQRT_LN2, s.alpha);
+      r.y = __ddiv_rn(__dmul_rn(SQRT_LN2, s.gamma), s.alpha);
+      r.amp = __dmul_rn(__ddiv_rn(VOIGT_K, s.alpha), s.S);
+    }
+  }
+  out[(long long)row * n_lines + j] = r;
+}
+
+__global__ void line_prep_f32_kernel(const LineIn* __restrict__ lines, const int* __restrict__ n_kept,
+                                     int n_lines, const LayerGroup* __restrict__ lg, int n_rows, int n_grp,
+                                     double nu_min, double step, LineF32* __restrict__ out, int* err) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  const int row = blockIdx.y;
+  if (j >= n_lines || row >= n_rows) return;
+  LineF32 r;
+  r.nuc = CUDART_NAN; r.j0 = 0; r.b = 0.f; r.a = 0.f; r.y = 0.f; r.amp = 0.f; r.amp_far = 0.f;
+  if (j < *n_kept) {
+    const LineIn L = lines[j];
+    const ScaledLine s = scale_line(L, lg[(long long)row * n_grp + L.gid], err, row * (n_grp + 1) + L.gid);
+    if (s.active) {
+      const double sc = SQRT_LN2 / s.alpha;
+      double jd = rint((s.nuc - nu_min) / step);
+      jd = fmin(fmax(jd, -2.0e9), 2.0e9);     // host guarantees |j0| < 2^31 for kept lines
+      const int j0 = (int)jd;
+      const double rem = s.nuc - grid_nu(nu_min, step, j0);
+      const double y = SQRT_LN2 * s.gamma / s.alpha;
+      const double amp = VOIGT_K / s.alpha * s.S;
+      r.nuc = s.nuc;
+      r.j0 = j0;
+      r.b = (float)(rem * sc);
+      r.a = (float)(step * sc);
+      r.y = (float)y;
+      r.amp = (float)amp;
+      r.amp_far = (float)(amp * y * INV_SQRT_PI);
+    }
+  }
+  out[(long long)row * n_lines + j] = r;
+}
+
+}  // namespace lbl
+
+using namespace lbl;
+
+static inline unsigned grid1(long long n, int bs) { return (unsigned)((n + bs - 1) / bs); }
+
+extern "C" int lbl_build_layers(const double* p_hpa, const double* t_k, const double* vmr, int n_prof,
+                                int n_lev, int n_gas, double col_factor, double* p_atm, double* t_layer,
+                                double* vmr_layer, double* col, void* stream) {
+  if (n_prof < 1 || n_lev < 2 || n_gas < 0 || !p_hpa || !t_k || !p_atm || !t_layer ||
+      (n_gas > 0 && (!vmr || !vmr_layer || !col)))
+    return lbl_set_error(LBL_EINVAL, "lbl_build_layers: bad arguments");
+  const long long n = (long long)n_prof * (n_lev - 1);
+  build_layers_kernel<<<grid1(n, 128), 128, 0, (cudaStream_t)stream>>>(
+      p_hpa, t_k, vmr, n_prof, n_lev, n_gas, col_factor, p_atm, t_layer, vmr_layer, col);
+  return lbl_check_launch("lbl_build_layers");
+}
+
+extern "C" int lbl_layer_groups(const double* t_layer, const double* p_atm, const double* vmr_layer,
+                                const double* col, int n_prof, int n_lay, int n_gas, int n_grp,
+                                const int* grp_gas, const double* grp_mass, const int* tips_off,
+                                const int* tips_len, const double* tips_t, const double* tips_q,
+                                LayerGroup* out, void* stream) {
+  if (n_prof < 1 || n_lay < 1 || n_grp < 1 || n_gas < 1 || !out)
+    return lbl_set_error(LBL_EINVAL, "lbl_layer_groups: bad arguments");
+  const long long n = (long long)n_prof * n_lay * n_grp;
+  layer_groups_kernel<<<grid1(n, 128), 128, 0, (cudaStream_t)stream>>>(
+      t_layer, p_atm, vmr_layer, col, n_prof * n_lay, n_lay, n_gas, n_grp, grp_gas, grp_mass, tips_off,
+      tips_len, tips_t, tips_q, out);
+  return lbl_check_launch("lbl_layer_groups");
+}
+
+static int pad_pow2(int n) {
+  int p = SORT_BLOCK;
+  while (p < n) p <<= 1;
+  return p;
+}
+
+extern "C" size_t lbl_sort_workspace_bytes(int n_lines) {
+  if (n_lines < 0) return 0;
+  const size_t n_pad = (size_t)pad_pow2(n_lines);
+  return n_pad * (sizeof(double) + sizeof(int));
+}
+
+extern "C" int lbl_sort_lines(const double* nu0, const double* shift, const int* gid, int n_lines,
+                              double mask_lo, double mask_hi, double p_max, void* workspace,
+                              size_t workspace_bytes, int* order, int* n_kept, double* max_shift_bound,
+                              void* stream) {
+  if (n_lines < 1 || n_lines > (1 << 30) || !nu0 || !shift || !gid || !workspace || !order || !n_kept ||
+      !max_shift_bound)
+    return lbl_set_error(LBL_EINVAL, "lbl_sort_lines: bad arguments");
+  if (workspace_bytes < lbl_sort_workspace_bytes(n_lines))
+    return lbl_set_error(LBL_EINVAL, "lbl_sort_lines: workspace too small");
+  cudaStream_t s = (cudaStream_t)stream;
+  const int n_pad = pad_pow2(n_lines);
+  double* keys = (double*)workspace;
+  int* vals = (int*)(keys + n_pad);
+  cudaMemsetAsync(n_kept, 0, sizeof(int), s);
+  cudaMemsetAsync(max_shift_bound, 0, sizeof(double), s);
+  sort_keys_kernel<<<grid1(n_pad, 256), 256, 0, s>>>(nu0, shift, gid, n_lines, n_pad, mask_lo, mask_hi,
+                                                     p_max, keys, vals, n_kept, max_shift_bound);
+  const int n_blk = n_pad / SORT_BLOCK;
+  bitonic_smem_kernel<<<n_blk, SORT_BLOCK / 2, 0, s>>>(keys, vals, 2, SORT_BLOCK);
+  for (int k = 2 * SORT_BLOCK; k <= n_pad; k <<= 1) {
+    for (int j = k >> 1; j >= SORT_BLOCK; j >>= 1)
+      bitonic_global_kernel<<<grid1(n_pad / 2, 256), 256, 0, s>>>(keys, vals, n_pad, k, j);
+    bitonic_smem_kernel<<<n_blk, SORT_BLOCK / 2, 0, s>>>(keys, vals, k, k);
+  }
+  cudaMemcpyAsync(order, vals, sizeof(int) * (size_t)n_lines, cudaMemcpyDeviceToDevice, s);
+  return lbl_check_launch("lbl_sort_lines");
+}
+
+extern "C" int lbl_gather_lines(const double* nu0, const double* sref, const double* g_air,
+                                const double* g_self, const double* elow, const double* n_air,
+                                const double* shift, const int* gid, const int* order, const int* n_kept,
+                                int n_lines, LineIn* out, void* stream) {
+  if (n_lines < 1 || !order || !n_kept || !out)
+    return lbl_set_error(LBL_EINVAL, "lbl_gather_lines: bad arguments");
+  gather_lines_kernel<<<grid1(n_lines, 256), 256, 0, (cudaStream_t)stream>>>(
+      nu0, sref, g_air, g_self, elow, n_air, shift, gid, order, n_kept, n_lines, out);
+  return lbl_check_launch("lbl_gather_lines");
+}
+
+extern "C" int lbl_tile_ranges(const LineIn* lines, const int* n_kept, double nu_min, double step,
+                               long long n_nu, int tile_samples, double cutoff, double pad, int n_tiles,
+                               int* ranges, void* stream) {
+  if (n_nu < 1 || tile_samples < 1 || n_tiles < 1 || !lines || !n_kept || !ranges)
+    return lbl_set_error(LBL_EINVAL, "lbl_tile_ranges: bad arguments");
+  tile_ranges_kernel<<<grid1(n_tiles, 128), 128, 0, (cudaStream_t)stream>>>(
+      lines, n_kept, nu_min, step, n_nu, tile_samples, cutoff, pad, n_tiles, (int2*)ranges);
+  return lbl_check_launch("lbl_tile_ranges");
+}
+
+extern "C" int lbl_line_prep_f64(const LineIn* lines, const int* n_kept, int n_lines, const LayerGroup* lg,
+                                 int n_rows, int n_grp, LineF64* out, int* err, void* stream) {
+  if (n_lines < 1 || n_rows < 1 || n_rows > 65535 || n_grp < 1 || !lines || !lg || !out)
+    return lbl_set_error(LBL_EINVAL, "lbl_line_prep_f64: bad arguments");
+  dim3 grid(grid1(n_lines, 128), n_rows);
+  line_prep_f64_kernel<<<grid, 128, 0, (cudaStream_t)stream>>>(lines, n_kept, n_lines, lg, n_rows, n_grp,
+                                                               out, err);
+  return lbl_check_launch("lbl_line_prep_f64");
+}
+
+extern "C" int lbl_line_prep_f32(const LineIn* lines, const int* n_kept, int n_lines, const LayerGroup* lg,
+                                 int n_rows, int n_grp, double nu_min, double step, LineF32* out, int* err,
+                                 void* stream) {
+  if (n_lines < 1 || n_rows < 1 || n_rows > 65535 || n_grp < 1 || !lines || !lg || !out || !(step > 0))
+    return lbl_set_error(LBL_EINVAL, "lbl_line_prep_f32: bad arguments");
+  dim3 grid(grid1(n_lines, 128), n_rows);
+  line_prep_f32_kernel<<<grid, 128, 0, (cudaStream_t)stream>>>(lines, n_kept, n_lines, lg, n_rows, n_grp,
+                                                               nu_min, step, out, err);
+  return lbl_check_launch("lbl_line_prep_f32");
+}

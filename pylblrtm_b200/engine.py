@@ -1,0 +1,444 @@
+"""Device pipeline of the line-by-line engine (host orchestration of the CUDA kernels).
+
+One call of :func:`optical_depth` runs, on the current CUDA stream:
+
+1. ``lbl_build_layers``  levels -> layers (or an upload of host layers)
+2. ``lbl_layer_groups``  per (layer, line group) pressures, column, Q(296)/Q(T)
+3. ``lbl_sort_lines``    reference band mask + sort by centre
+4. ``lbl_gather_lines``  sorted line records
+5. ``lbl_tile_ranges``   candidate lines of every reference tile
+6. ``lbl_line_prep_*``   per (layer, line) strengths and widths
+7. ``lbl_tau_tiles_*``   Voigt sums x R(nu, T) -> od[layer, nu]
+8. ``lbl_layer_sum_exp_*`` (optional) column tau and exp(-tau/mu)
+
+Host work is limited to what the reference does once per call in Python: the
+(mol, iso) group selection with its warnings and errors
+(``pylblrtm/forward.py:189-245``) and the grid and tile sizes
+(``forward.py:141-142, 175-176``). Everything per line or per grid point runs on
+the GPU. There is no CPU path.
+"""
+
+from __future__ import annotations
+
+import math
+import warnings
+from dataclasses import dataclass, field
+from typing import Dict, List, Optional, Sequence, Tuple
+
+import numpy as np
+
+from . import _lib
+from .atmosphere import COLUMN_FACTOR, P_STD_HPA
+from .hitran_ids import MOL_ID_TO_NAME
+from .spectral_data import SpectralData
+
+INT_MAX = 2**31 - 1
+PRECISIONS = ("fp32", "fp64")
+
+
+def _torch():
+    import torch
+    if not torch.cuda.is_available():
+        raise _lib.EngineUnavailable(
+            "no CUDA device is available; the line-by-line engine runs only on the GPU")
+    return torch
+
+
+@dataclass
+class Group:
+    """One (mol_id, iso_id) group that contributes, in reference order."""
+    mol_id: int
+    iso_id: int
+    gas: str
+    molar_mass: float
+    tips_t: np.ndarray
+    tips_q: np.ndarray
+
+
+@dataclass
+class Grid:
+    """Uniform grid nu_i = nu_min + i*step and the reference tile size."""
+    nu_min: float
+    step: float
+    n_nu: int
+    tile_samples: int
+
+    @property
+    def nu(self) -> np.ndarray:
+        return self.nu_min + np.arange(self.n_nu, dtype=np.float64) * self.step
+
+    def nu_at(self, i: int) -> float:
+        return float(self.nu_min + np.float64(i) * self.step)
+
+
+def make_grid(nu_min: float, nu_max: float, step: float, tile_width: float) -> Grid:
+    """Grid size (forward.py:141) and tile size (forward.py:175-176)."""
+    n = int(np.ceil((nu_max - nu_min) / step)) + 1
+    return Grid(float(nu_min), float(step), n, tile_samples_for(float(nu_min), float(step), n, tile_width))
+
+
+def tile_samples_for(nu_min: float, step: float, n_nu: int, tile_width: float) -> int:
+    """Reference tile length: floor(tile_width / (nu[1]-nu[0]) + 1e-8), at least 1."""
+    if n_nu > 1:
+        nu01 = nu_min + np.arange(2, dtype=np.float64) * step
+        eff = float(nu01[1] - nu01[0])
+    else:
+        eff = 0.001
+    return max(1, int(np.floor(tile_width / eff + 1e-8)))
+
+
+def grid_from_array(nu: np.ndarray, tile_width: float) -> Grid:
+    """Recover (nu_min, step) from a grid array built as nu_min + arange(n)*step."""
+    nu = np.asarray(nu, dtype=np.float64)
+    if nu.ndim != 1 or nu.size < 1:
+        raise ValueError("nu must be a non-empty 1-D array")
+    n = nu.size
+    if n == 1:
+        return Grid(float(nu[0]), 0.001, 1, tile_samples_for(float(nu[0]), 0.001, 1, tile_width))
+    d = float(nu[1] - nu[0])
+    idx = np.arange(n, dtype=np.float64)
+    for digits in (None, 15, 14, 13, 12, 11, 10, 9):
+        s = d if digits is None else float(np.round(d, digits))
+        if s > 0 and np.array_equal(nu[0] + idx * s, nu):
+            return Grid(float(nu[0]), s, n, tile_samples_for(float(nu[0]), s, n, tile_width))
+    raise ValueError("the GPU engine needs a uniform grid nu_min + arange(n) * step")
+
+
+def select_groups(sd: SpectralData, profile_gases: Sequence[str], nu_first: float, nu_last: float,
+                  cutoff: float, p_max: float, warn_level: int) -> Tuple[List[Group], np.ndarray]:
+    """Host replica of the group selection of forward.py:189-245.
+
+    Returns the contributing groups in sorted (mol_id, iso_id) order and the
+    group index of every line (-1 for lines of skipped groups). Emits the same
+    RuntimeWarnings and raises the same KeyError as the reference.
+    """
+    lines = sd.lines
+    mol = np.asarray(lines["mol_id"])
+    iso = np.asarray(lines["iso_id"])
+    nu0 = np.asarray(lines["nu0"], dtype=np.float64)
+    shift = np.asarray(lines["shift"], dtype=np.float64)
+    n = nu0.size
+    gid = np.full(n, -1, dtype=np.int32)
+    if n == 0:
+        return [], gid
+    mol64 = mol.astype(np.int64)
+    iso64 = iso.astype(np.int64)
+    small = (mol64.min() >= 0 and iso64.min() >= 0 and mol64.max() < 4096 and iso64.max() < 1024)
+    if small:
+        key = mol64 * 1024 + iso64
+        present = np.flatnonzero(np.bincount(key))
+        pairs = [(int(k // 1024), int(k % 1024)) for k in present]
+        inv = None
+    else:
+        key2 = np.stack([mol64, iso64], axis=1)
+        uniq, inv = np.unique(key2, axis=0, return_inverse=True)
+        pairs = [(int(a), int(b)) for a, b in uniq]
+        inv = inv.reshape(-1)
+    sb = np.abs(shift) * p_max                                         # forward.py:191
+    in_band = (nu0 >= nu_first - cutoff - sb) & (nu0 <= nu_last + cutoff + sb)
+    if small:
+        band_counts = np.bincount(key[in_band], minlength=int(key.max()) + 1)
+    else:
+        band_counts = np.bincount(inv[in_band], minlength=len(pairs))
+    groups: List[Group] = []
+    lut_pairs: Dict[int, int] = {}
+    for pi, (m, i) in enumerate(pairs):
+        gas = MOL_ID_TO_NAME.get(int(m))
+        if gas is None:
+            warnings.warn(f"mol_id={m} is not in the HITRAN catalogue; lines skipped.",
+                          RuntimeWarning, stacklevel=warn_level)
+            continue
+        if gas not in profile_gases:
+            warnings.warn(
+                f"Gas '{gas}' (mol_id={m}, iso_id={i}) is in the "
+                f"spectral data but not in the atmospheric profile vmr; "
+                f"its lines are skipped.", RuntimeWarning, stacklevel=warn_level)
+            continue
+        cnt = band_counts[m * 1024 + i] if small else band_counts[pi]
+        if cnt == 0:
+            continue
+        mm = sd.molar_masses.get((int(m), int(i)))
+        if mm is None:
+            warnings.warn(f"No molar mass found for (mol_id={m}, iso_id={i}); "
+                          f"using dry-air mass as fallback.", RuntimeWarning, stacklevel=warn_level)
+            mm = 28.97
+        tkey = (int(m), int(i))
+        if tkey not in sd.tips:
+            raise KeyError(f"No TIPS data for (mol_id={m}, iso_id={i}). "
+                           f"Available: {sorted(sd.tips.keys())}")
+        t_arr, q_arr = sd.tips[tkey]
+        if np.asarray(t_arr).size == 0 or np.asarray(t_arr).size != np.asarray(q_arr).size:
+            raise ValueError("array of sample points is empty" if np.asarray(t_arr).size == 0
+                             else "fp and xp are not of the same length.")
+        lut_pairs[m * 1024 + i if small else pi] = len(groups)
+        groups.append(Group(int(m), int(i), gas, float(mm), np.asarray(t_arr, np.float64),
+                            np.asarray(q_arr, np.float64)))
+    if groups:
+        if small:
+            lut = np.full(int(key.max()) + 1, -1, dtype=np.int32)
+            for k, g in lut_pairs.items():
+                lut[k] = g
+            gid = lut[key]
+        else:
+            lut = np.full(len(pairs), -1, dtype=np.int32)
+            for k, g in lut_pairs.items():
+                lut[k] = g
+            gid = lut[inv]
+    return groups, gid
+
+
+@dataclass
+class LayerInput:
+    """Either levels (built into layers on the device) or ready layers."""
+    gases: List[str]
+    levels_p: Optional[np.ndarray] = None   # [n_prof, n_lev] hPa
+    levels_t: Optional[np.ndarray] = None   # [n_prof, n_lev] K
+    levels_vmr: Optional[np.ndarray] = None  # [n_prof, n_gas, n_lev]
+    layer_p: Optional[np.ndarray] = None    # [n_prof, n_lay] atm
+    layer_t: Optional[np.ndarray] = None
+    layer_vmr: Optional[np.ndarray] = None  # [n_prof, n_gas, n_lay]
+    layer_col: Optional[np.ndarray] = None
+
+    @property
+    def n_prof(self) -> int:
+        return (self.levels_p if self.levels_p is not None else self.layer_p).shape[0]
+
+    @property
+    def n_lay(self) -> int:
+        if self.levels_p is not None:
+            return self.levels_p.shape[1] - 1
+        return self.layer_p.shape[1]
+
+    def p_max_atm(self) -> float:
+        """Largest layer pressure [atm], forward.py:190 (host copy of the device formula)."""
+        if self.layer_p is not None:
+            return float(self.layer_p.max()) if self.layer_p.size else 1.0
+        p = self.levels_p
+        return float((np.sqrt(p[:, :-1] * p[:, 1:]) / P_STD_HPA).max())
+
+
+@dataclass
+class EngineResult:
+    od: object = None              # torch tensor [n_prof, n_lay, n_nu] (float32 or float64)
+    trans: object = None           # torch float64 [n_prof, n_nu]
+    tau: object = None             # torch float64 [n_prof, n_nu]
+    evals: int = 0                 # Voigt evaluations under the reference tile rule
+    groups: List[Group] = field(default_factory=list)
+
+
+def _upload(torch, a, dtype, device):
+    return torch.from_numpy(np.ascontiguousarray(a, dtype=dtype)).to(device, non_blocking=False)
+
+
+def sort_launches(n_lines: int) -> int:
+    """Kernels enqueued by lbl_sort_lines for n_lines (keys + bitonic stages)."""
+    n_pad = 2048
+    while n_pad < n_lines:
+        n_pad <<= 1
+    n, k = 2, 4096
+    while k <= n_pad:
+        n += (k.bit_length() - 1) - 11 + 1
+        k <<= 1
+    return n
+
+
+class Job:
+    """Device-resident inputs of one forward call.
+
+    Construction does the host part (group selection with the reference's
+    warnings/errors, grid sizes) and uploads lines, levels and partition tables;
+    :meth:`run` then does only device work.
+    """
+
+    def __init__(self, sd: SpectralData, layers: LayerInput, grid: Grid, cutoff: float, warn_level: int = 4):
+        _lib.load()
+        torch = _torch()
+        self.torch = torch
+        self.dev = torch.device("cuda", torch.cuda.current_device())
+        self.grid, self.cutoff, self.layers = grid, float(cutoff), layers
+        self.n_prof, self.n_lay = layers.n_prof, layers.n_lay
+        self.p_max = layers.p_max_atm() if self.n_lay > 0 else 1.0
+        self.nu_first, self.nu_last = grid.nu_at(0), grid.nu_at(grid.n_nu - 1)
+        self.groups, gid = select_groups(sd, layers.gases, self.nu_first, self.nu_last, self.cutoff,
+                                         self.p_max, warn_level + 1)
+        self.n_lines = int(gid.size)
+        self.h2d_bytes = 0
+        self.empty = not self.groups or self.n_lay == 0
+        if self.empty:
+            return
+        if self.n_lines > (1 << 30):
+            raise ValueError("at most 2^30 lines per call")
+        span = (self.nu_last - self.nu_first + 2 * self.cutoff) / grid.step + 2 * grid.n_nu
+        if not math.isfinite(span) or span > 1.5e9:
+            raise ValueError("grid index range exceeds the engine's 32-bit line index")
+        up = self._up
+        dev = self.dev
+        if layers.levels_p is not None:
+            self.lv = (up(layers.levels_p, np.float64), up(layers.levels_t, np.float64),
+                       up(layers.levels_vmr, np.float64))
+            self.lay = None
+        else:
+            self.lv = None
+            self.lay = (up(layers.layer_p, np.float64), up(layers.layer_t, np.float64),
+                        up(layers.layer_vmr, np.float64), up(layers.layer_col, np.float64))
+        gas_index = {g: i for i, g in enumerate(layers.gases)}
+        offs = np.cumsum([0] + [g.tips_t.size for g in self.groups[:-1]])
+        self.grp = (up([gas_index[g.gas] for g in self.groups], np.int32),
+                    up([g.molar_mass for g in self.groups], np.float64),
+                    up(offs, np.int32), up([g.tips_t.size for g in self.groups], np.int32),
+                    up(np.concatenate([g.tips_t for g in self.groups]), np.float64),
+                    up(np.concatenate([g.tips_q for g in self.groups]), np.float64))
+        L = sd.lines
+        self.lines_in = tuple(up(L[k], np.float64) for k in ("nu0", "Sref", "g_air", "g_self", "Elow",
+                                                             "n_air", "shift"))
+        self.gid = up(gid, np.int32)
+        fin = np.abs(np.asarray(L["shift"], np.float64))
+        fin = fin[np.isfinite(fin)]
+        self.pad = (float(fin.max()) * self.p_max if fin.size else 0.0) * (1 + 1e-9) + 1e-9
+
+    def _up(self, a, dtype):
+        t = _upload(self.torch, a, dtype, self.dev)
+        self.h2d_bytes += t.numel() * t.element_size()
+        return t
+
+    def run(self, precision: str = "fp32", mu: Optional[Sequence[float]] = None, want_od: bool = True,
+            want_tau: bool = False, want_trans: bool = False, count_evals: bool = False,
+            timer: Optional[dict] = None) -> EngineResult:
+        """All device stages; ``timer`` (dict) receives CUDA-event times of the summation kernel."""
+        if precision not in PRECISIONS:
+            raise ValueError(f"precision must be one of {PRECISIONS}, got {precision!r}")
+        torch, dev = self.torch, self.dev
+        stream = torch.cuda.current_stream().cuda_stream
+        grid = self.grid
+        n_prof, n_lay, n_nu = self.n_prof, self.n_lay, grid.n_nu
+        n_rows = n_prof * n_lay
+        res = EngineResult(groups=self.groups)
+        od_dtype = torch.float32 if precision == "fp32" else torch.float64
+        self.launches = 0
+
+        def finish(od):
+            res.od = od if want_od else None
+            if want_tau or want_trans:
+                mu_d = torch.as_tensor(np.broadcast_to(np.asarray(1.0 if mu is None else mu, np.float64),
+                                                       (n_prof,)).copy()).to(dev)
+                tau = torch.empty((n_prof, n_nu), dtype=torch.float64, device=dev) if want_tau else None
+                tr = torch.empty((n_prof, n_nu), dtype=torch.float64, device=dev) if want_trans else None
+                fn = "lbl_layer_sum_exp_f32" if od.dtype == torch.float32 else "lbl_layer_sum_exp_f64"
+                _lib.call(fn, _lib.ptr(od), n_prof, n_lay, n_nu, _lib.ptr(mu_d), _lib.ptr(tr), _lib.ptr(tau),
+                          stream)
+                self.launches += 1
+                res.tau, res.trans = tau, tr
+            return res
+
+        if self.empty:
+            return finish(torch.zeros((n_prof, n_lay, n_nu), dtype=od_dtype, device=dev))
+
+        # layers
+        n_gas = len(self.layers.gases)
+        if self.lv is not None:
+            lp, lt, lv = self.lv
+            p_atm = torch.empty((n_prof, n_lay), dtype=torch.float64, device=dev)
+            t_lay = torch.empty_like(p_atm)
+            v_lay = torch.empty((n_prof, n_gas, n_lay), dtype=torch.float64, device=dev)
+            col = torch.empty_like(v_lay)
+            _lib.call("lbl_build_layers", lp.data_ptr(), lt.data_ptr(), lv.data_ptr(), n_prof, n_lay + 1, n_gas,
+                      COLUMN_FACTOR, p_atm.data_ptr(), t_lay.data_ptr(), v_lay.data_ptr(), col.data_ptr(),
+                      stream)
+            self.launches += 1
+        else:
+            p_atm, t_lay, v_lay, col = self.lay
+        # per (layer, group)
+        n_grp = len(self.groups)
+        grp_gas, grp_mass, tips_off, tips_len, tips_t, tips_q = self.grp
+        lg = torch.empty((n_rows * n_grp * _lib.SIZEOF_LAYER_GROUP // 8,), dtype=torch.float64, device=dev)
+        _lib.call("lbl_layer_groups", t_lay.data_ptr(), p_atm.data_ptr(), v_lay.data_ptr(), col.data_ptr(),
+                  n_prof, n_lay, n_gas, n_grp, grp_gas.data_ptr(), grp_mass.data_ptr(), tips_off.data_ptr(),
+                  tips_len.data_ptr(), tips_t.data_ptr(), tips_q.data_ptr(), lg.data_ptr(), stream)
+        self.launches += 1
+        # lines: mask, sort, gather
+        d_nu0, d_sref, d_gair, d_gself, d_elow, d_nair, d_shift = self.lines_in
+        n_lines = self.n_lines
+        ws_bytes = _lib.load().lbl_sort_workspace_bytes(n_lines)
+        ws = torch.empty((ws_bytes + 7) // 8, dtype=torch.float64, device=dev)
+        order = torch.empty(n_lines, dtype=torch.int32, device=dev)
+        kept = torch.empty(1, dtype=torch.int32, device=dev)
+        max_sb = torch.empty(1, dtype=torch.float64, device=dev)
+        _lib.call("lbl_sort_lines", d_nu0.data_ptr(), d_shift.data_ptr(), self.gid.data_ptr(), n_lines,
+                  self.nu_first - self.cutoff, self.nu_last + self.cutoff, self.p_max, ws.data_ptr(), ws_bytes,
+                  order.data_ptr(), kept.data_ptr(), max_sb.data_ptr(), stream)
+        self.launches += sort_launches(n_lines)
+        n_kept = int(kept.item())                      # one small device->host read
+        if n_kept == 0:
+            return finish(torch.zeros((n_prof, n_lay, n_nu), dtype=od_dtype, device=dev))
+        lines = torch.empty((n_kept * _lib.SIZEOF_LINE_IN // 8,), dtype=torch.float64, device=dev)
+        _lib.call("lbl_gather_lines", d_nu0.data_ptr(), d_sref.data_ptr(), d_gair.data_ptr(), d_gself.data_ptr(),
+                  d_elow.data_ptr(), d_nair.data_ptr(), d_shift.data_ptr(), self.gid.data_ptr(), order.data_ptr(),
+                  kept.data_ptr(), n_kept, lines.data_ptr(), stream)
+        n_tiles = (n_nu + grid.tile_samples - 1) // grid.tile_samples
+        ranges = torch.empty((n_tiles, 2), dtype=torch.int32, device=dev)
+        _lib.call("lbl_tile_ranges", lines.data_ptr(), kept.data_ptr(), grid.nu_min, grid.step, n_nu,
+                  grid.tile_samples, self.cutoff, self.pad, n_tiles, ranges.data_ptr(), stream)
+        self.launches += 2
+        # per (layer, line) prep and the Voigt sums
+        err = torch.full((1,), INT_MAX, dtype=torch.int32, device=dev)
+        evals = torch.zeros(1, dtype=torch.int64, device=dev) if count_evals else None
+        od = torch.empty((n_prof, n_lay, n_nu), dtype=od_dtype, device=dev)
+        rec = _lib.SIZEOF_LINE_F32 if precision == "fp32" else _lib.SIZEOF_LINE_F64
+        prep = torch.empty((n_rows * n_kept * rec // 8,), dtype=torch.float64, device=dev)
+        if precision == "fp32":
+            _lib.call("lbl_line_prep_f32", lines.data_ptr(), kept.data_ptr(), n_kept, lg.data_ptr(), n_rows, n_grp,
+                      grid.nu_min, grid.step, prep.data_ptr(), err.data_ptr(), stream)
+        else:
+            _lib.call("lbl_line_prep_f64", lines.data_ptr(), kept.data_ptr(), n_kept, lg.data_ptr(), n_rows, n_grp,
+                      prep.data_ptr(), err.data_ptr(), stream)
+        if timer is not None:
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+        _lib.call("lbl_tau_tiles_f32" if precision == "fp32" else "lbl_tau_tiles_f64", prep.data_ptr(), n_kept,
+                  ranges.data_ptr(), t_lay.data_ptr(), n_rows, grid.nu_min, grid.step, n_nu, grid.tile_samples,
+                  self.cutoff, n_grp, od.data_ptr(), err.data_ptr(), _lib.ptr(evals), stream)
+        if timer is not None:
+            e1.record()
+            timer.setdefault("tau_events", []).append((e0, e1))
+        self.launches += 2
+        key = int(err.item())
+        if key != INT_MAX:
+            row, g = divmod(key, n_grp + 1)
+            k = row % n_lay
+            if g < n_grp:
+                raise FloatingPointError(
+                    f"Layer {k}, gas '{self.groups[g].gas}': non-finite or negative line strength")
+            raise FloatingPointError(f"Layer {k}: non-finite optical depth after radiation term")
+        if evals is not None:
+            res.evals = int(evals.item())
+        return finish(od)
+
+
+def optical_depth(sd: SpectralData, layers: LayerInput, grid: Grid, cutoff: float,
+                  precision: str = "fp32", mu: Optional[Sequence[float]] = None,
+                  want_od: bool = True, want_tau: bool = False, want_trans: bool = False,
+                  warn_level: int = 4, count_evals: bool = False) -> EngineResult:
+    """Upload one forward call and run every device stage (see the module docstring)."""
+    if precision not in PRECISIONS:
+        raise ValueError(f"precision must be one of {PRECISIONS}, got {precision!r}")
+    job = Job(sd, layers, grid, cutoff, warn_level + 1)
+    return job.run(precision, mu, want_od, want_tau, want_trans, count_evals)
+
+
+def layer_input_from_profile(profile) -> LayerInput:
+    """Levels of one AtmosphericProfile (layers are built on the device)."""
+    gases = list(profile.vmr.keys())
+    vmr = np.stack([profile.vmr[g] for g in gases])[None] if gases else np.zeros((1, 0, profile.n_levels))
+    return LayerInput(gases=gases, levels_p=profile.pressure_hpa[None, :], levels_t=profile.temperature_k[None, :],
+                      levels_vmr=vmr)
+
+
+def layer_input_from_layers(layers) -> LayerInput:
+    """Host-built layers (the reference's _Layers object)."""
+    gases = list(layers.column_cm2.keys())
+    n = layers.n_layers
+    vmr = np.stack([layers.vmr[g] for g in gases])[None] if gases else np.zeros((1, 0, n))
+    col = np.stack([layers.column_cm2[g] for g in gases])[None] if gases else np.zeros((1, 0, n))
+    return LayerInput(gases=gases, layer_p=np.asarray(layers.pressure_atm, np.float64)[None, :],
+                      layer_t=np.asarray(layers.temperature_k, np.float64)[None, :],
+                      layer_vmr=vmr, layer_col=col)

@@ -1,0 +1,70 @@
+"""The C ABI library loads, exports every declared symbol, and the engine fails loudly without CUDA."""
+
+import ctypes
+import os
+import re
+
+import pytest
+
+from conftest import ROOT
+from pylblrtm_b200 import _lib
+
+HEADER = os.path.join(ROOT, "include", "lblgpu.h")
+
+
+def declared_functions():
+    text = open(HEADER).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(lbl_[a-z0-9_]+)\s*\(", text)))
+
+
+def test_library_exports_every_declared_symbol():
+    lib = ctypes.CDLL(_lib.LIB_PATH)
+    names = declared_functions()
+    assert len(names) >= 15
+    missing = [n for n in names if not hasattr(lib, n)]
+    assert not missing, missing
+
+
+def test_bindings_cover_header():
+    assert sorted(_lib.SIGNATURES) == declared_functions()
+
+
+def test_record_sizes_match_header():
+    class LayerGroup(ctypes.Structure):
+        _fields_ = [(n, ctypes.c_double) for n in ("T", "p_self", "p_air", "col", "q_ratio", "dop")]
+
+    class LineIn(ctypes.Structure):
+        _fields_ = [(n, ctypes.c_double) for n in ("nu0", "sref", "g_air", "g_self", "elow", "n_air",
+                                                   "shift")] + [("gid", ctypes.c_int), ("src", ctypes.c_int)]
+
+    class LineF32(ctypes.Structure):
+        _fields_ = [("nuc", ctypes.c_double), ("j0", ctypes.c_int)] + \
+                   [(n, ctypes.c_float) for n in ("b", "a", "y", "amp", "amp_far")]
+
+    assert ctypes.sizeof(LayerGroup) == _lib.SIZEOF_LAYER_GROUP
+    assert ctypes.sizeof(LineIn) == _lib.SIZEOF_LINE_IN
+    assert ctypes.sizeof(LineF32) == _lib.SIZEOF_LINE_F32
+    assert _lib.SIZEOF_LINE_F64 == 4 * 8
+
+
+def test_host_queries_and_argument_errors():
+    lib = _lib.load()
+    assert lib.lbl_abi_version() == 1
+    assert lib.lbl_sort_workspace_bytes(10) == 2048 * 12
+    assert lib.lbl_sort_workspace_bytes(5000) == 8192 * 12
+    # invalid arguments are rejected before any CUDA call
+    with pytest.raises(RuntimeError, match="bad arguments"):
+        _lib.call("lbl_tau_tiles_f32", 0, 0, 0, 0, 0, 700.0, 0.001, 10, 2000, 25.0, 1, 0, 0, 0, 0)
+    with pytest.raises(RuntimeError, match="bad arguments"):
+        _lib.call("lbl_faddeeva_f32", 0, 0, 5, 0, 0, 3, 0)
+
+
+def test_engine_without_cuda_raises():
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("CUDA present: the no-GPU error path is exercised on CPU-only hosts")
+    import pylblrtm_b200 as lbl
+    from pylblrtm_b200 import synthetic
+    with pytest.raises(_lib.EngineUnavailable, match="no CUDA device"):
+        lbl.compute_transmittance(synthetic.co2_band(50), lbl.us_standard_atmosphere(["CO2"]), 700, 701)

@@ -1,0 +1,216 @@
+"""GPU engine parity: device kernels against the reference's golden vectors and the oracle.
+
+Tolerances (stated per the spec): float64 engine |dT| <= 1e-6, float32 engine
+|dT| <= 1e-5; relative optical-depth errors are bounded separately because
+several goldens are optically thick (T ~ 0 everywhere makes |dT| vacuous).
+"""
+
+import warnings
+
+import numpy as np
+import pytest
+
+import pylblrtm_b200 as lbl
+from conftest import ALL_GOLDEN, SMALL_GOLDEN, golden_case, oracle_inputs
+from oracle import restate
+from pylblrtm_b200 import _lib, engine, synthetic
+from pylblrtm_b200.atmosphere import COLUMN_FACTOR
+from pylblrtm_b200.spectral_data import SpectralData
+
+pytestmark = pytest.mark.gpu
+
+TOL = {"fp64": dict(dT=1e-6, rtau=1e-9, rod=1e-9), "fp32": dict(dT=1e-5, rtau=2e-5, rod=3e-5)}
+
+
+def _run(sd, prof, prm, precision, layers=False):
+    cfg = {"spectral": {"nu_min_cm1": prm["nu_min"], "nu_max_cm1": prm["nu_max"], "step_cm1": prm["step"]},
+           "calculation": {"mu_view": prm["mu"], "line_cutoff_cm1": prm["cutoff"],
+                           "tile_width_cm1": prm["tile"]},
+           "output": {"transmittance": True, "optical_depth": True, "optical_depth_layers": layers},
+           "engine": {"precision": precision}}
+    with warnings.catch_warnings(record=True) as wl:
+        warnings.simplefilter("always")
+        res = lbl.run_forward(sd, prof, cfg)
+    return res, sorted(str(w.message) for w in wl)
+
+
+def _rel(a, b):
+    den = np.abs(b)
+    m = den > 1e-300
+    return float(np.max(np.abs(a - b)[m] / den[m])) if m.any() else 0.0
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+@pytest.mark.parametrize("name", ALL_GOLDEN)
+def test_golden(cuda, name, precision):
+    sd, prof, prm, data = golden_case(name)
+    res, warns = _run(sd, prof, prm, precision, layers="od_layers" in data)
+    tol = TOL[precision]
+    assert res.wavenumber_cm1.size == int(data["n_nu"])
+    assert np.max(np.abs(res.transmittance - data["T"])) <= tol["dT"]
+    assert _rel(res.optical_depth, data["tau"]) <= tol["rtau"]
+    if "od_layers" in data:
+        assert _rel(res.optical_depth_layers, data["od_layers"]) <= tol["rod"]
+    assert warns == sorted(m for m in data["warnings"].tolist() if m)
+
+
+def test_compute_transmittance_matches_golden(cuda):
+    sd, prof, prm, data = golden_case("tile0.5")
+    nu, T = lbl.compute_transmittance(sd, prof, prm["nu_min"], prm["nu_max"], step_cm1=prm["step"],
+                                      line_cutoff_cm1=prm["cutoff"], tile_width_cm1=prm["tile"],
+                                      mu_view=prm["mu"], precision="fp64")
+    assert nu.dtype == np.float64 and T.dtype == np.float64
+    assert np.array_equal(nu, restate.grid(prm["nu_min"], prm["nu_max"], prm["step"]))
+    assert np.max(np.abs(T - data["T"])) <= 1e-9
+
+
+def test_internal_build_optical_depth(cuda):
+    from pylblrtm_b200.forward import _build_optical_depth
+    sd, prof, prm, data = golden_case("tile2.0")
+    nu = restate.grid(prm["nu_min"], prm["nu_max"], prm["step"])
+    od = _build_optical_depth(nu, sd, prof.build_layers(), prm["cutoff"], prm["tile"], precision="fp64")
+    assert od.shape == data["od_layers"].shape and od.dtype == np.float64
+    assert _rel(od, data["od_layers"]) <= 1e-9
+
+
+def test_layers_built_on_device_bitwise(cuda):
+    import torch
+    for prof in (lbl.us_standard_atmosphere(), synthetic.logp_profile()):
+        li = engine.layer_input_from_profile(prof)
+        n_gas, n_lev = len(li.gases), prof.n_levels
+        p = torch.tensor(li.levels_p, device=cuda)
+        t = torch.tensor(li.levels_t, device=cuda)
+        v = torch.tensor(li.levels_vmr, device=cuda)
+        outs = [torch.empty((1, n_lev - 1), dtype=torch.float64, device=cuda) for _ in range(2)]
+        vo = [torch.empty((1, n_gas, n_lev - 1), dtype=torch.float64, device=cuda) for _ in range(2)]
+        _lib.call("lbl_build_layers", p.data_ptr(), t.data_ptr(), v.data_ptr(), 1, n_lev, n_gas, COLUMN_FACTOR,
+                  outs[0].data_ptr(), outs[1].data_ptr(), vo[0].data_ptr(), vo[1].data_ptr(),
+                  torch.cuda.current_stream().cuda_stream)
+        host = prof.build_layers()
+        assert np.array_equal(outs[0].cpu().numpy()[0], host.pressure_atm)
+        assert np.array_equal(outs[1].cpu().numpy()[0], host.temperature_k)
+        for gi, g in enumerate(li.gases):
+            assert np.array_equal(vo[0].cpu().numpy()[0, gi], host.vmr[g])
+            assert np.array_equal(vo[1].cpu().numpy()[0, gi], host.column_cm2[g])
+
+
+def test_partition_ratio_on_device_matches_np_interp(cuda):
+    import torch
+    prof = synthetic.logp_profile()
+    host = prof.build_layers()
+    tables = [synthetic.tips_power_law(174.0), synthetic.tips_power_law(3483.0, 150.0, 400.0, 2.5),
+              (np.array([200.0, 230.0, 250.0]), np.array([100.0, 150.0, 120.0]))]   # clamps both ends
+    gases = list(prof.vmr)
+    n_lay, n_grp = host.n_layers, len(tables)
+    f = lambda a, dt=torch.float64: torch.tensor(np.asarray(a), dtype=dt, device=cuda)
+    t_l, p_l = f(host.temperature_k), f(host.pressure_atm)
+    v_l = f(np.stack([host.vmr[g] for g in gases]))
+    c_l = f(np.stack([host.column_cm2[g] for g in gases]))
+    offs = np.cumsum([0] + [t.size for t, _ in tables[:-1]])
+    out = torch.empty(n_lay * n_grp * 6, dtype=torch.float64, device=cuda)
+    _lib.call("lbl_layer_groups", t_l.data_ptr(), p_l.data_ptr(), v_l.data_ptr(), c_l.data_ptr(), 1, n_lay,
+              len(gases), n_grp, f([0, 1, 2], torch.int32).data_ptr(), f([18.01, 47.98, 43.99]).data_ptr(),
+              f(offs, torch.int32).data_ptr(), f([t.size for t, _ in tables], torch.int32).data_ptr(),
+              f(np.concatenate([t for t, _ in tables])).data_ptr(),
+              f(np.concatenate([q for _, q in tables])).data_ptr(), out.data_ptr(),
+              torch.cuda.current_stream().cuda_stream)
+    lg = out.cpu().numpy().reshape(n_lay, n_grp, 6)
+    for g, (tt, qq) in enumerate(tables):
+        gas = gases[g]
+        for k in range(n_lay):
+            T, P = host.temperature_k[k], host.pressure_atm[k]
+            assert lg[k, g, 4] == np.interp(296.0, tt, qq) / np.interp(float(T), tt, qq)
+            p_self = host.vmr[gas][k] * P
+            assert lg[k, g, 1] == p_self and lg[k, g, 2] == P - p_self
+            assert lg[k, g, 3] == host.column_cm2[gas][k]
+
+
+def test_eval_count_matches_oracle(cuda):
+    sd, prof, prm, _ = golden_case("edge_mix")
+    grid = engine.make_grid(prm["nu_min"], prm["nu_max"], prm["step"], prm["tile"])
+    with warnings.catch_warnings():
+        warnings.simplefilter("ignore")
+        res = engine.optical_depth(sd, engine.layer_input_from_profile(prof), grid, prm["cutoff"],
+                                   precision="fp32", count_evals=True)
+        inp = oracle_inputs(sd, prof)
+        n = restate.count_evals(grid.nu, inp["lines"], inp["tips"], inp["masses"], inp["p_atm"],
+                                inp["t_layer"], inp["vmr_layer"], inp["col"], prm["cutoff"], prm["tile"])
+    assert res.evals == n > 0
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+def test_nonfinite_or_negative_strength_raises(cuda, precision):
+    sd, prof, prm, _ = golden_case("edge_mix")
+    lines = {k: v.copy() for k, v in sd.lines.items()}
+    co2 = np.flatnonzero((lines["mol_id"] == 2) & (lines["iso_id"] == 1) & (lines["nu0"] > 700.5))
+    lines["Sref"][co2[0]] = np.nan
+    bad = SpectralData(lines, sd.tips, sd.molar_masses)
+    with warnings.catch_warnings():
+        warnings.simplefilter("ignore")
+        with pytest.raises(FloatingPointError, match=r"^Layer 0, gas 'CO2': non-finite or negative line strength$"):
+            lbl.compute_transmittance(bad, prof, prm["nu_min"], prm["nu_max"], step_cm1=prm["step"],
+                                      line_cutoff_cm1=prm["cutoff"], tile_width_cm1=prm["tile"],
+                                      precision=precision)
+
+
+def test_missing_tips_raises_keyerror(cuda):
+    sd, prof, prm, _ = golden_case("tile2.0")
+    with pytest.raises(KeyError, match="No TIPS data"):
+        lbl.compute_transmittance(SpectralData(sd.lines, {}, sd.molar_masses), prof, 705.0, 712.0)
+
+
+def test_no_contributing_lines_gives_unit_transmittance(cuda):
+    sd = synthetic.co2_band(100, 900.0, 950.0)
+    nu, T = lbl.compute_transmittance(sd, lbl.us_standard_atmosphere(["CO2"]), 700.0, 710.0, step_cm1=0.01)
+    assert np.all(T == 1.0) and nu.size == 1001
+
+
+def test_fp32_is_deterministic(cuda):
+    sd, prof, prm, _ = golden_case("coarse_step")
+    a = _run(sd, prof, prm, "fp32", layers=True)[0]
+    b = _run(sd, prof, prm, "fp32", layers=True)[0]
+    assert np.array_equal(a.optical_depth_layers, b.optical_depth_layers)
+
+
+@pytest.mark.parametrize("seed", [1, 2, 3, 4])
+def test_random_cases_against_oracle(cuda, seed):
+    """Seeded small cases with mixed groups, odd tiles, grids and cutoffs against the oracle."""
+    rng = np.random.default_rng(seed)
+    lo = float(rng.uniform(600, 2400))
+    width = float(rng.uniform(1, 6))
+    step = float(rng.choice([0.001, 0.0025, 0.004]))
+    cutoff = float(rng.uniform(0.5, 8))
+    tile = float(rng.uniform(0.2, 3))
+    sd = synthetic.restrict(synthetic.three_gas_lines(20000, lo - cutoff - 1, lo + width + cutoff + 1,
+                                                      seed=seed), lo - cutoff - 1, lo + width + cutoff + 1)
+    lv = synthetic.logp_levels(int(rng.integers(3, 12)))
+    prof = synthetic.profile_from_levels(lv)
+    mu = float(rng.uniform(0.3, 1.0))
+    prm = dict(nu_min=lo, nu_max=lo + width, step=step, cutoff=cutoff, tile=tile, mu=mu)
+    inp = oracle_inputs(sd, prof)
+    nu = restate.grid(lo, lo + width, step)
+    od = restate.optical_depth(nu, inp["lines"], inp["tips"], inp["masses"], inp["p_atm"], inp["t_layer"],
+                               inp["vmr_layer"], inp["col"], cutoff, tile)
+    tau, T = od.sum(0), restate.transmittance(nu, od, mu)
+    for precision in ("fp64", "fp32"):
+        res, _ = _run(sd, prof, prm, precision, layers=True)
+        tol = TOL[precision]
+        assert np.max(np.abs(res.transmittance - T)) <= tol["dT"]
+        assert _rel(res.optical_depth, tau) <= tol["rtau"]
+        assert _rel(res.optical_depth_layers, od) <= tol["rod"]
+
+
+def test_full_size_three_gas_fp32_against_fp64(cuda):
+    """200k lines x 60 layers x 1.9M points: size-independent agreement of the two engines."""
+    sd = synthetic.three_gas_lines()
+    prof = synthetic.logp_profile()
+    grid = engine.make_grid(600.0, 2500.0, 0.001, 2.0)
+    li = engine.layer_input_from_profile(prof)
+    r32 = engine.optical_depth(sd, li, grid, 25.0, precision="fp32", mu=[0.8], want_od=False, want_tau=True,
+                               want_trans=True, count_evals=True)
+    r64 = engine.optical_depth(sd, li, grid, 25.0, precision="fp64", mu=[0.8], want_od=False, want_tau=True,
+                               want_trans=True, count_evals=True)
+    assert r32.evals == r64.evals > 6e11
+    t32, t64 = r32.tau[0].cpu().numpy(), r64.tau[0].cpu().numpy()
+    assert np.all(t64 > 0) and _rel(t32, t64) <= 2e-5
+    assert np.max(np.abs(r32.trans[0].cpu().numpy() - r64.trans[0].cpu().numpy())) <= 1e-5
