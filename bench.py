@@ -48,6 +48,8 @@ def parse():
     ap.add_argument("--precision", default="fp32", choices=["fp32", "fp64"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--nu-min", type=float, default=600.0, help="grid start (smaller cases for profiling)")
+    ap.add_argument("--nu-max", type=float, default=2500.0, help="grid end (smaller cases for profiling)")
     return ap.parse_args()
 
 
@@ -231,7 +233,7 @@ def main():
     from pylblrtm_b200 import engine
 
     sd, prof = workload(rank)
-    grid = engine.make_grid(600.0, 2500.0, 0.001, 2.0)
+    grid = engine.make_grid(a.nu_min, a.nu_max, 0.001, 2.0)
     job = engine.Job(sd, engine.layer_input_from_profile(prof), grid, 25.0)
     # evaluation count of one spectrum (the reference tile rule), from the kernel's own counter
     r0 = job.run(a.precision, mu=[0.8], want_od=False, want_trans=True, count_evals=True)
@@ -269,11 +271,11 @@ def main():
     if not a.no_e2e:
         pin = {k: torch.from_numpy(np.ascontiguousarray(v)).pin_memory().numpy() for k, v in sd.lines.items()}
         sd_pin = lbl.SpectralData(pin, sd.tips, sd.molar_masses, sd.molecule)
-        lbl.compute_transmittance(sd_pin, prof, 600.0, 2500.0, mu_view=0.8)
+        lbl.compute_transmittance(sd_pin, prof, a.nu_min, a.nu_max, mu_view=0.8)
         barrier()
         t0 = time.perf_counter()
         for _ in range(a.steps):
-            nu, T = lbl.compute_transmittance(sd_pin, prof, 600.0, 2500.0, mu_view=0.8)
+            nu, T = lbl.compute_transmittance(sd_pin, prof, a.nu_min, a.nu_max, mu_view=0.8)
         barrier()
         e2e_s = time.perf_counter() - t0
         if world > 1:
@@ -305,7 +307,8 @@ def main():
         "dtype": "f32" if a.precision == "fp32" else "f64", "data": "synthetic",
         "spectra_per_s": a.steps * world / (ms * 1e-3),
         "evals_per_spectrum": evals_per_step,
-        "config": {"workload": WORKLOAD, "precision": a.precision, "lines": 200000, "layers": 60,
+        "config": {"workload": WORKLOAD if (a.nu_min, a.nu_max) == (600.0, 2500.0)
+                   else f"{WORKLOAD} restricted to grid {a.nu_min}-{a.nu_max} cm^-1", "precision": a.precision, "lines": 200000, "layers": 60,
                    "grid_points": grid.n_nu, "parallelism": f"replicas{world}" if world > 1 else "single",
                    "l2": "inputs and outputs larger than L2 (line records 384 MB, od 456 MB)"},
         "roofline": {"bound": "fp32", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",

@@ -108,12 +108,14 @@ def test_partition_ratio_on_device_matches_np_interp(cuda):
     c_l = f(np.stack([host.column_cm2[g] for g in gases]))
     offs = np.cumsum([0] + [t.size for t, _ in tables[:-1]])
     out = torch.empty(n_lay * n_grp * 6, dtype=torch.float64, device=cuda)
+    # every argument tensor stays referenced until the kernel has run
+    args = [f([0, 1, 2], torch.int32), f([18.01, 47.98, 43.99]), f(offs, torch.int32),
+            f([t.size for t, _ in tables], torch.int32), f(np.concatenate([t for t, _ in tables])),
+            f(np.concatenate([q for _, q in tables]))]
     _lib.call("lbl_layer_groups", t_l.data_ptr(), p_l.data_ptr(), v_l.data_ptr(), c_l.data_ptr(), 1, n_lay,
-              len(gases), n_grp, f([0, 1, 2], torch.int32).data_ptr(), f([18.01, 47.98, 43.99]).data_ptr(),
-              f(offs, torch.int32).data_ptr(), f([t.size for t, _ in tables], torch.int32).data_ptr(),
-              f(np.concatenate([t for t, _ in tables])).data_ptr(),
-              f(np.concatenate([q for _, q in tables])).data_ptr(), out.data_ptr(),
+              len(gases), n_grp, *[a.data_ptr() for a in args], out.data_ptr(),
               torch.cuda.current_stream().cuda_stream)
+    torch.cuda.synchronize()
     lg = out.cpu().numpy().reshape(n_lay, n_grp, 6)
     for g, (tt, qq) in enumerate(tables):
         gas = gases[g]
