@@ -91,6 +91,21 @@ int lbl_sort_lines(const double* nu0, const double* shift, const int* gid, int n
                    double mask_hi, double p_max, void* workspace, size_t workspace_bytes, int* order,
                    int* n_kept, double* max_shift_bound, void* stream);
 
+/* Same as lbl_sort_lines without caller-provided workspace, for callers that
+ * cannot allocate device memory when they run (for example a host application
+ * whose memory pool owns the whole GPU and forbids further cudaMalloc calls).
+ * No counterpart in the reference. The scratch is a static device array inside
+ * the library (3 MiB on every GPU that loads it, held until the process exits),
+ * so n_lines may not exceed 262,144 (LBL_EINVAL otherwise). The first call on a
+ * device looks up the array's device address (cudaGetSymbolAddress) with that
+ * device current; make that first call before any stream capture. All calls
+ * share the one array: calls that overlap on the GPU (different streams, or
+ * threads on one device) race and must be serialised by the caller. Allocates
+ * nothing; same outputs as lbl_sort_lines. */
+int lbl_sort_lines_noalloc(const double* nu0, const double* shift, const int* gid, int n_lines, double mask_lo,
+                           double mask_hi, double p_max, int* order, int* n_kept, double* max_shift_bound,
+                           void* stream);
+
 /* Gathers the sorted lines into LineIn records (out[0 .. *n_kept)). */
 int lbl_gather_lines(const double* nu0, const double* sref, const double* g_air, const double* g_self,
                      const double* elow, const double* n_air, const double* shift, const int* gid,

@@ -35,6 +35,7 @@ SIGNATURES = {
     "lbl_layer_groups": (_I, [_P, _P, _P, _P, _I, _I, _I, _I, _P, _P, _P, _P, _P, _P, _P, _P]),
     "lbl_sort_workspace_bytes": (_S, [_I]),
     "lbl_sort_lines": (_I, [_P, _P, _P, _I, _D, _D, _D, _P, _S, _P, _P, _P, _P]),
+    "lbl_sort_lines_noalloc": (_I, [_P, _P, _P, _I, _D, _D, _D, _P, _P, _P, _P]),
     "lbl_gather_lines": (_I, [_P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _I, _P, _P]),
     "lbl_tile_ranges": (_I, [_P, _P, _D, _D, _L, _I, _D, _D, _I, _P, _P]),
     "lbl_line_prep_f64": (_I, [_P, _P, _I, _P, _I, _I, _P, _P, _P]),

@@ -405,3 +405,60 @@ extern "C" int lbl_line_prep_f32(const LineIn* lines, const int* n_kept, int n_l
                                                                nu_min, step, out, err);
   return lbl_check_launch("lbl_line_prep_f32");
 }
+
+// ---------------------------------------------------------------------------
+// Allocation-free variant of lbl_sort_lines.
+//
+// Some callers cannot allocate device memory at the time they sort lines: host
+// programs that hand all GPU memory to their own pool or allocator at start-up
+// and forbid later cudaMalloc calls, or plugins running inside such a host. For
+// them the sort scratch (keys and values of the bitonic sort) lives in the
+// static array below, which every GPU that loads this library holds until the
+// process exits.
+constexpr int NOALLOC_MAX_LINES = 1 << 18;                                   // 262,144 lines
+constexpr size_t NOALLOC_SCRATCH_BYTES = (size_t)NOALLOC_MAX_LINES * (sizeof(double) + sizeof(int));  // 3 MiB
+static __device__ __align__(256) unsigned char g_sort_scratch[NOALLOC_SCRATCH_BYTES];
+
+#include <mutex>
+static std::mutex g_scratch_mutex;
+constexpr int NOALLOC_MAX_DEVICES = 64;
+static void* g_scratch_addr[NOALLOC_MAX_DEVICES] = {};
+
+// Device address of g_sort_scratch on the current device. The name is only a
+// host-side stand-in; the real address comes from cudaGetSymbolAddress, queried
+// once per device with that device current and then cached.
+static int sort_scratch_address(void** out) {
+  int dev = -1;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return lbl_set_error(LBL_ECUDA, "lbl_sort_lines_noalloc: %s", cudaGetErrorString(e));
+  if (dev < 0 || dev >= NOALLOC_MAX_DEVICES)
+    return lbl_set_error(LBL_EINVAL, "lbl_sort_lines_noalloc: device %d out of range", dev);
+  std::lock_guard<std::mutex> lock(g_scratch_mutex);
+  if (!g_scratch_addr[dev]) {
+    void* p = nullptr;
+    e = cudaGetSymbolAddress(&p, g_sort_scratch);
+    if (e != cudaSuccess || !p)
+      return lbl_set_error(LBL_ECUDA, "lbl_sort_lines_noalloc: cudaGetSymbolAddress failed: %s",
+                           cudaGetErrorString(e));
+    g_scratch_addr[dev] = p;
+  }
+  *out = g_scratch_addr[dev];
+  return LBL_OK;
+}
+
+extern "C" int lbl_sort_lines_noalloc(const double* nu0, const double* shift, const int* gid, int n_lines,
+                                      double mask_lo, double mask_hi, double p_max, int* order, int* n_kept,
+                                      double* max_shift_bound, void* stream) {
+  if (n_lines > NOALLOC_MAX_LINES)
+    return lbl_set_error(LBL_EINVAL,
+                         "lbl_sort_lines_noalloc: %d lines exceed the static scratch limit of %d lines; "
+                         "use lbl_sort_lines with caller-provided workspace",
+                         n_lines, NOALLOC_MAX_LINES);
+  void* scratch = nullptr;
+  const int st = sort_scratch_address(&scratch);
+  if (st != LBL_OK) return st;
+  // Every entry of the scratch that the sort reads is written first by
+  // sort_keys_kernel, so the previous call's contents never leak into this one.
+  return lbl_sort_lines(nu0, shift, gid, n_lines, mask_lo, mask_hi, p_max, scratch, NOALLOC_SCRATCH_BYTES,
+                        order, n_kept, max_shift_bound, stream);
+}
