@@ -7,7 +7,7 @@ Workload: 200,000 synthetic lines (H2O-, CO2-, O3-like, 50/30/20) over
 reference tiles, mu = 0.8. A step is one full spectrum: every device stage from
 levels and line parameters resident in HBM to the transmittance in HBM.
 
-    python bench.py [--gpus N] [--steps K] [--warmup W] [--precision fp32|fp64]
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--precision fp32|fp32-direct|fp64]
     python bench.py --impl reference     # the reference's CPU path on this host
 
 Under torchrun each rank computes its own spectrum (rank r uses a profile with
@@ -35,7 +35,7 @@ sys.path.insert(0, ROOT)
 METRIC = "Voigt line-evals/s"
 UNIT = "line-evals/s"
 WORKLOAD = "three_gas_200k_lines_60_layers_600-2500cm-1_step0.001_cutoff25_tile2_mu0.8"
-FLOPS_PER_EVAL_FAR = 12      # far-wing branch of tau_f32_kernel: 5 FFMA + 1 FMUL + 1 RCP
+FLOPS_PER_EVAL_FAR = 12      # far-wing branch of the float32 kernels: 5 FFMA + 1 FMUL + 1 RCP
 CPU_SAMPLE = (1000.0, 1000.5)  # sub-window timed on the host (all 60 layers)
 
 
@@ -45,7 +45,7 @@ def parse():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--precision", default="fp32", choices=["fp32", "fp64"])
+    ap.add_argument("--precision", default="fp32", choices=["fp32", "fp32-direct", "fp64"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--nu-min", type=float, default=600.0, help="grid start (smaller cases for profiling)")
@@ -238,6 +238,7 @@ def main():
     # evaluation count of one spectrum (the reference tile rule), from the kernel's own counter
     r0 = job.run(a.precision, mu=[0.8], want_od=False, want_trans=True, count_evals=True)
     evals_per_step = r0.evals
+    work_per_step = r0.work          # Faddeeva evaluations the kernel actually performs
     launches_per_step = job.launches
 
     def barrier():
@@ -293,7 +294,7 @@ def main():
         return
     peak = fp32_peak(torch)
     tau_avg = sum(tau_ms) / len(tau_ms)
-    achieved = evals_per_step * FLOPS_PER_EVAL_FAR / (tau_avg * 1e-3) / 1e12
+    achieved = work_per_step * FLOPS_PER_EVAL_FAR / (tau_avg * 1e-3) / 1e12
     cpu = None
     if world == 1 and not a.no_cpu_baseline:
         n, dt = cpu_reference_sample(1)
@@ -304,7 +305,7 @@ def main():
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": a.steps, "warmup": a.warmup,
         "ms_per_step": ms / a.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": "f32" if a.precision == "fp32" else "f64", "data": "synthetic",
+        "dtype": "f64" if a.precision == "fp64" else "f32", "data": "synthetic",
         "spectra_per_s": a.steps * world / (ms * 1e-3),
         "evals_per_spectrum": evals_per_step,
         "config": {"workload": WORKLOAD if (a.nu_min, a.nu_max) == (600.0, 2500.0)
@@ -313,7 +314,9 @@ def main():
                    "l2": "inputs and outputs larger than L2 (line records 384 MB, od 456 MB)"},
         "roofline": {"bound": "fp32", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                      "frac": achieved / peak, "traffic": None,
-                     "kernel": "tau_f32_kernel" if a.precision == "fp32" else "tau_f64_kernel",
+                     "kernel": {"fp32": "tau_ml_kernel", "fp32-direct": "tau_f32_kernel",
+                                "fp64": "tau_f64_kernel"}[a.precision],
+                     "faddeeva_evals_per_launch": work_per_step,
                      "kernel_ms": tau_avg,
                      "peak_source": "measured live: lbl_probe_fma_f32 (MEASURED_PEAKS.json has no fp32 entry)",
                      "flops_per_eval": FLOPS_PER_EVAL_FAR},

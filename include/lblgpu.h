@@ -140,6 +140,17 @@ int lbl_tau_tiles_f32(const LineF32* prep, int n_lines, const int* ranges, const
                       double nu_min, double step, long long n_nu, int tile_samples, double cutoff, int n_grp,
                       float* od, int* err, unsigned long long* evals, void* stream);
 
+/* Same contract as lbl_tau_tiles_f32, multi-level float32 summation (the
+ * default float32 engine): per CTA chunk (<= 2048 points of one reference
+ * tile), lines farther than a chunk half-width contribute through 16 Chebyshev
+ * nodes over the chunk, the remaining lines farther than a 256-point sub-chunk
+ * half-width through 16 nodes over that sub-chunk, the rest directly. evals
+ * counts reference-rule evaluations, work (nullable) the Faddeeva evaluations
+ * actually performed. Replaces pylblrtm/forward.py:295-315. */
+int lbl_tau_tiles_ml_f32(const LineF32* prep, int n_lines, const int* ranges, const double* t_layer, int n_rows,
+                         double nu_min, double step, long long n_nu, int tile_samples, double cutoff, int n_grp,
+                         float* od, int* err, unsigned long long* evals, unsigned long long* work, void* stream);
+
 /* Column sums over layers and transmittance exp(-tau / mu); replaces
  * pylblrtm/forward.py:151 and config.py:266-270. od: [n_prof, n_lay, n_nu]
  * (float32 or float64); trans, tau (each nullable): [n_prof, n_nu] float64;

@@ -1,0 +1,339 @@
+// Multi-level float32 Voigt summation (the default float32 engine).
+//
+// Same result contract as tau_f32_kernel (voigt.cu): od[row, p] = R(nu_p, T_row) *
+// sum over the lines admitted by the reference's tile window (forward.py:295-301)
+// of S * phi(nu_p). The sum is split by distance so that most lines are
+// evaluated at a handful of points instead of every grid point:
+//
+//  level 1  lines farther than one chunk half-width from the CTA's chunk
+//           (<= 2048 points of one reference tile): their summed profile is
+//           analytic on a Bernstein ellipse with rho >= 2 + sqrt(3) around the
+//           chunk, so it is evaluated at K1 = 16 Chebyshev nodes and interpolated
+//           (interpolation error ~rho^-16 ~ 1e-9 of the level-1 sum);
+//  level 2  the other lines farther than one sub-chunk half-width from a warp's
+//           256-point sub-chunk: 16 Chebyshev nodes per sub-chunk, same geometry;
+//  level 3  the remaining lines: direct evaluation at every point. The warp's
+//           loop is branch-free: it evaluates the two-term far-wing form with
+//           |z|^2 clamped to >= FAR_Z2, so every point inside a line's near zone
+//           receives the same constant. A per-warp near pass then walks each
+//           line's near zone with consecutive points on consecutive lanes and
+//           adds (accurate value - that constant): three-term asymptotic form,
+//           float continued fraction, or Weideman's float64 approximation in the
+//           core |z|^2 < 36.
+//
+// Inside a reference tile the set of lines is fixed, so every level-1/2 sum is
+// smooth over its interval; the window test keeps the reference's truncation.
+#include <math.h>
+
+#include "faddeeva.cuh"
+#include "lbl_common.cuh"
+#include "sum_common.cuh"
+
+namespace lbl {
+
+constexpr int ML_P = 8;                        // points per lane (level 3)
+constexpr int ML_WARP_PTS = 32 * ML_P;         // points per warp sub-chunk
+constexpr int ML_THREADS = 256;                // max threads per CTA = lines staged per round
+constexpr int ML_CHUNK = ML_THREADS * ML_P;    // max points per CTA
+constexpr int ML_K = 16;                       // Chebyshev nodes per level
+constexpr float ML_MIN_H1 = 32.f;              // smallest chunk half-width (points) using level 1
+constexpr float ML_MIN_H2 = 16.f;              // smallest sub-chunk half-width using level 2
+
+struct MlLine {
+  float4 g;   // jf (centre index relative to the chunk start), a, b, amp_far
+  float4 h;   // y, y^2, amp, hw (points within which |z|^2 < FAR_Z2; -1: never)
+};
+
+// Re w times the line amplitude at one point, any distance (fast far wing first).
+__device__ __forceinline__ float line_value(float x, const MlLine& L) {
+  const float z2 = fmaf(x, x, L.h.y);
+  if (z2 >= FAR_Z2 && L.h.x >= 0.f) {
+    const float r = rcp_approx(z2);
+    return L.g.w * r * fmaf(fmaf(-2.0f * L.h.y, r, 1.5f), r, 1.0f);
+  }
+  if (z2 >= CORE_Z2 && L.h.x >= 0.f) return L.h.z * re_w_f32_mid(x, L.h.x, L.h.y, z2);
+  return (float)((double)L.h.z * weideman_re((double)x, (double)L.h.x));
+}
+
+// Far-wing form with |z|^2 clamped to >= FAR_Z2 (the level-3 loop body).
+__device__ __forceinline__ float far_clamped(float x, float y2, float n2y2, float amp_far) {
+  const float r = rcp_approx(fmaxf(fmaf(x, x, y2), FAR_Z2));
+  return amp_far * (r * fmaf(fmaf(n2y2, r, 1.5f), r, 1.0f));
+}
+
+__device__ __forceinline__ void kahan_add(float& sum, float& comp, float v) {
+  const float yk = v - comp;
+  const float t = sum + yk;
+  comp = (t - sum) - yk;
+  sum = t;
+}
+
+// p(t) = c0/2 + sum_{k>=1} c_k T_k(t) by Clenshaw's recurrence.
+__device__ __forceinline__ float clenshaw16(const float* c, float t) {
+  float b1 = 0.f, b2 = 0.f;
+  const float t2 = 2.f * t;
+#pragma unroll
+  for (int k = ML_K - 1; k >= 1; --k) {
+    const float b0 = fmaf(t2, b1, c[k] - b2);
+    b2 = b1;
+    b1 = b0;
+  }
+  return fmaf(t, b1, 0.5f * c[0] - b2);
+}
+
+__global__ void __launch_bounds__(ML_THREADS, 2)
+tau_ml_kernel(const LineF32* __restrict__ prep, int n_lines, const int2* __restrict__ ranges,
+              const double* __restrict__ t_layer, double nu_min, double step, long long n_nu,
+              int tile_samples, int chunks_per_tile, double cutoff, int n_grp, float* __restrict__ od,
+              int* err, unsigned long long* evals, unsigned long long* work) {
+  constexpr int P = ML_P;
+  __shared__ MlLine s1[ML_THREADS];                 // level-1 lines of the round
+  __shared__ MlLine s2[ML_THREADS];                 // inner lines of the round
+  __shared__ unsigned char s_l2[ML_THREADS / 32][ML_THREADS];   // per-warp level-2 slots
+  __shared__ unsigned char s_l3[ML_THREADS / 32][ML_THREADS];   // per-warp level-3 slots
+  __shared__ int s_cnt[2][ML_THREADS / 32];
+  __shared__ float s_core[ML_CHUNK];
+  __shared__ double s_red[ML_THREADS];
+  __shared__ float s_c1[ML_K];
+  __shared__ float s_c2[ML_THREADS / 32][ML_K];
+
+  const int row = blockIdx.y;
+  const int tile = blockIdx.x / chunks_per_tile, chunk = blockIdx.x % chunks_per_tile;
+  const long long t0 = (long long)tile * tile_samples;
+  const long long t1 = min(t0 + (long long)tile_samples, n_nu);
+  const long long c0 = t0 + (long long)chunk * (blockDim.x * P);
+  if (c0 >= t1) return;
+  const int n_c = (int)(min(c0 + (long long)(blockDim.x * P), t1) - c0);
+  const double wlo = __dsub_rn(grid_nu(nu_min, step, t0), cutoff);
+  const double whi = __dadd_rn(grid_nu(nu_min, step, t1 - 1), cutoff);
+  const int2 rng = ranges[tile];
+  const LineF32* lp = prep + (long long)row * n_lines;
+
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, n_warps = blockDim.x >> 5;
+  // chunk geometry (points relative to c0)
+  const float H1 = 0.5f * (float)(n_c - 1), C1 = H1;
+  const bool use_l1 = H1 >= ML_MIN_H1;
+  // this warp's sub-chunk
+  const int w0 = warp * ML_WARP_PTS;
+  const int n_w = max(0, min(ML_WARP_PTS, n_c - w0));
+  const float H2 = 0.5f * (float)(n_w - 1), C2w = (float)w0 + H2;
+  const bool use_l2 = H2 >= ML_MIN_H2;
+  // Chebyshev node offsets owned by this thread: level 1 node (tid & 15), level 2 node (lane & 15)
+  const float xn1 = H1 * (float)cospi((2.0 * (tid & 15) + 1.0) / (2.0 * ML_K));
+  const float xn2 = H2 * (float)cospi((2.0 * (lane & 15) + 1.0) / (2.0 * ML_K));
+  const float pf = (float)(w0 + lane * P);                   // this lane's first point
+  constexpr float WHW = 0.5f * (ML_WARP_PTS - 1);
+  const float wc = (float)w0 + WHW;
+
+  for (int i = tid; i < ML_CHUNK; i += blockDim.x) s_core[i] = 0.f;
+
+  float sum[P], comp[P], acc[P];
+#pragma unroll
+  for (int m = 0; m < P; ++m) sum[m] = comp[m] = acc[m] = 0.f;
+  float sum1 = 0.f, comp1 = 0.f, sum2 = 0.f, comp2 = 0.f;
+  unsigned long long n_pass = 0, n_work = 0;
+
+  // register prefetch of the next round's line records
+  LineF32 nxt;
+  int li = rng.x + tid;
+  if (li < rng.y) nxt = lp[li];
+
+  for (int base = rng.x; base < rng.y; base += blockDim.x) {
+    const LineF32 L = nxt;
+    const bool have = base + tid < rng.y;
+    if (base + blockDim.x + tid < rng.y) nxt = lp[base + blockDim.x + tid];
+    const bool pass = have && (L.nuc >= wlo) && (L.nuc <= whi);
+    const float jf = (float)((long long)L.j0 - c0);
+    const bool lev1 = pass && use_l1 && (fabsf(jf - C1) - H1 > H1 + 1.f);
+    const bool inner = pass && !lev1;
+    const unsigned b1 = __ballot_sync(0xffffffffu, lev1), b2 = __ballot_sync(0xffffffffu, inner);
+    if (lane == 0) { s_cnt[0][warp] = __popc(b1); s_cnt[1][warp] = __popc(b2); }
+    __syncthreads();
+    int off1 = 0, off2 = 0, n1 = 0, n2 = 0;
+    for (int w = 0; w < n_warps; ++w) {
+      const int a1 = s_cnt[0][w], a2 = s_cnt[1][w];
+      off1 += (w < warp) ? a1 : 0;
+      off2 += (w < warp) ? a2 : 0;
+      n1 += a1;
+      n2 += a2;
+    }
+    if (pass) {
+      const float y2 = L.y * L.y;
+      MlLine r;
+      r.g = make_float4(lev1 ? C1 - jf : jf, L.a, L.b, L.amp_far);
+      const float hw = (y2 >= FAR_Z2 && L.y >= 0.f) ? -1.0f : sqrtf(fmaxf(FAR_Z2 - y2, 0.f)) / L.a + 1.0f;
+      r.h = make_float4(L.y, y2, L.amp, hw);
+      const unsigned lt = (1u << lane) - 1u;
+      if (lev1) s1[off1 + __popc(b1 & lt)] = r;
+      else s2[off2 + __popc(b2 & lt)] = r;
+    }
+    __syncthreads();
+    n_pass += (unsigned long long)(n1 + n2);
+
+    // ---- level 1: thread (tid & 15) evaluates its node for lines tid>>4, +16, ...
+    {
+      float a1 = 0.f;
+      const int stride = blockDim.x >> 4;
+      for (int l = tid >> 4; l < n1; l += stride) {
+        const MlLine R = s1[l];
+        const float x = fmaf(xn1 + R.g.x, R.g.y, -R.g.z);     // (node - centre) * s
+        a1 += line_value(x, R);
+      }
+      kahan_add(sum1, comp1, a1);
+      if (tid == 0) n_work += (unsigned long long)n1 * ML_K;
+    }
+
+    // ---- per-warp split of the inner lines into level 2 and level 3
+    int n2w = 0, n3w = 0;
+    for (int k = 0; k < n2; k += 32) {
+      const int l = k + lane;
+      bool is2 = false, is3 = false;
+      if (l < n2) {
+        const float d = fabsf(s2[l].g.x - C2w) - H2;
+        is2 = use_l2 && d > H2 + 1.f;
+        is3 = !is2 && n_w > 0;
+      }
+      const unsigned q2 = __ballot_sync(0xffffffffu, is2), q3 = __ballot_sync(0xffffffffu, is3);
+      const unsigned lt = (1u << lane) - 1u;
+      if (is2) s_l2[warp][n2w + __popc(q2 & lt)] = (unsigned char)l;
+      if (is3) s_l3[warp][n3w + __popc(q3 & lt)] = (unsigned char)l;
+      n2w += __popc(q2);
+      n3w += __popc(q3);
+    }
+    __syncwarp();
+
+    // ---- level 2: half-warps take one line each, lane (& 15) = node
+    {
+      float a2 = 0.f;
+      for (int i = lane >> 4; i < n2w; i += 2) {
+        const MlLine R = s2[s_l2[warp][i]];
+        const float e = C2w - R.g.x;                          // exact: half-integer minus integer
+        const float x = fmaf(xn2 + e, R.g.y, -R.g.z);
+        a2 += line_value(x, R);
+      }
+      kahan_add(sum2, comp2, a2);
+      if (lane == 0) n_work += (unsigned long long)n2w * ML_K;
+    }
+
+    // ---- level 3, far part: every point of the warp, |z|^2 clamped (branch-free)
+    for (int i = 0; i < n3w; ++i) {
+      const MlLine R = s2[s_l3[warp][i]];
+      const float x0 = fmaf(pf - R.g.x, R.g.y, -R.g.z);
+      const float n2y2 = -2.0f * R.h.y;
+#pragma unroll
+      for (int m = 0; m < P; ++m) {
+        const float x = fmaf((float)m, R.g.y, x0);
+        const float r = rcp_approx(fmaxf(fmaf(x, x, R.h.y), FAR_Z2));
+        acc[m] = fmaf(R.g.w, r * fmaf(fmaf(n2y2, r, 1.5f), r, 1.0f), acc[m]);
+      }
+    }
+    if (lane == 0) n_work += (unsigned long long)n3w * n_w;
+    // ---- level 3, near part: points with |z|^2 < FAR_Z2 get (accurate - clamped value).
+    // x is formed exactly as in the loop above, so the clamped value cancels.
+    for (int i = 0; i < n3w; ++i) {
+      const MlLine R = s2[s_l3[warp][i]];
+      if (R.h.w < 0.f) continue;                         // |z|^2 >= FAR_Z2 everywhere
+      const float q = R.g.x + R.g.z / R.g.y;             // centre in points
+      const float lo_f = fmaxf(ceilf(q - R.h.w), (float)w0);
+      const float hi_f = fminf(floorf(q + R.h.w), (float)(w0 + n_w - 1));
+      if (!(lo_f <= hi_f)) continue;
+      const int lo = (int)lo_f, hi = (int)hi_f;
+      const float n2y2 = -2.0f * R.h.y;
+      const float clamp_val = far_clamped(0.f, FAR_Z2, n2y2, R.g.w);   // value of the clamped form
+      for (int p = lo + lane; p <= hi; p += 32) {
+        const int pl = p - w0;
+        const float x0 = fmaf((float)(w0 + (pl & ~(P - 1))) - R.g.x, R.g.y, -R.g.z);
+        const float x = fmaf((float)(pl & (P - 1)), R.g.y, x0);
+        const float z2 = fmaf(x, x, R.h.y);
+        if (z2 >= FAR_Z2) continue;
+        float v;
+        if (z2 >= MID_Z2 && R.h.x >= 0.f) v = R.h.z * re_w_asym3(R.h.x, R.h.y, 1.0f / z2);
+        else if (z2 >= CORE_Z2 && R.h.x >= 0.f) v = R.h.z * re_w_cf32(x, R.h.x, z2);
+        else v = (float)((double)R.h.z * weideman_re((double)x, (double)R.h.x));
+        s_core[p] += v - clamp_val;                      // lanes hold distinct points
+      }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int m = 0; m < P; ++m) {
+      kahan_add(sum[m], comp[m], acc[m]);
+      acc[m] = 0.f;
+    }
+  }
+
+  // ---- level-1 node values: reduce the 16-thread groups, then Chebyshev coefficients
+  s_red[tid] = (double)sum1 - (double)comp1;
+  __syncthreads();
+  if (tid < ML_K) {
+    double f = 0.0;
+    for (int i = tid; i < (int)blockDim.x; i += ML_K) f += s_red[i];
+    s_red[tid] = f;      // only read back after the barrier below, by threads < ML_K
+  }
+  __syncthreads();
+  if (tid < ML_K) {
+    double c = 0.0;
+    for (int j = 0; j < ML_K; ++j) c += s_red[j] * cospi((double)tid * (2.0 * j + 1.0) / (2.0 * ML_K));
+    s_c1[tid] = use_l1 ? (float)(c * (2.0 / ML_K)) : 0.f;
+  }
+  // ---- level-2 node values of this warp: lanes j and j+16 hold halves of node j
+  {
+    float f2 = sum2 - comp2;
+    f2 += __shfl_xor_sync(0xffffffffu, f2, 16);
+    double c = 0.0;
+    for (int j = 0; j < ML_K; ++j) {
+      const float fj = __shfl_sync(0xffffffffu, f2, j);
+      c += (double)fj * cospi((double)(lane & 15) * (2.0 * j + 1.0) / (2.0 * ML_K));
+    }
+    if (lane < ML_K) s_c2[warp][lane] = use_l2 ? (float)(c * (2.0 / ML_K)) : 0.f;
+  }
+  __syncthreads();
+
+  const double T = t_layer[row];
+  float* out = od + (long long)row * n_nu;
+  float c1[ML_K], c2[ML_K];
+#pragma unroll
+  for (int k = 0; k < ML_K; ++k) { c1[k] = s_c1[k]; c2[k] = s_c2[warp][k]; }
+  const float inv_h1 = use_l1 ? 1.0f / H1 : 0.f, inv_h2 = use_l2 ? 1.0f / H2 : 0.f;
+  bool bad = false;
+#pragma unroll
+  for (int m = 0; m < P; ++m) {
+    const int pl = w0 + lane * P + m;
+    if (pl < n_c) {
+      float v = s_core[pl];
+      if (use_l1) v += clenshaw16(c1, ((float)pl - C1) * inv_h1);
+      if (use_l2) v += clenshaw16(c2, ((float)pl - C2w) * inv_h2);
+      const long long p = c0 + pl;
+      const double nu = grid_nu(nu_min, step, p);
+      const float o = (float)(((double)sum[m] - (double)comp[m] + (double)v) * radiation_term_grid(nu, T));
+      bad |= !isfinite(o);
+      out[p] = o;
+    }
+  }
+  if (bad) flag_error(err, row * (n_grp + 1) + n_grp);
+  if (tid == 0 && evals && n_pass) atomicAdd(evals, n_pass * (unsigned long long)n_c);
+  if (work && n_work) atomicAdd(work, n_work);
+}
+
+}  // namespace lbl
+
+using namespace lbl;
+
+extern "C" int lbl_tau_tiles_ml_f32(const LineF32* prep, int n_lines, const int* ranges, const double* t_layer,
+                                    int n_rows, double nu_min, double step, long long n_nu, int tile_samples,
+                                    double cutoff, int n_grp, float* od, int* err, unsigned long long* evals,
+                                    unsigned long long* work, void* stream) {
+  if (!prep || !ranges || !t_layer || !od || n_lines < 1 || n_rows < 1 || n_rows > 65535 || n_nu < 1 ||
+      tile_samples < 1 || !(step > 0) || !(cutoff >= 0) || n_grp < 1)
+    return lbl_set_error(LBL_EINVAL, "lbl_tau_tiles_ml_f32: bad arguments");
+  const int per_tile = tile_samples < ML_CHUNK ? tile_samples : ML_CHUNK;
+  const int threads = 32 * ((per_tile + ML_WARP_PTS - 1) / ML_WARP_PTS);
+  const int cp = threads * ML_P;
+  const long long n_tiles = (n_nu + tile_samples - 1) / tile_samples;
+  const long long chunks = (tile_samples + cp - 1) / cp;
+  if (n_tiles * chunks > 0x7fffffffLL) return lbl_set_error(LBL_EINVAL, "lbl_tau_tiles_ml_f32: grid too large");
+  dim3 grid((unsigned)(n_tiles * chunks), (unsigned)n_rows);
+  tau_ml_kernel<<<grid, threads, 0, (cudaStream_t)stream>>>(prep, n_lines, (const int2*)ranges, t_layer, nu_min,
+                                                             step, n_nu, tile_samples, (int)chunks, cutoff, n_grp,
+                                                             od, err, evals, work);
+  return lbl_check_launch("lbl_tau_tiles_ml_f32");
+}

@@ -33,7 +33,9 @@ from .hitran_ids import MOL_ID_TO_NAME
 from .spectral_data import SpectralData
 
 INT_MAX = 2**31 - 1
-PRECISIONS = ("fp32", "fp64")
+# "fp32": multi-level float32 summation (default); "fp32-direct": float32 summation of
+# every line at every point; "fp64": the plain float64 method.
+PRECISIONS = ("fp32", "fp32-direct", "fp64")
 
 
 def _torch():
@@ -223,6 +225,7 @@ class EngineResult:
     trans: object = None           # torch float64 [n_prof, n_nu]
     tau: object = None             # torch float64 [n_prof, n_nu]
     evals: int = 0                 # Voigt evaluations under the reference tile rule
+    work: int = 0                  # Faddeeva evaluations actually performed (multi-level engine)
     groups: List[Group] = field(default_factory=list)
 
 
@@ -313,7 +316,8 @@ class Job:
         n_prof, n_lay, n_nu = self.n_prof, self.n_lay, grid.n_nu
         n_rows = n_prof * n_lay
         res = EngineResult(groups=self.groups)
-        od_dtype = torch.float32 if precision == "fp32" else torch.float64
+        single = precision != "fp64"
+        od_dtype = torch.float32 if single else torch.float64
         self.launches = 0
 
         def finish(od):
@@ -381,11 +385,11 @@ class Job:
         self.launches += 2
         # per (layer, line) prep and the Voigt sums
         err = torch.full((1,), INT_MAX, dtype=torch.int32, device=dev)
-        evals = torch.zeros(1, dtype=torch.int64, device=dev) if count_evals else None
+        evals = torch.zeros(2, dtype=torch.int64, device=dev) if count_evals else None
         od = torch.empty((n_prof, n_lay, n_nu), dtype=od_dtype, device=dev)
-        rec = _lib.SIZEOF_LINE_F32 if precision == "fp32" else _lib.SIZEOF_LINE_F64
+        rec = _lib.SIZEOF_LINE_F32 if single else _lib.SIZEOF_LINE_F64
         prep = torch.empty((n_rows * n_kept * rec // 8,), dtype=torch.float64, device=dev)
-        if precision == "fp32":
+        if single:
             _lib.call("lbl_line_prep_f32", lines.data_ptr(), kept.data_ptr(), n_kept, lg.data_ptr(), n_rows, n_grp,
                       grid.nu_min, grid.step, prep.data_ptr(), err.data_ptr(), stream)
         else:
@@ -394,9 +398,13 @@ class Job:
         if timer is not None:
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             e0.record()
-        _lib.call("lbl_tau_tiles_f32" if precision == "fp32" else "lbl_tau_tiles_f64", prep.data_ptr(), n_kept,
-                  ranges.data_ptr(), t_lay.data_ptr(), n_rows, grid.nu_min, grid.step, n_nu, grid.tile_samples,
-                  self.cutoff, n_grp, od.data_ptr(), err.data_ptr(), _lib.ptr(evals), stream)
+        common = (prep.data_ptr(), n_kept, ranges.data_ptr(), t_lay.data_ptr(), n_rows, grid.nu_min, grid.step,
+                  n_nu, grid.tile_samples, self.cutoff, n_grp, od.data_ptr(), err.data_ptr(), _lib.ptr(evals))
+        if precision == "fp32":
+            _lib.call("lbl_tau_tiles_ml_f32", *common,
+                      0 if evals is None else evals.data_ptr() + 8, stream)
+        else:
+            _lib.call("lbl_tau_tiles_f32" if single else "lbl_tau_tiles_f64", *common, stream)
         if timer is not None:
             e1.record()
             timer.setdefault("tau_events", []).append((e0, e1))
@@ -410,7 +418,9 @@ class Job:
                     f"Layer {k}, gas '{self.groups[g].gas}': non-finite or negative line strength")
             raise FloatingPointError(f"Layer {k}: non-finite optical depth after radiation term")
         if evals is not None:
-            res.evals = int(evals.item())
+            ev = evals.cpu().tolist()
+            res.evals = int(ev[0])
+            res.work = int(ev[1]) if precision == "fp32" else int(ev[0])
         return finish(od)
 
 

@@ -19,7 +19,8 @@ from pylblrtm_b200.spectral_data import SpectralData
 
 pytestmark = pytest.mark.gpu
 
-TOL = {"fp64": dict(dT=1e-6, rtau=1e-9, rod=1e-9), "fp32": dict(dT=1e-5, rtau=2e-5, rod=3e-5)}
+TOL = {"fp64": dict(dT=1e-6, rtau=1e-9, rod=1e-9), "fp32": dict(dT=1e-5, rtau=2e-5, rod=3e-5),
+       "fp32-direct": dict(dT=1e-5, rtau=2e-5, rod=3e-5)}
 
 
 def _run(sd, prof, prm, precision, layers=False):
@@ -40,7 +41,7 @@ def _rel(a, b):
     return float(np.max(np.abs(a - b)[m] / den[m])) if m.any() else 0.0
 
 
-@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+@pytest.mark.parametrize("precision", ["fp64", "fp32", "fp32-direct"])
 @pytest.mark.parametrize("name", ALL_GOLDEN)
 def test_golden(cuda, name, precision):
     sd, prof, prm, data = golden_case(name)
@@ -140,7 +141,7 @@ def test_eval_count_matches_oracle(cuda):
     assert res.evals == n > 0
 
 
-@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+@pytest.mark.parametrize("precision", ["fp64", "fp32", "fp32-direct"])
 def test_nonfinite_or_negative_strength_raises(cuda, precision):
     sd, prof, prm, _ = golden_case("edge_mix")
     lines = {k: v.copy() for k, v in sd.lines.items()}
@@ -194,7 +195,7 @@ def test_random_cases_against_oracle(cuda, seed):
     od = restate.optical_depth(nu, inp["lines"], inp["tips"], inp["masses"], inp["p_atm"], inp["t_layer"],
                                inp["vmr_layer"], inp["col"], cutoff, tile)
     tau, T = od.sum(0), restate.transmittance(nu, od, mu)
-    for precision in ("fp64", "fp32"):
+    for precision in ("fp64", "fp32", "fp32-direct"):
         res, _ = _run(sd, prof, prm, precision, layers=True)
         tol = TOL[precision]
         assert np.max(np.abs(res.transmittance - T)) <= tol["dT"]
@@ -203,16 +204,20 @@ def test_random_cases_against_oracle(cuda, seed):
 
 
 def test_full_size_three_gas_fp32_against_fp64(cuda):
-    """200k lines x 60 layers x 1.9M points: size-independent agreement of the two engines."""
+    """200k lines x 60 layers x 1.9M points: size-independent agreement of the engines."""
     sd = synthetic.three_gas_lines()
     prof = synthetic.logp_profile()
     grid = engine.make_grid(600.0, 2500.0, 0.001, 2.0)
     li = engine.layer_input_from_profile(prof)
-    r32 = engine.optical_depth(sd, li, grid, 25.0, precision="fp32", mu=[0.8], want_od=False, want_tau=True,
-                               want_trans=True, count_evals=True)
-    r64 = engine.optical_depth(sd, li, grid, 25.0, precision="fp64", mu=[0.8], want_od=False, want_tau=True,
-                               want_trans=True, count_evals=True)
-    assert r32.evals == r64.evals > 6e11
-    t32, t64 = r32.tau[0].cpu().numpy(), r64.tau[0].cpu().numpy()
-    assert np.all(t64 > 0) and _rel(t32, t64) <= 2e-5
-    assert np.max(np.abs(r32.trans[0].cpu().numpy() - r64.trans[0].cpu().numpy())) <= 1e-5
+    r = {p: engine.optical_depth(sd, li, grid, 25.0, precision=p, mu=[0.8], want_od=True, want_tau=True,
+                                 want_trans=True, count_evals=True) for p in ("fp64", "fp32", "fp32-direct")}
+    assert r["fp32"].evals == r["fp32-direct"].evals == r["fp64"].evals > 6e11
+    assert r["fp32"].work < r["fp32"].evals / 20          # the multi-level split does far fewer evaluations
+    t64 = r["fp64"].tau[0].cpu().numpy()
+    od64 = r["fp64"].od[0]
+    assert np.all(t64 > 0)
+    for p in ("fp32", "fp32-direct"):
+        assert _rel(r[p].tau[0].cpu().numpy(), t64) <= 2e-5
+        assert np.max(np.abs(r[p].trans[0].cpu().numpy() - r["fp64"].trans[0].cpu().numpy())) <= 1e-5
+        rel_od = ((r[p].od[0].double() - od64).abs() / od64.abs()).max().item()
+        assert rel_od <= 3e-5, (p, rel_od)
