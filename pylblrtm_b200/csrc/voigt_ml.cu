@@ -91,7 +91,9 @@ tau_ml_kernel(const LineF32* __restrict__ prep, int n_lines, const int2* __restr
   __shared__ MlLine s2[ML_THREADS];                 // inner lines of the round
   __shared__ unsigned char s_l2[ML_THREADS / 32][ML_THREADS];   // per-warp level-2 slots
   __shared__ unsigned char s_l3[ML_THREADS / 32][ML_THREADS];   // per-warp level-3 slots
-  __shared__ int s_cnt[2][ML_THREADS / 32];
+  __shared__ int s_cnt[3][ML_THREADS / 32];
+  __shared__ int s_seg_start[ML_THREADS + 1];       // near-item prefix per inner slot
+  __shared__ short s_seg_lo[ML_THREADS];            // first near point per inner slot
   __shared__ float s_core[ML_CHUNK];
   __shared__ double s_red[ML_THREADS];
   __shared__ float s_c1[ML_K];
@@ -127,9 +129,11 @@ tau_ml_kernel(const LineF32* __restrict__ prep, int n_lines, const int2* __restr
 
   for (int i = tid; i < ML_CHUNK; i += blockDim.x) s_core[i] = 0.f;
 
-  float sum[P], comp[P], acc[P];
+  // level-3 sums hold only the lines within ~2 sub-chunk widths (tens of terms), so
+  // plain float accumulation suffices; the long node sums use Kahan compensation.
+  float acc[P];
 #pragma unroll
-  for (int m = 0; m < P; ++m) sum[m] = comp[m] = acc[m] = 0.f;
+  for (int m = 0; m < P; ++m) acc[m] = 0.f;
   float sum1 = 0.f, comp1 = 0.f, sum2 = 0.f, comp2 = 0.f;
   unsigned long long n_pass = 0, n_work = 0;
 
@@ -146,27 +150,54 @@ tau_ml_kernel(const LineF32* __restrict__ prep, int n_lines, const int2* __restr
     const float jf = (float)((long long)L.j0 - c0);
     const bool lev1 = pass && use_l1 && (fabsf(jf - C1) - H1 > H1 + 1.f);
     const bool inner = pass && !lev1;
+    // near range (points with possibly |z|^2 < FAR_Z2) of an inner line, clipped to the chunk
+    const float y2 = L.y * L.y;
+    const float hw = (y2 >= FAR_Z2 && L.y >= 0.f) ? -1.0f : sqrtf(fmaxf(FAR_Z2 - y2, 0.f)) / L.a + 1.0f;
+    int near_lo = 0, near_n = 0;
+    if (inner && hw >= 0.f) {
+      const float q = jf + L.b / L.a;                       // centre in points
+      const float lo_f = fmaxf(ceilf(q - hw), 0.f);
+      const float hi_f = fminf(floorf(q + hw), (float)(n_c - 1));
+      if (lo_f <= hi_f) {
+        near_lo = (int)lo_f;
+        near_n = (int)hi_f - near_lo + 1;
+      }
+    }
+    int near_scan = near_n;                                  // inclusive warp scan
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int t = __shfl_up_sync(0xffffffffu, near_scan, o);
+      if (lane >= o) near_scan += t;
+    }
     const unsigned b1 = __ballot_sync(0xffffffffu, lev1), b2 = __ballot_sync(0xffffffffu, inner);
     if (lane == 0) { s_cnt[0][warp] = __popc(b1); s_cnt[1][warp] = __popc(b2); }
+    if (lane == 31) s_cnt[2][warp] = near_scan;
     __syncthreads();
-    int off1 = 0, off2 = 0, n1 = 0, n2 = 0;
+    int off1 = 0, off2 = 0, off3 = 0, n1 = 0, n2 = 0, n_near = 0;
     for (int w = 0; w < n_warps; ++w) {
-      const int a1 = s_cnt[0][w], a2 = s_cnt[1][w];
+      const int a1 = s_cnt[0][w], a2 = s_cnt[1][w], a3 = s_cnt[2][w];
       off1 += (w < warp) ? a1 : 0;
       off2 += (w < warp) ? a2 : 0;
+      off3 += (w < warp) ? a3 : 0;
       n1 += a1;
       n2 += a2;
+      n_near += a3;
     }
     if (pass) {
-      const float y2 = L.y * L.y;
       MlLine r;
       r.g = make_float4(lev1 ? C1 - jf : jf, L.a, L.b, L.amp_far);
-      const float hw = (y2 >= FAR_Z2 && L.y >= 0.f) ? -1.0f : sqrtf(fmaxf(FAR_Z2 - y2, 0.f)) / L.a + 1.0f;
       r.h = make_float4(L.y, y2, L.amp, hw);
       const unsigned lt = (1u << lane) - 1u;
-      if (lev1) s1[off1 + __popc(b1 & lt)] = r;
-      else s2[off2 + __popc(b2 & lt)] = r;
+      if (lev1) {
+        s1[off1 + __popc(b1 & lt)] = r;
+      } else {
+        const int slot = off2 + __popc(b2 & lt);
+        s2[slot] = r;
+        s_seg_start[slot] = off3 + near_scan - near_n;       // exclusive prefix in slot order
+        s_seg_lo[slot] = (short)near_lo;
+      }
     }
+    if (tid == 0) s_seg_start[n2] = n_near;
     __syncthreads();
     n_pass += (unsigned long long)(n1 + n2);
 
@@ -228,37 +259,35 @@ tau_ml_kernel(const LineF32* __restrict__ prep, int n_lines, const int2* __restr
       }
     }
     if (lane == 0) n_work += (unsigned long long)n3w * n_w;
-    // ---- level 3, near part: points with |z|^2 < FAR_Z2 get (accurate - clamped value).
-    // x is formed exactly as in the loop above, so the clamped value cancels.
-    for (int i = 0; i < n3w; ++i) {
-      const MlLine R = s2[s_l3[warp][i]];
-      if (R.h.w < 0.f) continue;                         // |z|^2 >= FAR_Z2 everywhere
-      const float q = R.g.x + R.g.z / R.g.y;             // centre in points
-      const float lo_f = fmaxf(ceilf(q - R.h.w), (float)w0);
-      const float hi_f = fminf(floorf(q + R.h.w), (float)(w0 + n_w - 1));
-      if (!(lo_f <= hi_f)) continue;
-      const int lo = (int)lo_f, hi = (int)hi_f;
-      const float n2y2 = -2.0f * R.h.y;
-      const float clamp_val = far_clamped(0.f, FAR_Z2, n2y2, R.g.w);   // value of the clamped form
-      for (int p = lo + lane; p <= hi; p += 32) {
-        const int pl = p - w0;
-        const float x0 = fmaf((float)(w0 + (pl & ~(P - 1))) - R.g.x, R.g.y, -R.g.z);
-        const float x = fmaf((float)(pl & (P - 1)), R.g.y, x0);
+    // ---- level 3, near part, spread over the CTA: near item i is point
+    // s_seg_lo[l] + (i - s_seg_start[l]) of inner line l. It gets (accurate value -
+    // clamped far-loop value) if the line is level 3 for the warp owning the point
+    // and |z|^2 < FAR_Z2 there; x is formed exactly as in the far loop, so the
+    // clamped value cancels. Consecutive threads take consecutive points of a line.
+    {
+      int l = 0;
+      for (int i = tid; i < n_near; i += blockDim.x) {
+        while (s_seg_start[l + 1] <= i) ++l;
+        const int p = s_seg_lo[l] + (i - s_seg_start[l]);
+        const MlLine R = s2[l];
+        const int wp = p >> 8;                                  // warp owning point p
+        const int nwp = min(ML_WARP_PTS, n_c - wp * ML_WARP_PTS);
+        const float h2p = 0.5f * (float)(nwp - 1);
+        if (h2p >= ML_MIN_H2 && fabsf(R.g.x - ((float)(wp * ML_WARP_PTS) + h2p)) - h2p > h2p + 1.f) continue;
+        const float x0 = fmaf((float)(p & ~(P - 1)) - R.g.x, R.g.y, -R.g.z);
+        const float x = fmaf((float)(p & (P - 1)), R.g.y, x0);
         const float z2 = fmaf(x, x, R.h.y);
         if (z2 >= FAR_Z2) continue;
         float v;
         if (z2 >= MID_Z2 && R.h.x >= 0.f) v = R.h.z * re_w_asym3(R.h.x, R.h.y, 1.0f / z2);
         else if (z2 >= CORE_Z2 && R.h.x >= 0.f) v = R.h.z * re_w_cf32(x, R.h.x, z2);
         else v = (float)((double)R.h.z * weideman_re((double)x, (double)R.h.x));
-        s_core[p] += v - clamp_val;                      // lanes hold distinct points
+        const float clamp_val = far_clamped(0.f, FAR_Z2, -2.0f * R.h.y, R.g.w);
+        atomicAdd(&s_core[p], v - clamp_val);
       }
+      if (tid == 0) n_work += (unsigned long long)n_near;
     }
     __syncthreads();
-#pragma unroll
-    for (int m = 0; m < P; ++m) {
-      kahan_add(sum[m], comp[m], acc[m]);
-      acc[m] = 0.f;
-    }
   }
 
   // ---- level-1 node values: reduce the 16-thread groups, then Chebyshev coefficients
@@ -304,7 +333,7 @@ tau_ml_kernel(const LineF32* __restrict__ prep, int n_lines, const int2* __restr
       if (use_l2) v += clenshaw16(c2, ((float)pl - C2w) * inv_h2);
       const long long p = c0 + pl;
       const double nu = grid_nu(nu_min, step, p);
-      const float o = (float)(((double)sum[m] - (double)comp[m] + (double)v) * radiation_term_grid(nu, T));
+      const float o = (float)(((double)acc[m] + (double)v) * radiation_term_grid(nu, T));
       bad |= !isfinite(o);
       out[p] = o;
     }
