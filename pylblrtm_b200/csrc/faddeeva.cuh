@@ -210,8 +210,8 @@ LBL_HD double weideman_re(double x, double y) {
 // approximation): inside it a float complex evaluation loses relative accuracy
 // in the real part for small y.
 constexpr float CORE_Z2 = 36.0f;
-// |z|^2 above which three asymptotic terms suffice (relative error <= 4e-7).
-constexpr float MID_Z2 = 400.0f;
+// |z|^2 above which five asymptotic terms suffice (relative error <= 4e-7).
+constexpr float MID_Z2 = 64.0f;
 
 // Re w by the asymptotic series, two terms: (y/sqrt(pi)) r (1 + 1.5 r - 2 y^2 r^2)
 // with r = 1/|z|^2 (valid for |z|^2 >= FAR_Z2).
@@ -219,13 +219,31 @@ LBL_HD float re_w_asym2(float y, float y2, float r) {
   return float(INV_SQRT_PI) * y * r * (1.0f + r * (1.5f - 2.0f * y2 * r));
 }
 
-// Re w by the asymptotic series, three terms (valid for |z|^2 >= MID_Z2):
-// (y/sqrt(pi)) r (1 + r (1.5 - 2q + r (3.75 - 15 q + 12 q^2))), q = y^2 r.
-LBL_HD float re_w_asym3(float y, float y2, float r) {
+// Bracket S of the five-term asymptotic real part, Re w = (y/sqrt(pi)) r S, with
+// r = 1/|z|^2 and q = y^2 r (valid for |z|^2 >= MID_Z2). Term k of
+// (i/sqrt(pi)) sum (2k-1)!!/2^k z^-(2k+1) contributes r^k A_k(q) with
+//   A_1 = 1.5 - 2q, A_2 = 3.75 - 15q + 12q^2, A_3 = 13.125 - 105q + 210q^2 - 120q^3,
+//   A_4 = 59.0625 - 787.5q + 2835q^2 - 3780q^3 + 1680q^4
+// (from Im z^(2k+1) / |z|^(4k+2) written in |z|^2 and y^2).
+LBL_HD float asym5_bracket(float y2, float r) {
   const float q = y2 * r;
-  const float inner = (12.0f * q - 15.0f) * q + 3.75f;
-  const float t = r * inner + (1.5f - 2.0f * q);
-  return float(INV_SQRT_PI) * y * r * (1.0f + r * t);
+  const float a4 = (((1680.0f * q - 3780.0f) * q + 2835.0f) * q - 787.5f) * q + 59.0625f;
+  const float a3 = ((-120.0f * q + 210.0f) * q - 105.0f) * q + 13.125f;
+  const float a2 = (12.0f * q - 15.0f) * q + 3.75f;
+  const float a1 = 1.5f - 2.0f * q;
+  return 1.0f + r * (a1 + r * (a2 + r * (a3 + r * a4)));
+}
+
+LBL_HD float re_w_asym5(float y, float y2, float r) {
+  return float(INV_SQRT_PI) * y * r * asym5_bracket(y2, r);
+}
+
+LBL_HD float approx_div(float a, float b) {
+#ifdef __CUDA_ARCH__
+  return __fdividef(a, b);
+#else
+  return a / b;
+#endif
 }
 
 // Re w by the Laplace continued fraction in float (valid for |z|^2 >= CORE_Z2,
@@ -236,7 +254,7 @@ LBL_HD float re_w_cf32(float x, float y, float z2) {
   for (int n = depth - 1; n >= 0; --n) {
     const float cr = y + float(n + 1) * rr;
     const float ci = -x + float(n + 1) * ri;
-    const float inv = 0.5f / (cr * cr + ci * ci);
+    const float inv = approx_div(0.5f, cr * cr + ci * ci);
     rr = cr * inv;
     ri = -ci * inv;
   }
@@ -253,7 +271,7 @@ LBL_HD float faddeeva_re_f32(float x, float y) {
   const float z2 = x * x + y2;
   if (y < 0.0f || z2 < CORE_Z2) return (float)weideman_re((double)x, (double)y);
   if (z2 >= FAR_Z2) return re_w_asym2(y, y2, 1.0f / z2);
-  if (z2 >= MID_Z2) return re_w_asym3(y, y2, 1.0f / z2);
+  if (z2 >= MID_Z2) return re_w_asym5(y, y2, 1.0f / z2);
   return re_w_cf32(x, y, z2);
 }
 

@@ -47,7 +47,7 @@ __device__ __forceinline__ int stage_round(const Rec* __restrict__ lp, int li, i
 }
 
 static __device__ __noinline__ float re_w_f32_mid(float x, float y, float y2, float z2) {
-  if (z2 >= MID_Z2) return re_w_asym3(y, y2, 1.0f / z2);
+  if (z2 >= MID_Z2) return re_w_asym5(y, y2, 1.0f / z2);
   return re_w_cf32(x, y, z2);
 }
 

@@ -41,7 +41,7 @@ constexpr float ML_MIN_H2 = 16.f;              // smallest sub-chunk half-width 
 
 struct MlLine {
   float4 g;   // jf (centre index relative to the chunk start), a, b, amp_far
-  float4 h;   // y, y^2, amp, hw (points within which |z|^2 < FAR_Z2; -1: never)
+  float4 h;   // y, y^2, amp, value the clamped far-wing loop adds inside the near zone
 };
 
 // Re w times the line amplitude at one point, any distance (fast far wing first).
@@ -94,6 +94,7 @@ tau_ml_kernel(const LineF32* __restrict__ prep, int n_lines, const int2* __restr
   __shared__ int s_cnt[3][ML_THREADS / 32];
   __shared__ int s_seg_start[ML_THREADS + 1];       // near-item prefix per inner slot
   __shared__ short s_seg_lo[ML_THREADS];            // first near point per inner slot
+  __shared__ unsigned char s_seg_mask[ML_THREADS];  // warps treating the inner line directly (level 3)
   __shared__ float s_core[ML_CHUNK];
   __shared__ double s_red[ML_THREADS];
   __shared__ float s_c1[ML_K];
@@ -154,7 +155,17 @@ tau_ml_kernel(const LineF32* __restrict__ prep, int n_lines, const int2* __restr
     const float y2 = L.y * L.y;
     const float hw = (y2 >= FAR_Z2 && L.y >= 0.f) ? -1.0f : sqrtf(fmaxf(FAR_Z2 - y2, 0.f)) / L.a + 1.0f;
     int near_lo = 0, near_n = 0;
-    if (inner && hw >= 0.f) {
+    unsigned l3mask = 0;
+    if (inner) {
+      for (int w = 0; w < n_warps; ++w) {             // same test as the per-warp split below
+        const int nw = min(ML_WARP_PTS, n_c - w * ML_WARP_PTS);
+        if (nw <= 0) break;
+        const float h2 = 0.5f * (float)(nw - 1);
+        const bool l2 = h2 >= ML_MIN_H2 && fabsf(jf - ((float)(w * ML_WARP_PTS) + h2)) - h2 > h2 + 1.f;
+        if (!l2) l3mask |= 1u << w;
+      }
+    }
+    if (inner && hw >= 0.f && l3mask) {
       const float q = jf + L.b / L.a;                       // centre in points
       const float lo_f = fmaxf(ceilf(q - hw), 0.f);
       const float hi_f = fminf(floorf(q + hw), (float)(n_c - 1));
@@ -186,7 +197,9 @@ tau_ml_kernel(const LineF32* __restrict__ prep, int n_lines, const int2* __restr
     if (pass) {
       MlLine r;
       r.g = make_float4(lev1 ? C1 - jf : jf, L.a, L.b, L.amp_far);
-      r.h = make_float4(L.y, y2, L.amp, hw);
+      const float rc = rcp_approx(FAR_Z2);
+      const float clamp_val = L.amp_far * (rc * fmaf(fmaf(-2.0f * y2, rc, 1.5f), rc, 1.0f));
+      r.h = make_float4(L.y, y2, L.amp, clamp_val);
       const unsigned lt = (1u << lane) - 1u;
       if (lev1) {
         s1[off1 + __popc(b1 & lt)] = r;
@@ -195,6 +208,7 @@ tau_ml_kernel(const LineF32* __restrict__ prep, int n_lines, const int2* __restr
         s2[slot] = r;
         s_seg_start[slot] = off3 + near_scan - near_n;       // exclusive prefix in slot order
         s_seg_lo[slot] = (short)near_lo;
+        s_seg_mask[slot] = (unsigned char)l3mask;
       }
     }
     if (tid == 0) s_seg_start[n2] = n_near;
@@ -269,21 +283,17 @@ tau_ml_kernel(const LineF32* __restrict__ prep, int n_lines, const int2* __restr
       for (int i = tid; i < n_near; i += blockDim.x) {
         while (s_seg_start[l + 1] <= i) ++l;
         const int p = s_seg_lo[l] + (i - s_seg_start[l]);
+        if (!((s_seg_mask[l] >> (p >> 8)) & 1u)) continue;   // level 2 for the owning warp
         const MlLine R = s2[l];
-        const int wp = p >> 8;                                  // warp owning point p
-        const int nwp = min(ML_WARP_PTS, n_c - wp * ML_WARP_PTS);
-        const float h2p = 0.5f * (float)(nwp - 1);
-        if (h2p >= ML_MIN_H2 && fabsf(R.g.x - ((float)(wp * ML_WARP_PTS) + h2p)) - h2p > h2p + 1.f) continue;
         const float x0 = fmaf((float)(p & ~(P - 1)) - R.g.x, R.g.y, -R.g.z);
         const float x = fmaf((float)(p & (P - 1)), R.g.y, x0);
         const float z2 = fmaf(x, x, R.h.y);
         if (z2 >= FAR_Z2) continue;
         float v;
-        if (z2 >= MID_Z2 && R.h.x >= 0.f) v = R.h.z * re_w_asym3(R.h.x, R.h.y, 1.0f / z2);
+        if (z2 >= MID_Z2 && R.h.x >= 0.f) v = R.g.w * (rcp_approx(z2) * asym5_bracket(R.h.y, rcp_approx(z2)));
         else if (z2 >= CORE_Z2 && R.h.x >= 0.f) v = R.h.z * re_w_cf32(x, R.h.x, z2);
         else v = (float)((double)R.h.z * weideman_re((double)x, (double)R.h.x));
-        const float clamp_val = far_clamped(0.f, FAR_Z2, -2.0f * R.h.y, R.g.w);
-        atomicAdd(&s_core[p], v - clamp_val);
+        atomicAdd(&s_core[p], v - R.h.w);
       }
       if (tid == 0) n_work += (unsigned long long)n_near;
     }
