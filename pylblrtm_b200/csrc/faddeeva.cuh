@@ -186,12 +186,15 @@ LBL_HD cpx<double> weideman_upper(double x, double y) {
   const double nr = L - y, ni = x;              // L + i z
   const double inv = 1.0 / (dr * dr + di * di);
   const double zr = (nr * dr + ni * di) * inv, zi = (ni * dr - nr * di) * inv;   // Z
-  double pr = kWeidemanA[LBL_WEIDEMAN_N - 1], pi = 0.0;
+  const double a[LBL_WEIDEMAN_N] = {LBL_WEIDEMAN_COEFFS};   // folded into immediates when unrolled
+  double pr = a[LBL_WEIDEMAN_N - 1], pim = 0.0;
+#pragma unroll
   for (int k = LBL_WEIDEMAN_N - 2; k >= 0; --k) {
-    const double tr = pr * zr - pi * zi + kWeidemanA[k];
-    pi = pr * zi + pi * zr;
+    const double tr = pr * zr - pim * zi + a[k];
+    pim = pr * zi + pim * zr;
     pr = tr;
   }
+  const double pi = pim;
   const double er = dr * inv, ei = -di * inv;           // 1 / (L - iz)
   const double e2r = er * er - ei * ei, e2i = 2.0 * er * ei;
   cpx<double> w;

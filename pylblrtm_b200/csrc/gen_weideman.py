@@ -33,11 +33,11 @@ def main():
     print("#pragma once")
     print(f"#define LBL_WEIDEMAN_N {N}")
     print(f"#define LBL_WEIDEMAN_L {float(big_l)!r}")
-    print("// a_1 .. a_N (polynomial in Z: sum a_n Z^(n-1))")
-    print("static __host__ __device__ constexpr double kWeidemanA[LBL_WEIDEMAN_N] = {")
+    print("// a_1 .. a_N (polynomial in Z: sum a_n Z^(n-1)), as an initializer list")
+    print("#define LBL_WEIDEMAN_COEFFS \\")
     for i in range(0, N, 3):
-        print("    " + ", ".join(repr(float(v)) for v in a[i:i + 3]) + ",")
-    print("};")
+        tail = ", \\" if i + 3 < N else ""
+        print("    " + ", ".join(repr(float(v)) for v in a[i:i + 3]) + tail)
 
 
 if __name__ == "__main__":

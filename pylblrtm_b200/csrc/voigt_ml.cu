@@ -13,13 +13,11 @@
 //  level 2  the other lines farther than one sub-chunk half-width from a warp's
 //           256-point sub-chunk: 16 Chebyshev nodes per sub-chunk, same geometry;
 //  level 3  the remaining lines: direct evaluation at every point. The warp's
-//           loop is branch-free: it evaluates the two-term far-wing form with
-//           |z|^2 clamped to >= FAR_Z2, so every point inside a line's near zone
-//           receives the same constant. A per-warp near pass then walks each
-//           line's near zone with consecutive points on consecutive lanes and
-//           adds (accurate value - that constant): three-term asymptotic form,
-//           float continued fraction, or Weideman's float64 approximation in the
-//           core |z|^2 < 36.
+//           loop is branch-free: it evaluates the five-term asymptotic form with
+//           |z|^2 clamped to >= MID_Z2 = 64, so every point inside a line's near
+//           zone receives the same constant. A CTA-wide near pass then gives each
+//           near point (accurate value - that constant): float continued fraction
+//           for 36 <= |z|^2 < 64, Weideman's float64 approximation below.
 //
 // Inside a reference tile the set of lines is fixed, so every level-1/2 sum is
 // smooth over its interval; the window test keeps the reference's truncation.
@@ -55,10 +53,11 @@ __device__ __forceinline__ float line_value(float x, const MlLine& L) {
   return (float)((double)L.h.z * weideman_re((double)x, (double)L.h.x));
 }
 
-// Far-wing form with |z|^2 clamped to >= FAR_Z2 (the level-3 loop body).
-__device__ __forceinline__ float far_clamped(float x, float y2, float n2y2, float amp_far) {
-  const float r = rcp_approx(fmaxf(fmaf(x, x, y2), FAR_Z2));
-  return amp_far * (r * fmaf(fmaf(n2y2, r, 1.5f), r, 1.0f));
+// Five-term asymptotic form with |z|^2 clamped to >= MID_Z2 (the level-3 loop
+// body, times amp_far); inside the near zone it is the constant rc S(rc), rc = 1/MID_Z2.
+__device__ __forceinline__ float mid_clamped_term(float x, float y2) {
+  const float r = rcp_approx(fmaxf(fmaf(x, x, y2), MID_Z2));
+  return r * asym5_bracket(y2, r);
 }
 
 __device__ __forceinline__ void kahan_add(float& sum, float& comp, float v) {
@@ -125,8 +124,6 @@ tau_ml_kernel(const LineF32* __restrict__ prep, int n_lines, const int2* __restr
   const float xn1 = H1 * (float)cospi((2.0 * (tid & 15) + 1.0) / (2.0 * ML_K));
   const float xn2 = H2 * (float)cospi((2.0 * (lane & 15) + 1.0) / (2.0 * ML_K));
   const float pf = (float)(w0 + lane * P);                   // this lane's first point
-  constexpr float WHW = 0.5f * (ML_WARP_PTS - 1);
-  const float wc = (float)w0 + WHW;
 
   for (int i = tid; i < ML_CHUNK; i += blockDim.x) s_core[i] = 0.f;
 
@@ -151,9 +148,9 @@ tau_ml_kernel(const LineF32* __restrict__ prep, int n_lines, const int2* __restr
     const float jf = (float)((long long)L.j0 - c0);
     const bool lev1 = pass && use_l1 && (fabsf(jf - C1) - H1 > H1 + 1.f);
     const bool inner = pass && !lev1;
-    // near range (points with possibly |z|^2 < FAR_Z2) of an inner line, clipped to the chunk
+    // near range (points with possibly |z|^2 < MID_Z2) of an inner line, clipped to the chunk
     const float y2 = L.y * L.y;
-    const float hw = (y2 >= FAR_Z2 && L.y >= 0.f) ? -1.0f : sqrtf(fmaxf(FAR_Z2 - y2, 0.f)) / L.a + 1.0f;
+    const float hw = (y2 >= MID_Z2 && L.y >= 0.f) ? -1.0f : sqrtf(fmaxf(MID_Z2 - y2, 0.f)) / L.a + 1.0f;
     int near_lo = 0, near_n = 0;
     unsigned l3mask = 0;
     if (inner) {
@@ -197,8 +194,7 @@ tau_ml_kernel(const LineF32* __restrict__ prep, int n_lines, const int2* __restr
     if (pass) {
       MlLine r;
       r.g = make_float4(lev1 ? C1 - jf : jf, L.a, L.b, L.amp_far);
-      const float rc = rcp_approx(FAR_Z2);
-      const float clamp_val = L.amp_far * (rc * fmaf(fmaf(-2.0f * y2, rc, 1.5f), rc, 1.0f));
+      const float clamp_val = L.amp_far * mid_clamped_term(0.f, y2);   // r = 1/MID_Z2 when y2 < MID_Z2
       r.h = make_float4(L.y, y2, L.amp, clamp_val);
       const unsigned lt = (1u << lane) - 1u;
       if (lev1) {
@@ -264,20 +260,15 @@ tau_ml_kernel(const LineF32* __restrict__ prep, int n_lines, const int2* __restr
     for (int i = 0; i < n3w; ++i) {
       const MlLine R = s2[s_l3[warp][i]];
       const float x0 = fmaf(pf - R.g.x, R.g.y, -R.g.z);
-      const float n2y2 = -2.0f * R.h.y;
 #pragma unroll
-      for (int m = 0; m < P; ++m) {
-        const float x = fmaf((float)m, R.g.y, x0);
-        const float r = rcp_approx(fmaxf(fmaf(x, x, R.h.y), FAR_Z2));
-        acc[m] = fmaf(R.g.w, r * fmaf(fmaf(n2y2, r, 1.5f), r, 1.0f), acc[m]);
-      }
+      for (int m = 0; m < P; ++m) acc[m] = fmaf(R.g.w, mid_clamped_term(fmaf((float)m, R.g.y, x0), R.h.y), acc[m]);
     }
     if (lane == 0) n_work += (unsigned long long)n3w * n_w;
     // ---- level 3, near part, spread over the CTA: near item i is point
     // s_seg_lo[l] + (i - s_seg_start[l]) of inner line l. It gets (accurate value -
-    // clamped far-loop value) if the line is level 3 for the warp owning the point
-    // and |z|^2 < FAR_Z2 there; x is formed exactly as in the far loop, so the
-    // clamped value cancels. Consecutive threads take consecutive points of a line.
+    // clamped loop value) if the line is level 3 for the warp owning the point and
+    // |z|^2 < MID_Z2 there; x is formed exactly as in the loop, so the clamped value
+    // cancels. Consecutive threads take consecutive points of a line.
     {
       int l = 0;
       for (int i = tid; i < n_near; i += blockDim.x) {
@@ -288,10 +279,9 @@ tau_ml_kernel(const LineF32* __restrict__ prep, int n_lines, const int2* __restr
         const float x0 = fmaf((float)(p & ~(P - 1)) - R.g.x, R.g.y, -R.g.z);
         const float x = fmaf((float)(p & (P - 1)), R.g.y, x0);
         const float z2 = fmaf(x, x, R.h.y);
-        if (z2 >= FAR_Z2) continue;
+        if (z2 >= MID_Z2) continue;
         float v;
-        if (z2 >= MID_Z2 && R.h.x >= 0.f) v = R.g.w * (rcp_approx(z2) * asym5_bracket(R.h.y, rcp_approx(z2)));
-        else if (z2 >= CORE_Z2 && R.h.x >= 0.f) v = R.h.z * re_w_cf32(x, R.h.x, z2);
+        if (z2 >= CORE_Z2 && R.h.x >= 0.f) v = R.h.z * re_w_cf32(x, R.h.x, z2);
         else v = (float)((double)R.h.z * weideman_re((double)x, (double)R.h.x));
         atomicAdd(&s_core[p], v - R.h.w);
       }
