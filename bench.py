@@ -35,7 +35,12 @@ sys.path.insert(0, ROOT)
 METRIC = "Voigt line-evals/s"
 UNIT = "line-evals/s"
 WORKLOAD = "three_gas_200k_lines_60_layers_600-2500cm-1_step0.001_cutoff25_tile2_mu0.8"
-FLOPS_PER_EVAL_FAR = 12      # far-wing branch of the float32 kernels: 5 FFMA + 1 FMUL + 1 RCP
+FLOPS_PER_EVAL_FAR = 12      # two-term far-wing form: 5 FFMA + 1 FMUL + 1 RCP (FMA = 2 flops)
+# multi-level kernel, per unit of each work category (FMA = 2 flops, RCP = 1):
+FLOPS_NODE = 12              # Chebyshev-node evaluation (two-term form)
+FLOPS_L3 = 38                # level-3 loop evaluation (clamped five-term form)
+FLOPS_NEAR = 60              # near-zone point (float continued fraction / float64 rational, average)
+FLOPS_CHEB_PER_POINT = 128   # two 16-term Clenshaw sums per point and layer
 CPU_SAMPLE = (1000.0, 1000.5)  # sub-window timed on the host (all 60 layers)
 
 
@@ -294,7 +299,15 @@ def main():
         return
     peak = fp32_peak(torch)
     tau_avg = sum(tau_ms) / len(tau_ms)
-    achieved = work_per_step * FLOPS_PER_EVAL_FAR / (tau_avg * 1e-3) / 1e12
+    if a.precision == "fp32":
+        nodes, l3, near = r0.work_split
+        flops = nodes * FLOPS_NODE + l3 * FLOPS_L3 + near * FLOPS_NEAR + FLOPS_CHEB_PER_POINT * grid.n_nu * 60
+        flops_note = (f"{nodes:.3e} node evals x {FLOPS_NODE} + {l3:.3e} level-3 evals x {FLOPS_L3} + "
+                      f"{near:.3e} near points x {FLOPS_NEAR} + Chebyshev {FLOPS_CHEB_PER_POINT}/point/layer")
+    else:
+        flops = work_per_step * FLOPS_PER_EVAL_FAR
+        flops_note = f"{work_per_step:.3e} evaluations x {FLOPS_PER_EVAL_FAR}"
+    achieved = flops / (tau_avg * 1e-3) / 1e12
     cpu = None
     if world == 1 and not a.no_cpu_baseline:
         n, dt = cpu_reference_sample(1)
@@ -319,7 +332,7 @@ def main():
                      "faddeeva_evals_per_launch": work_per_step,
                      "kernel_ms": tau_avg,
                      "peak_source": "measured live: lbl_probe_fma_f32 (MEASURED_PEAKS.json has no fp32 entry)",
-                     "flops_per_eval": FLOPS_PER_EVAL_FAR},
+                     "flops_per_launch": flops, "flops_count": flops_note},
         "gpu_launches": launches_per_step * a.steps,
         "clocks": clocks.summary(),
         "e2e": e2e,

@@ -145,8 +145,9 @@ int lbl_tau_tiles_f32(const LineF32* prep, int n_lines, const int* ranges, const
  * tile), lines farther than a chunk half-width contribute through 16 Chebyshev
  * nodes over the chunk, the remaining lines farther than a 256-point sub-chunk
  * half-width through 16 nodes over that sub-chunk, the rest directly. evals
- * counts reference-rule evaluations, work (nullable) the Faddeeva evaluations
- * actually performed. Replaces pylblrtm/forward.py:295-315. */
+ * counts reference-rule evaluations; work (nullable, 3 x u64) receives the
+ * evaluations actually performed: [0] Chebyshev-node evaluations, [1] level-3
+ * loop evaluations, [2] near-zone points. Replaces pylblrtm/forward.py:295-315. */
 int lbl_tau_tiles_ml_f32(const LineF32* prep, int n_lines, const int* ranges, const double* t_layer, int n_rows,
                          double nu_min, double step, long long n_nu, int tile_samples, double cutoff, int n_grp,
                          float* od, int* err, unsigned long long* evals, unsigned long long* work, void* stream);

@@ -133,7 +133,7 @@ tau_ml_kernel(const LineF32* __restrict__ prep, int n_lines, const int2* __restr
 #pragma unroll
   for (int m = 0; m < P; ++m) acc[m] = 0.f;
   float sum1 = 0.f, comp1 = 0.f, sum2 = 0.f, comp2 = 0.f;
-  unsigned long long n_pass = 0, n_work = 0;
+  unsigned long long n_pass = 0, n_nodes = 0, n_l3 = 0, n_near_items = 0;
 
   // register prefetch of the next round's line records
   LineF32 nxt;
@@ -221,7 +221,7 @@ tau_ml_kernel(const LineF32* __restrict__ prep, int n_lines, const int2* __restr
         a1 += line_value(x, R);
       }
       kahan_add(sum1, comp1, a1);
-      if (tid == 0) n_work += (unsigned long long)n1 * ML_K;
+      if (tid == 0) n_nodes += (unsigned long long)n1 * ML_K;
     }
 
     // ---- per-warp split of the inner lines into level 2 and level 3
@@ -253,7 +253,7 @@ tau_ml_kernel(const LineF32* __restrict__ prep, int n_lines, const int2* __restr
         a2 += line_value(x, R);
       }
       kahan_add(sum2, comp2, a2);
-      if (lane == 0) n_work += (unsigned long long)n2w * ML_K;
+      if (lane == 0) n_nodes += (unsigned long long)n2w * ML_K;
     }
 
     // ---- level 3, far part: every point of the warp, |z|^2 clamped (branch-free)
@@ -263,7 +263,7 @@ tau_ml_kernel(const LineF32* __restrict__ prep, int n_lines, const int2* __restr
 #pragma unroll
       for (int m = 0; m < P; ++m) acc[m] = fmaf(R.g.w, mid_clamped_term(fmaf((float)m, R.g.y, x0), R.h.y), acc[m]);
     }
-    if (lane == 0) n_work += (unsigned long long)n3w * n_w;
+    if (lane == 0) n_l3 += (unsigned long long)n3w * n_w;
     // ---- level 3, near part, spread over the CTA: near item i is point
     // s_seg_lo[l] + (i - s_seg_start[l]) of inner line l. It gets (accurate value -
     // clamped loop value) if the line is level 3 for the warp owning the point and
@@ -285,7 +285,7 @@ tau_ml_kernel(const LineF32* __restrict__ prep, int n_lines, const int2* __restr
         else v = (float)((double)R.h.z * weideman_re((double)x, (double)R.h.x));
         atomicAdd(&s_core[p], v - R.h.w);
       }
-      if (tid == 0) n_work += (unsigned long long)n_near;
+      if (tid == 0) n_near_items += (unsigned long long)n_near;
     }
     __syncthreads();
   }
@@ -340,7 +340,11 @@ tau_ml_kernel(const LineF32* __restrict__ prep, int n_lines, const int2* __restr
   }
   if (bad) flag_error(err, row * (n_grp + 1) + n_grp);
   if (tid == 0 && evals && n_pass) atomicAdd(evals, n_pass * (unsigned long long)n_c);
-  if (work && n_work) atomicAdd(work, n_work);
+  if (work) {   // work[0]: node evaluations, work[1]: level-3 loop evaluations, work[2]: near items
+    if (n_nodes) atomicAdd(&work[0], n_nodes);
+    if (n_l3) atomicAdd(&work[1], n_l3);
+    if (n_near_items) atomicAdd(&work[2], n_near_items);
+  }
 }
 
 }  // namespace lbl

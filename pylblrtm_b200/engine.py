@@ -226,6 +226,7 @@ class EngineResult:
     tau: object = None             # torch float64 [n_prof, n_nu]
     evals: int = 0                 # Voigt evaluations under the reference tile rule
     work: int = 0                  # Faddeeva evaluations actually performed (multi-level engine)
+    work_split: tuple = ()         # (node evaluations, level-3 loop evaluations, near-zone points)
     groups: List[Group] = field(default_factory=list)
 
 
@@ -385,7 +386,7 @@ class Job:
         self.launches += 2
         # per (layer, line) prep and the Voigt sums
         err = torch.full((1,), INT_MAX, dtype=torch.int32, device=dev)
-        evals = torch.zeros(2, dtype=torch.int64, device=dev) if count_evals else None
+        evals = torch.zeros(4, dtype=torch.int64, device=dev) if count_evals else None
         od = torch.empty((n_prof, n_lay, n_nu), dtype=od_dtype, device=dev)
         rec = _lib.SIZEOF_LINE_F32 if single else _lib.SIZEOF_LINE_F64
         prep = torch.empty((n_rows * n_kept * rec // 8,), dtype=torch.float64, device=dev)
@@ -420,7 +421,11 @@ class Job:
         if evals is not None:
             ev = evals.cpu().tolist()
             res.evals = int(ev[0])
-            res.work = int(ev[1]) if precision == "fp32" else int(ev[0])
+            if precision == "fp32":
+                res.work_split = tuple(int(v) for v in ev[1:4])
+                res.work = sum(res.work_split)
+            else:
+                res.work = int(ev[0])
         return finish(od)
 
 
