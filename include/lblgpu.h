@@ -161,6 +161,16 @@ int lbl_layer_sum_exp_f32(const float* od, int n_prof, int n_lay, long long n_nu
 int lbl_layer_sum_exp_f64(const double* od, int n_prof, int n_lay, long long n_nu, const double* mu,
                           double* trans, double* tau, void* stream);
 
+/* Channel box-average of the transmittance (no reference counterpart; serves
+ * channel-averaged retrievals and the surrogate's training targets): out[b, c] =
+ * mean over p in [first + c*width, first + (c+1)*width) of
+ * exp(-sum_k od[b, k, p] / mu[b]); od [n_prof, n_lay, n_nu], mu [n_prof] and
+ * out [n_prof, n_ch] in device memory. */
+int lbl_channel_mean_f32(const float* od, int n_prof, int n_lay, long long n_nu, const double* mu, long long first,
+                         int width, int n_ch, double* out, void* stream);
+int lbl_channel_mean_f64(const double* od, int n_prof, int n_lay, long long n_nu, const double* mu, long long first,
+                         int width, int n_ch, double* out, void* stream);
+
 /* Faddeeva function on arrays (diagnostics; replaces the scipy.special.wofz call
  * at forward.py:62). mode 0: general algorithm; mode 1 (f32 only): the
  * engine's real part with the far-wing branch (im not written). */

@@ -9,6 +9,7 @@ line-by-line sums run as hand-written sm_100a CUDA kernels
 """
 
 from .atmosphere import AtmosphericProfile
+from .batch import transmittance_batch
 from .config import ForwardResult, load_config, run_forward
 from .forward import compute_transmittance
 from .hitran_ids import MOLECULE_IDS
@@ -27,4 +28,5 @@ __all__ = [
     "us_standard_atmosphere",
     "list_profile_gases",
     "MOLECULE_IDS",
+    "transmittance_batch",
 ]

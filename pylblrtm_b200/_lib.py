@@ -45,6 +45,8 @@ SIGNATURES = {
     "lbl_tau_tiles_ml_f32": (_I, [_P, _I, _P, _P, _I, _D, _D, _L, _I, _D, _I, _P, _P, _P, _P, _P]),
     "lbl_layer_sum_exp_f32": (_I, [_P, _I, _I, _L, _P, _P, _P, _P]),
     "lbl_layer_sum_exp_f64": (_I, [_P, _I, _I, _L, _P, _P, _P, _P]),
+    "lbl_channel_mean_f32": (_I, [_P, _I, _I, _L, _P, _L, _I, _I, _P, _P]),
+    "lbl_channel_mean_f64": (_I, [_P, _I, _I, _L, _P, _L, _I, _I, _P, _P]),
     "lbl_faddeeva_f64": (_I, [_P, _P, _L, _P, _P, _P]),
     "lbl_faddeeva_f32": (_I, [_P, _P, _L, _P, _P, _I, _P]),
     "lbl_probe_fma_f32": (_I, [_P, _I, _I, _P]),

@@ -370,3 +370,54 @@ extern "C" int lbl_probe_fma_f32(float* out, int iters, int blocks, void* stream
   fma_probe_kernel<<<blocks, 256, 0, (cudaStream_t)stream>>>(out, iters, 1.0f);
   return lbl_check_launch("lbl_probe_fma_f32");
 }
+
+// ---------------------------------------------------------------------------
+// Fused column sum, transmittance and channel box-average: channel c of profile b
+// is the mean of exp(-sum_k od[b,k,p] / mu[b]) over the half-open point range
+// [first + c*width, first + (c+1)*width). One CTA per (channel, profile); the
+// per-point transmittance never goes to memory.
+template <typename T>
+__global__ void __launch_bounds__(256)
+channel_mean_kernel(const T* __restrict__ od, int n_lay, long long n_nu, const double* __restrict__ mu,
+                    long long first, int width, int n_ch, double* __restrict__ out) {
+  __shared__ double s_part[8];
+  const int c = blockIdx.x, b = blockIdx.y;
+  const T* base = od + (long long)b * n_lay * n_nu;
+  const double inv_mu = 1.0 / mu[b];
+  double acc = 0.0;
+  for (int t = threadIdx.x; t < width; t += blockDim.x) {
+    const long long p = first + (long long)c * width + t;
+    double s = 0.0;
+    for (int k = 0; k < n_lay; ++k) s = __dadd_rn(s, (double)base[(long long)k * n_nu + p]);
+    acc += exp(-s * inv_mu);
+  }
+  for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+  if ((threadIdx.x & 31) == 0) s_part[threadIdx.x >> 5] = acc;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = 0.0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += s_part[w];
+    out[(long long)b * n_ch + c] = t / width;
+  }
+}
+
+template <typename T>
+static int launch_channel_mean(const T* od, int n_prof, int n_lay, long long n_nu, const double* mu, long long first,
+                               int width, int n_ch, double* out, void* stream, const char* name) {
+  if (!od || !mu || !out || n_prof < 1 || n_prof > 65535 || n_lay < 0 || width < 1 || n_ch < 1 || first < 0 ||
+      first + (long long)width * n_ch > n_nu)
+    return lbl_set_error(LBL_EINVAL, "%s: bad arguments", name);
+  dim3 grid((unsigned)n_ch, (unsigned)n_prof);
+  channel_mean_kernel<T><<<grid, 256, 0, (cudaStream_t)stream>>>(od, n_lay, n_nu, mu, first, width, n_ch, out);
+  return lbl_check_launch(name);
+}
+
+extern "C" int lbl_channel_mean_f32(const float* od, int n_prof, int n_lay, long long n_nu, const double* mu,
+                                    long long first, int width, int n_ch, double* out, void* stream) {
+  return launch_channel_mean(od, n_prof, n_lay, n_nu, mu, first, width, n_ch, out, stream, "lbl_channel_mean_f32");
+}
+
+extern "C" int lbl_channel_mean_f64(const double* od, int n_prof, int n_lay, long long n_nu, const double* mu,
+                                    long long first, int width, int n_ch, double* out, void* stream) {
+  return launch_channel_mean(od, n_prof, n_lay, n_nu, mu, first, width, n_ch, out, stream, "lbl_channel_mean_f64");
+}

@@ -224,6 +224,7 @@ class EngineResult:
     od: object = None              # torch tensor [n_prof, n_lay, n_nu] (float32 or float64)
     trans: object = None           # torch float64 [n_prof, n_nu]
     tau: object = None             # torch float64 [n_prof, n_nu]
+    channels: object = None        # torch float64 [n_prof, n_ch] channel-mean transmittance
     evals: int = 0                 # Voigt evaluations under the reference tile rule
     work: int = 0                  # Faddeeva evaluations actually performed (multi-level engine)
     work_split: tuple = ()         # (node evaluations, level-3 loop evaluations, near-zone points)
@@ -307,8 +308,12 @@ class Job:
 
     def run(self, precision: str = "fp32", mu: Optional[Sequence[float]] = None, want_od: bool = True,
             want_tau: bool = False, want_trans: bool = False, count_evals: bool = False,
-            timer: Optional[dict] = None) -> EngineResult:
-        """All device stages; ``timer`` (dict) receives CUDA-event times of the summation kernel."""
+            timer: Optional[dict] = None, channels: Optional[Tuple[int, int]] = None) -> EngineResult:
+        """All device stages; ``timer`` (dict) receives CUDA-event times of the summation kernel.
+
+        ``channels = (width_points, n_channels)`` adds channel-mean transmittances
+        over consecutive half-open blocks of ``width_points`` grid points.
+        """
         if precision not in PRECISIONS:
             raise ValueError(f"precision must be one of {PRECISIONS}, got {precision!r}")
         torch, dev = self.torch, self.dev
@@ -323,9 +328,19 @@ class Job:
 
         def finish(od):
             res.od = od if want_od else None
-            if want_tau or want_trans:
+            mu_d = None
+            if want_tau or want_trans or channels is not None:
                 mu_d = torch.as_tensor(np.broadcast_to(np.asarray(1.0 if mu is None else mu, np.float64),
                                                        (n_prof,)).copy()).to(dev)
+            if channels is not None:
+                width, n_ch = channels
+                out = torch.empty((n_prof, n_ch), dtype=torch.float64, device=dev)
+                fn = "lbl_channel_mean_f32" if od.dtype == torch.float32 else "lbl_channel_mean_f64"
+                _lib.call(fn, od.data_ptr(), n_prof, n_lay, n_nu, mu_d.data_ptr(), 0, int(width), int(n_ch),
+                          out.data_ptr(), stream)
+                self.launches += 1
+                res.channels = out
+            if want_tau or want_trans:
                 tau = torch.empty((n_prof, n_nu), dtype=torch.float64, device=dev) if want_tau else None
                 tr = torch.empty((n_prof, n_nu), dtype=torch.float64, device=dev) if want_trans else None
                 fn = "lbl_layer_sum_exp_f32" if od.dtype == torch.float32 else "lbl_layer_sum_exp_f64"

@@ -221,3 +221,30 @@ def test_full_size_three_gas_fp32_against_fp64(cuda):
         assert np.max(np.abs(r[p].trans[0].cpu().numpy() - r["fp64"].trans[0].cpu().numpy())) <= 1e-5
         rel_od = ((r[p].od[0].double() - od64).abs() / od64.abs()).max().item()
         assert rel_od <= 3e-5, (p, rel_od)
+
+
+def test_batch_equals_single_profiles_bitwise(cuda):
+    """A batch of perturbed profiles gives exactly the per-profile spectra."""
+    sd = synthetic.restrict(synthetic.three_gas_lines(30000, 1480.0, 1540.0, seed=9), 1480.0, 1540.0)
+    lv = synthetic.perturbed_levels(synthetic.logp_levels(13), 3, seed=5)
+    mu = np.array([1.0, 0.7, 0.45])
+    for precision in ("fp32", "fp64"):
+        nu, tb = lbl.transmittance_batch(sd, lv["p"], lv["t"], {g: lv[g] for g in ("H2O", "CO2", "O3")},
+                                         1500.0, 1510.0, mu_view=mu, precision=precision)
+        for i in range(3):
+            _, t1 = lbl.compute_transmittance(sd, synthetic.profile_from_levels(lv, i), 1500.0, 1510.0,
+                                              mu_view=float(mu[i]), precision=precision)
+            assert np.array_equal(tb[i], t1), (precision, i)
+
+
+def test_channel_mean_matches_host_box_average(cuda):
+    sd = synthetic.restrict(synthetic.three_gas_lines(30000, 1480.0, 1540.0, seed=9), 1480.0, 1540.0)
+    lv = synthetic.perturbed_levels(synthetic.logp_levels(9), 2, seed=6)
+    vmr = {g: lv[g] for g in ("H2O", "CO2", "O3")}
+    nu, tb = lbl.transmittance_batch(sd, lv["p"], lv["t"], vmr, 1500.0, 1505.0, mu_view=0.8)
+    centres, ch = lbl.transmittance_batch(sd, lv["p"], lv["t"], vmr, 1500.0, 1505.0, mu_view=0.8,
+                                          channel_width_cm1=0.25)
+    assert ch.shape == (2, 20) and centres.size == 20
+    ref = tb[:, :20 * 250].reshape(2, 20, 250).mean(axis=2)
+    np.testing.assert_allclose(ch, ref, rtol=1e-12, atol=1e-15)
+    np.testing.assert_allclose(centres, nu[:5000].reshape(20, 250).mean(axis=1), rtol=0, atol=1e-9)

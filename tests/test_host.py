@@ -191,3 +191,17 @@ def test_api_type_and_range_errors():
         lbl.compute_transmittance(sd, prof, 700, 701, mu_view=0)
     with pytest.raises(TypeError):
         lbl.run_forward(sd, None, {})
+
+
+def test_batch_validation_errors():
+    sd = _sd()
+    p = np.array([[1.0, 10.0, 100.0], [1.0, 10.0, 100.0]])
+    t = np.full_like(p, 250.0)
+    with pytest.raises(ValueError, match="strictly increasing"):
+        lbl.transmittance_batch(sd, p[:, ::-1], t, {"H2O": np.full_like(p, 1e-3)}, 700, 701)
+    with pytest.raises(ValueError, match=r"vmr\['H2O'\] must be finite and in \[0, 1\]"):
+        lbl.transmittance_batch(sd, p, t, {"H2O": np.full_like(p, 2.0)}, 700, 701)
+    with pytest.raises(ValueError, match="mu_view"):
+        lbl.transmittance_batch(sd, p, t, {"H2O": np.full_like(p, 1e-3)}, 700, 701, mu_view=[1.0, 0.0])
+    with pytest.raises(TypeError):
+        lbl.transmittance_batch(None, p, t, {}, 700, 701)
