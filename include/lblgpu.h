@@ -54,6 +54,11 @@ typedef struct {
   float b, a, y, amp, amp_far;
 } LineF32;
 
+/* Jacobian coefficients of one prepared line (see lbl_line_prep_jac). */
+typedef struct {
+  float jT_u, jT_x, jT_y, jv_u, jv_y, jv_x, pad0, pad1;
+} LineJac;
+
 /* Last error message of the calling thread ("" if none). */
 const char* lbl_last_error(void);
 /* ABI version of this library. */
@@ -126,6 +131,15 @@ int lbl_line_prep_f64(const LineIn* lines, const int* n_kept, int n_lines, const
 int lbl_line_prep_f32(const LineIn* lines, const int* n_kept, int n_lines, const LayerGroup* lg, int n_rows,
                       int n_grp, double nu_min, double step, LineF32* out, int* err, void* stream);
 
+/* Per (row, sorted line) coefficients of the layer Jacobians d od / dT_layer and
+ * d od / d ln VMR_layer (no reference counterpart: the retrieval adjoint). They
+ * differentiate the expressions of pylblrtm/forward.py:257-292. jac_grp_mask has
+ * bit g set for the groups of the gas whose VMR is differentiated; dlnq_scratch
+ * holds n_rows * n_grp doubles (d ln Q / dT). */
+int lbl_line_prep_jac(const LineIn* lines, int n_lines, const LayerGroup* lg, int n_rows, int n_grp,
+                      const int* tips_off, const int* tips_len, const double* tips_t, const double* tips_q,
+                      int jac_grp_mask, double* dlnq_scratch, LineJac* out, void* stream);
+
 /* Optical depth of every (row, grid point): the Voigt sum over the lines of
  * the point's reference tile window, times R(nu, T_row); replaces
  * pylblrtm/forward.py:295-315 (tile loop, _voigt, phi @ S, radiation term and
@@ -151,6 +165,20 @@ int lbl_tau_tiles_f32(const LineF32* prep, int n_lines, const int* ranges, const
 int lbl_tau_tiles_ml_f32(const LineF32* prep, int n_lines, const int* ranges, const double* t_layer, int n_rows,
                          double nu_min, double step, long long n_nu, int tile_samples, double cutoff, int n_grp,
                          float* od, int* err, unsigned long long* evals, unsigned long long* work, void* stream);
+
+/* Layer Jacobians by the multi-level float32 summation (no reference
+ * counterpart; the retrieval adjoint): writes od (as lbl_tau_tiles_ml_f32),
+ * d_t = d od / dT_layer and d_v = d od / d ln VMR_layer of the gas chosen in
+ * lbl_line_prep_jac, all [n_rows, n_nu] (rows = n_prof * n_lay). Since layer k's
+ * T and VMR enter only od_k, these are the full per-layer Jacobians of
+ * tau = sum_k od_k. With g_tau ([n_prof, n_nu] float64, d loss / d tau) the
+ * kernel writes nothing per point and instead adds sum_p g_tau * d_t (d_v) into
+ * vjp_t[row] (vjp_v[row]) (caller zeroes them): the vector-Jacobian product,
+ * recomputing every Voigt value instead of storing the Jacobian. */
+int lbl_jacobian_ml_f32(const LineF32* prep, const LineJac* jprep, int n_lines, const int* ranges,
+                        const double* t_layer, int n_rows, int n_lay, double nu_min, double step, long long n_nu,
+                        int tile_samples, double cutoff, float* od, float* d_t, float* d_v, const double* g_tau,
+                        double* vjp_t, double* vjp_v, void* stream);
 
 /* Column sums over layers and transmittance exp(-tau / mu); replaces
  * pylblrtm/forward.py:151 and config.py:266-270. od: [n_prof, n_lay, n_nu]

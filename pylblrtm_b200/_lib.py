@@ -20,6 +20,7 @@ SIZEOF_LAYER_GROUP = 48
 SIZEOF_LINE_IN = 64
 SIZEOF_LINE_F64 = 32
 SIZEOF_LINE_F32 = 32
+SIZEOF_LINE_JAC = 32
 
 _P = ctypes.c_void_p
 _I = ctypes.c_int
@@ -43,6 +44,8 @@ SIGNATURES = {
     "lbl_tau_tiles_f64": (_I, [_P, _I, _P, _P, _I, _D, _D, _L, _I, _D, _I, _P, _P, _P, _P]),
     "lbl_tau_tiles_f32": (_I, [_P, _I, _P, _P, _I, _D, _D, _L, _I, _D, _I, _P, _P, _P, _P]),
     "lbl_tau_tiles_ml_f32": (_I, [_P, _I, _P, _P, _I, _D, _D, _L, _I, _D, _I, _P, _P, _P, _P, _P]),
+    "lbl_line_prep_jac": (_I, [_P, _I, _P, _I, _I, _P, _P, _P, _P, _I, _P, _P, _P]),
+    "lbl_jacobian_ml_f32": (_I, [_P, _P, _I, _P, _P, _I, _I, _D, _D, _L, _I, _D, _P, _P, _P, _P, _P, _P, _P]),
     "lbl_layer_sum_exp_f32": (_I, [_P, _I, _I, _L, _P, _P, _P, _P]),
     "lbl_layer_sum_exp_f64": (_I, [_P, _I, _I, _L, _P, _P, _P, _P]),
     "lbl_channel_mean_f32": (_I, [_P, _I, _I, _L, _P, _L, _I, _I, _P, _P]),

@@ -16,8 +16,8 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 PKG = os.path.dirname(HERE)
 ROOT = os.path.dirname(PKG)
-SOURCES = ["capi.cu", "prep.cu", "voigt.cu", "voigt_ml.cu"]
-HEADERS = ["lbl_common.cuh", "faddeeva.cuh", "sum_common.cuh", os.path.join("..", "..", "include", "lblgpu.h")]
+SOURCES = ["capi.cu", "prep.cu", "voigt.cu", "voigt_ml.cu", "voigt_ml_jac.cu"]
+HEADERS = ["lbl_common.cuh", "faddeeva.cuh", "sum_common.cuh", "weideman_coeffs.h", os.path.join("..", "..", "include", "lblgpu.h")]
 LIB = os.path.join(PKG, "liblblgpu.so")
 HOST_LIB = os.path.join(PKG, "libfaddeeva_host.so")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]

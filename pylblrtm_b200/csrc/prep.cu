@@ -462,3 +462,93 @@ extern "C" int lbl_sort_lines_noalloc(const double* nu0, const double* shift, co
   return lbl_sort_lines(nu0, shift, gid, n_lines, mask_lo, mask_hi, p_max, scratch, NOALLOC_SCRATCH_BYTES,
                         order, n_kept, max_shift_bound, stream);
 }
+
+// ---------------------------------------------------------------------------
+// Jacobian coefficients (no reference counterpart; the retrieval adjoint).
+//
+// With u = Re w(z), u_x = Re w'(z), u_y = -Im w'(z) (w' = -2 z w + 2i/sqrt(pi)) and
+// amp = S sqrt(ln2/pi)/alpha_D, one line's contribution to a layer's optical depth
+// (before the radiation factor R(nu, T)) is amp * u and its derivatives are
+//   d/dT      = jT_u u - jT_x x u_x - jT_y u_y
+//   d/dlnVMR  = jv_u u + jv_y u_y - jv_x u_x        (lines of the chosen gas only)
+// with, per (layer, line),
+//   jT_u = amp (dlnS/dT - 1/(2T)),  jT_x = amp/(2T),  jT_y = amp y (1/(2T) + n_air/T),
+//   jv_u = amp (1 - dlnR(nuc)/dnuc * c_v),  jv_y = amp s dgamma/dlnVMR,  jv_x = amp s c_v,
+// where s = sqrt(ln2)/alpha_D, c_v = dnuc/dlnVMR = -shift p_self,
+//   dgamma/dlnVMR = (296/T)^n_air (g_self - g_air) p_self,
+//   dlnS/dT = -Q'(T)/Q(T) + c2 E''/T^2 - (c2 nu0/T^2)/(exp(c2 nu0/T) - 1) + (2v/T)/sinh(2v),
+//   v = c2 nuc/(2T)  (the last term is -dlnR(nuc, T)/dT), dlnR(nu)/dnu = 1/nu + (c2/T)/sinh(2v).
+// They follow from differentiating the expressions of pylblrtm/forward.py:257-292
+// (alpha_D scales as sqrt(T), gamma as T^-n_air, the column as the VMR).
+
+// d ln Q / dT of np.interp's piecewise-linear table (0 where clamped).
+__device__ double interp_dlog(double x, const double* __restrict__ xp, const double* __restrict__ fp, int n) {
+  if (isnan(x) || n < 2 || x >= xp[n - 1] || x < xp[0]) return 0.0;
+  int lo = 0, hi = n - 1;
+  while (hi - lo > 1) {
+    const int mid = (lo + hi) >> 1;
+    if (xp[mid] <= x) lo = mid; else hi = mid;
+  }
+  const double slope = (fp[lo + 1] - fp[lo]) / (xp[lo + 1] - xp[lo]);
+  return slope / interp_clamped(x, xp, fp, n);
+}
+
+__global__ void layer_groups_dlnq_kernel(const LayerGroup* __restrict__ lg, int n_rows, int n_grp,
+                                         const int* __restrict__ tips_off, const int* __restrict__ tips_len,
+                                         const double* __restrict__ tips_t, const double* __restrict__ tips_q,
+                                         double* __restrict__ dlnq) {
+  const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= (long long)n_rows * n_grp) return;
+  const int g = (int)(idx % n_grp);
+  dlnq[idx] = interp_dlog(lg[idx].T, tips_t + tips_off[g], tips_q + tips_off[g], tips_len[g]);
+}
+
+__global__ void line_prep_jac_kernel(const LineIn* __restrict__ lines, int n_lines, const LayerGroup* __restrict__ lg,
+                                     const double* __restrict__ dlnq, int n_rows, int n_grp, int jac_grp_mask,
+                                     LineJac* __restrict__ out) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  const int row = blockIdx.y;
+  if (j >= n_lines || row >= n_rows) return;
+  const LineIn L = lines[j];
+  const long long gi = (long long)row * n_grp + L.gid;
+  const LayerGroup G = lg[gi];
+  LineJac r = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+  const ScaledLine s = scale_line(L, G, nullptr, 0);
+  if (s.active) {
+    const double T = G.T;
+    const double amp = VOIGT_K / s.alpha * s.S;
+    const double sc = SQRT_LN2 / s.alpha;
+    const double y = sc * s.gamma;
+    const double a = C2 * L.nu0 / T;
+    const double v = 0.5 * C2 * s.nuc / T;
+    const double dlnS = -dlnq[gi] + C2 * L.elow / (T * T) - (a / T) / expm1(a) + (2.0 * v / T) / sinh(2.0 * v);
+    r.jT_u = (float)(amp * (dlnS - 0.5 / T));
+    r.jT_x = (float)(amp * 0.5 / T);
+    r.jT_y = (float)(amp * y * (0.5 / T + L.n_air / T));
+    if ((jac_grp_mask >> L.gid) & 1) {
+      const double c_v = -L.shift * G.p_self;
+      const double dlnR_dnu = 1.0 / s.nuc + (C2 / T) / sinh(2.0 * v);
+      const double dgamma = pow(T_REF / T, L.n_air) * (L.g_self - L.g_air) * G.p_self;
+      r.jv_u = (float)(amp * (1.0 - dlnR_dnu * c_v));
+      r.jv_y = (float)(amp * sc * dgamma);
+      r.jv_x = (float)(amp * sc * c_v);
+    }
+  }
+  out[(long long)row * n_lines + j] = r;
+}
+
+extern "C" int lbl_line_prep_jac(const LineIn* lines, int n_lines, const LayerGroup* lg, int n_rows, int n_grp,
+                                 const int* tips_off, const int* tips_len, const double* tips_t,
+                                 const double* tips_q, int jac_grp_mask, double* dlnq_scratch, LineJac* out,
+                                 void* stream) {
+  if (n_lines < 1 || n_rows < 1 || n_rows > 65535 || n_grp < 1 || n_grp > 31 || !lines || !lg || !out ||
+      !dlnq_scratch || !tips_off || !tips_len || !tips_t || !tips_q)
+    return lbl_set_error(LBL_EINVAL, "lbl_line_prep_jac: bad arguments");
+  cudaStream_t st = (cudaStream_t)stream;
+  const long long n = (long long)n_rows * n_grp;
+  layer_groups_dlnq_kernel<<<grid1(n, 128), 128, 0, st>>>(lg, n_rows, n_grp, tips_off, tips_len, tips_t, tips_q,
+                                                           dlnq_scratch);
+  dim3 grid(grid1(n_lines, 128), n_rows);
+  line_prep_jac_kernel<<<grid, 128, 0, st>>>(lines, n_lines, lg, dlnq_scratch, n_rows, n_grp, jac_grp_mask, out);
+  return lbl_check_launch("lbl_line_prep_jac");
+}

@@ -1,0 +1,465 @@
+// Layer Jacobians by the multi-level summation (no reference counterpart: the
+// retrieval adjoint).
+//
+// For every (row = profile-layer, grid point) it accumulates three sums over the
+// lines admitted by the reference tile window (pylblrtm/forward.py:295-301):
+//   od       = sum amp u
+//   d/dT     = sum jT_u u - jT_x x u_x - jT_y u_y
+//   d/dlnVMR = sum jv_u u + jv_y u_y - jv_x u_x
+// with u = Re w, u_x = Re w', u_y = -Im w' (coefficients: lbl_line_prep_jac), and
+// writes od R, d(od R)/dT = R_T od + R dT and R d/dlnVMR. Because a layer's
+// temperature and mixing ratio enter only that layer's optical depth, these are
+// the full per-layer Jacobians of tau = sum_k od_k; Voigt values are recomputed,
+// never stored. With a loss gradient g(nu) the epilogue contracts instead
+// (vector-Jacobian product), so backward passes need no Jacobian storage.
+//
+// The distance split is the one of tau_ml_kernel (voigt_ml.cu) with 4 points per
+// lane: Chebyshev nodes for lines far from the chunk (level 1) or from a warp's
+// 128-point sub-chunk (level 2), and a branch-free clamped loop plus a CTA-wide
+// near-zone correction for the rest (level 3). The far field uses the five-term
+// asymptotic series of w and its termwise derivative for w' (forming
+// w' = -2zw + 2i/sqrt(pi) there would cancel catastrophically).
+#include <math.h>
+
+#include "faddeeva.cuh"
+#include "lbl_common.cuh"
+#include "sum_common.cuh"
+
+namespace lbl {
+
+constexpr int MJ_P = 4;
+constexpr int MJ_WARP_PTS = 32 * MJ_P;
+constexpr int MJ_THREADS = 256;
+constexpr int MJ_CHUNK = MJ_THREADS * MJ_P;       // 1024 points
+constexpr int MJ_K = 16;
+constexpr float MJ_MIN_H1 = 32.f;
+constexpr float MJ_MIN_H2 = 16.f;
+
+struct JLine {
+  float4 g;   // jf (or C1 - jf for level 1), a, b, amp
+  float4 h;   // y, y^2, jT_u, jT_x
+  float4 k;   // jT_y, jv_u, jv_y, jv_x
+};
+
+struct U3 { float u, ux, uy; };
+
+// u, u_x, u_y from the five-term series with a given r (1/|z|^2, or 1/max(|z|^2, c)):
+//   w  = (i/sqrt(pi)) q (1 + p/2 + 3p^2/4 + 15p^3/8 + 105p^4/16),
+//   w' = -(i/sqrt(pi)) p (1 + 3p/2 + 15p^2/4 + 105p^3/8 + 945p^4/16),
+// q = conj(z) r (= 1/z unclamped), p = q^2.
+__device__ __forceinline__ U3 series5(float x, float y, float r) {
+  const float qr = x * r, qi = -y * r;
+  const float pr = qr * qr - qi * qi, pi_ = 2.f * qr * qi;
+  float ar = 6.5625f, ai = 0.f, tr;
+  tr = ar * pr - ai * pi_ + 1.875f; ai = ar * pi_ + ai * pr; ar = tr;
+  tr = ar * pr - ai * pi_ + 0.75f;  ai = ar * pi_ + ai * pr; ar = tr;
+  tr = ar * pr - ai * pi_ + 0.5f;   ai = ar * pi_ + ai * pr; ar = tr;
+  tr = ar * pr - ai * pi_ + 1.0f;   ai = ar * pi_ + ai * pr; ar = tr;
+  float br = 59.0625f, bi = 0.f;
+  tr = br * pr - bi * pi_ + 13.125f; bi = br * pi_ + bi * pr; br = tr;
+  tr = br * pr - bi * pi_ + 3.75f;   bi = br * pi_ + bi * pr; br = tr;
+  tr = br * pr - bi * pi_ + 1.5f;    bi = br * pi_ + bi * pr; br = tr;
+  tr = br * pr - bi * pi_ + 1.0f;    bi = br * pi_ + bi * pr; br = tr;
+  const float xi = qr * ai + qi * ar;           // Im(q P1)
+  const float yr = pr * br - pi_ * bi;          // Re(p P2)
+  const float yi = pr * bi + pi_ * br;          // Im(p P2)
+  const float k = float(INV_SQRT_PI);
+  U3 o;
+  o.u = -k * xi;      // Re w  = -Im(q P1) / sqrt(pi)
+  o.ux = k * yi;      // Re w' =  Im(p P2) / sqrt(pi)
+  o.uy = k * yr;      // -Im w' = Re(p P2) / sqrt(pi)
+  return o;
+}
+
+// Accurate u, u_x, u_y for |z|^2 < MID_Z2 (continued fraction or Weideman).
+__device__ __noinline__ U3 near3(float x, float y, float z2) {
+  double wr, wi;
+  if (z2 >= CORE_Z2 && y >= 0.f) {
+    const int depth = cf_depth<float>(z2);
+    float rr = 0.f, ri = 0.f;
+    for (int n = depth - 1; n >= 0; --n) {
+      const float cr = y + float(n + 1) * rr;
+      const float ci = -x + float(n + 1) * ri;
+      const float inv = __fdividef(0.5f, cr * cr + ci * ci);
+      rr = cr * inv;
+      ri = -ci * inv;
+    }
+    wr = TWO_INV_SQRT_PI * rr;
+    wi = TWO_INV_SQRT_PI * ri;
+    if (y < 0.1f) wr += exp(fmin((double)y * y - (double)x * x, 0.0)) * cos(2.0 * x * y);
+  } else if (y >= 0.f) {
+    const cpx<double> w = weideman_upper(x, y);
+    wr = w.re;
+    wi = w.im;
+  } else {
+    const cpx<double> wm = weideman_upper(-(double)x, -(double)y);
+    const double e = 2.0 * exp((double)y * y - (double)x * x);
+    wr = e * cos(2.0 * x * y) - wm.re;
+    wi = -e * sin(2.0 * x * y) - wm.im;
+  }
+  const double dr = -2.0 * (x * wr - y * wi);                         // w' = -2 z w + 2i/sqrt(pi)
+  const double di = -2.0 * (x * wi + y * wr) + TWO_INV_SQRT_PI;
+  U3 o;
+  o.u = (float)wr;
+  o.ux = (float)dr;
+  o.uy = (float)(-di);
+  return o;
+}
+
+__device__ __forceinline__ U3 value3(float x, const JLine& L) {
+  const float z2 = fmaf(x, x, L.h.y);
+  if (z2 >= MID_Z2) return series5(x, L.h.x, rcp_approx(z2));
+  return near3(x, L.h.x, z2);
+}
+
+__device__ __forceinline__ void add3(float* a, const U3& v, float x, const JLine& L) {
+  a[0] = fmaf(L.g.w, v.u, a[0]);
+  a[1] = fmaf(L.h.z, v.u, fmaf(-L.h.w * x, v.ux, fmaf(-L.k.x, v.uy, a[1])));
+  a[2] = fmaf(L.k.y, v.u, fmaf(L.k.z, v.uy, fmaf(-L.k.w, v.ux, a[2])));
+}
+
+__device__ __forceinline__ void kahan3(float* sum, float* comp, const float* v) {
+#pragma unroll
+  for (int q = 0; q < 3; ++q) {
+    const float yk = v[q] - comp[q];
+    const float t = sum[q] + yk;
+    comp[q] = (t - sum[q]) - yk;
+    sum[q] = t;
+  }
+}
+
+__device__ __forceinline__ float clenshaw_k(const float* c, float t) {
+  float b1 = 0.f, b2 = 0.f;
+  const float t2 = 2.f * t;
+#pragma unroll
+  for (int k = MJ_K - 1; k >= 1; --k) {
+    const float b0 = fmaf(t2, b1, c[k] - b2);
+    b2 = b1;
+    b1 = b0;
+  }
+  return fmaf(t, b1, 0.5f * c[0] - b2);
+}
+
+__global__ void __launch_bounds__(MJ_THREADS, 1)
+jac_ml_kernel(const LineF32* __restrict__ prep, const LineJac* __restrict__ jprep, int n_lines,
+              const int2* __restrict__ ranges, const double* __restrict__ t_layer, double nu_min, double step,
+              long long n_nu, int tile_samples, int chunks_per_tile, double cutoff, float* __restrict__ od,
+              float* __restrict__ d_t, float* __restrict__ d_v, int n_lay, const double* __restrict__ g_tau,
+              double* __restrict__ vjp_t, double* __restrict__ vjp_v) {
+  constexpr int P = MJ_P;
+  __shared__ JLine s1[MJ_THREADS];
+  __shared__ JLine s2[MJ_THREADS];
+  __shared__ unsigned char s_l2[MJ_THREADS / 32][MJ_THREADS];
+  __shared__ unsigned char s_l3[MJ_THREADS / 32][MJ_THREADS];
+  __shared__ int s_cnt[3][MJ_THREADS / 32];
+  __shared__ int s_seg_start[MJ_THREADS + 1];
+  __shared__ short s_seg_lo[MJ_THREADS];
+  __shared__ unsigned char s_seg_mask[MJ_THREADS];
+  __shared__ float s_core[3][MJ_CHUNK];
+  __shared__ float s_c1[3][MJ_K];
+  __shared__ float s_c2[MJ_THREADS / 32][3][MJ_K];
+  // the level-1 line records are dead after the last round; their space holds the reductions
+  double (*s_red)[MJ_THREADS] = reinterpret_cast<double (*)[MJ_THREADS]>(&s1[0]);
+  static_assert(sizeof(s1) >= 3 * MJ_THREADS * sizeof(double), "reduction buffer");
+
+  const int row = blockIdx.y;
+  const int tile = blockIdx.x / chunks_per_tile, chunk = blockIdx.x % chunks_per_tile;
+  const long long t0 = (long long)tile * tile_samples;
+  const long long t1 = min(t0 + (long long)tile_samples, n_nu);
+  const long long c0 = t0 + (long long)chunk * (blockDim.x * P);
+  if (c0 >= t1) return;
+  const int n_c = (int)(min(c0 + (long long)(blockDim.x * P), t1) - c0);
+  const double wlo = __dsub_rn(grid_nu(nu_min, step, t0), cutoff);
+  const double whi = __dadd_rn(grid_nu(nu_min, step, t1 - 1), cutoff);
+  const int2 rng = ranges[tile];
+  const LineF32* lp = prep + (long long)row * n_lines;
+  const LineJac* jp = jprep + (long long)row * n_lines;
+
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, n_warps = blockDim.x >> 5;
+  const float H1 = 0.5f * (float)(n_c - 1), C1 = H1;
+  const bool use_l1 = H1 >= MJ_MIN_H1;
+  const int w0 = warp * MJ_WARP_PTS;
+  const int n_w = max(0, min(MJ_WARP_PTS, n_c - w0));
+  const float H2 = 0.5f * (float)(n_w - 1), C2w = (float)w0 + H2;
+  const bool use_l2 = H2 >= MJ_MIN_H2;
+  const float xn1 = H1 * (float)cospi((2.0 * (tid & 15) + 1.0) / (2.0 * MJ_K));
+  const float xn2 = H2 * (float)cospi((2.0 * (lane & 15) + 1.0) / (2.0 * MJ_K));
+  const float pf = (float)(w0 + lane * P);
+
+  for (int i = tid; i < 3 * MJ_CHUNK; i += blockDim.x) (&s_core[0][0])[i] = 0.f;
+
+  float acc[3][P];
+#pragma unroll
+  for (int q = 0; q < 3; ++q)
+#pragma unroll
+    for (int m = 0; m < P; ++m) acc[q][m] = 0.f;
+  float sum1[3] = {0.f, 0.f, 0.f}, comp1[3] = {0.f, 0.f, 0.f};
+  float sum2[3] = {0.f, 0.f, 0.f}, comp2[3] = {0.f, 0.f, 0.f};
+
+  for (int base = rng.x; base < rng.y; base += blockDim.x) {
+    const int li = base + tid;
+    const bool have = li < rng.y;
+    LineF32 L;
+    LineJac J;
+    if (have) {
+      L = lp[li];
+      J = jp[li];
+    }
+    const bool pass = have && (L.nuc >= wlo) && (L.nuc <= whi);
+    const float jf = (float)((long long)L.j0 - c0);
+    const bool lev1 = pass && use_l1 && (fabsf(jf - C1) - H1 > H1 + 1.f);
+    const bool inner = pass && !lev1;
+    const float y2 = L.y * L.y;
+    const float hw = (y2 >= MID_Z2 && L.y >= 0.f) ? -1.0f : sqrtf(fmaxf(MID_Z2 - y2, 0.f)) / L.a + 1.0f;
+    int near_lo = 0, near_n = 0;
+    unsigned l3mask = 0;
+    if (inner) {
+      for (int w = 0; w < n_warps; ++w) {              // same test as the per-warp split below
+        const int nw = min(MJ_WARP_PTS, n_c - w * MJ_WARP_PTS);
+        if (nw <= 0) break;
+        const float h2 = 0.5f * (float)(nw - 1);
+        const bool l2 = h2 >= MJ_MIN_H2 && fabsf(jf - ((float)(w * MJ_WARP_PTS) + h2)) - h2 > h2 + 1.f;
+        if (!l2) l3mask |= 1u << w;
+      }
+    }
+    if (inner && hw >= 0.f && l3mask) {
+      const float q = jf + L.b / L.a;
+      const float lo_f = fmaxf(ceilf(q - hw), 0.f);
+      const float hi_f = fminf(floorf(q + hw), (float)(n_c - 1));
+      if (lo_f <= hi_f) {
+        near_lo = (int)lo_f;
+        near_n = (int)hi_f - near_lo + 1;
+      }
+    }
+    int near_scan = near_n;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int t = __shfl_up_sync(0xffffffffu, near_scan, o);
+      if (lane >= o) near_scan += t;
+    }
+    const unsigned b1 = __ballot_sync(0xffffffffu, lev1), b2 = __ballot_sync(0xffffffffu, inner);
+    if (lane == 0) {
+      s_cnt[0][warp] = __popc(b1);
+      s_cnt[1][warp] = __popc(b2);
+    }
+    if (lane == 31) s_cnt[2][warp] = near_scan;
+    __syncthreads();
+    int off1 = 0, off2 = 0, off3 = 0, n1 = 0, n2 = 0, n_near = 0;
+    for (int w = 0; w < n_warps; ++w) {
+      const int a1 = s_cnt[0][w], a2 = s_cnt[1][w], a3 = s_cnt[2][w];
+      off1 += (w < warp) ? a1 : 0;
+      off2 += (w < warp) ? a2 : 0;
+      off3 += (w < warp) ? a3 : 0;
+      n1 += a1;
+      n2 += a2;
+      n_near += a3;
+    }
+    if (pass) {
+      JLine r;
+      r.g = make_float4(lev1 ? C1 - jf : jf, L.a, L.b, L.amp);
+      r.h = make_float4(L.y, y2, J.jT_u, J.jT_x);
+      r.k = make_float4(J.jT_y, J.jv_u, J.jv_y, J.jv_x);
+      const unsigned lt = (1u << lane) - 1u;
+      if (lev1) {
+        s1[off1 + __popc(b1 & lt)] = r;
+      } else {
+        const int slot = off2 + __popc(b2 & lt);
+        s2[slot] = r;
+        s_seg_start[slot] = off3 + near_scan - near_n;
+        s_seg_lo[slot] = (short)near_lo;
+        s_seg_mask[slot] = (unsigned char)l3mask;
+      }
+    }
+    if (tid == 0) s_seg_start[n2] = n_near;
+    __syncthreads();
+
+    // level 1: thread (tid & 15) evaluates its node for lines tid>>4, +16, ...
+    {
+      float a[3] = {0.f, 0.f, 0.f};
+      for (int l = tid >> 4; l < n1; l += (blockDim.x >> 4)) {
+        const JLine R = s1[l];
+        const float x = fmaf(xn1 + R.g.x, R.g.y, -R.g.z);
+        add3(a, value3(x, R), x, R);
+      }
+      kahan3(sum1, comp1, a);
+    }
+    // per-warp split of the inner lines into level 2 and level 3
+    int n2w = 0, n3w = 0;
+    for (int k = 0; k < n2; k += 32) {
+      const int l = k + lane;
+      bool is2 = false, is3 = false;
+      if (l < n2) {
+        const float d = fabsf(s2[l].g.x - C2w) - H2;
+        is2 = use_l2 && d > H2 + 1.f;
+        is3 = !is2 && n_w > 0;
+      }
+      const unsigned q2 = __ballot_sync(0xffffffffu, is2), q3 = __ballot_sync(0xffffffffu, is3);
+      const unsigned lt = (1u << lane) - 1u;
+      if (is2) s_l2[warp][n2w + __popc(q2 & lt)] = (unsigned char)l;
+      if (is3) s_l3[warp][n3w + __popc(q3 & lt)] = (unsigned char)l;
+      n2w += __popc(q2);
+      n3w += __popc(q3);
+    }
+    __syncwarp();
+    // level 2: half-warps take one line each, lane (& 15) = node
+    {
+      float a[3] = {0.f, 0.f, 0.f};
+      for (int i = lane >> 4; i < n2w; i += 2) {
+        const JLine R = s2[s_l2[warp][i]];
+        const float x = fmaf(xn2 + (C2w - R.g.x), R.g.y, -R.g.z);
+        add3(a, value3(x, R), x, R);
+      }
+      kahan3(sum2, comp2, a);
+    }
+    // level 3, clamped loop (branch-free)
+    for (int i = 0; i < n3w; ++i) {
+      const JLine R = s2[s_l3[warp][i]];
+      const float x0 = fmaf(pf - R.g.x, R.g.y, -R.g.z);
+#pragma unroll
+      for (int m = 0; m < P; ++m) {
+        const float x = fmaf((float)m, R.g.y, x0);
+        const U3 v = series5(x, R.h.x, rcp_approx(fmaxf(fmaf(x, x, R.h.y), MID_Z2)));
+        float a3[3] = {acc[0][m], acc[1][m], acc[2][m]};
+        add3(a3, v, x, R);
+        acc[0][m] = a3[0];
+        acc[1][m] = a3[1];
+        acc[2][m] = a3[2];
+      }
+    }
+    // level 3, near correction (accurate - clamped) spread over the CTA; x is
+    // formed exactly as in the loop above, so the clamped values cancel
+    {
+      int l = 0;
+      for (int i = tid; i < n_near; i += blockDim.x) {
+        while (s_seg_start[l + 1] <= i) ++l;
+        const int p = s_seg_lo[l] + (i - s_seg_start[l]);
+        if (!((s_seg_mask[l] >> (p / MJ_WARP_PTS)) & 1u)) continue;
+        const JLine R = s2[l];
+        const float x0 = fmaf((float)(p & ~(P - 1)) - R.g.x, R.g.y, -R.g.z);
+        const float x = fmaf((float)(p & (P - 1)), R.g.y, x0);
+        const float z2 = fmaf(x, x, R.h.y);
+        if (z2 >= MID_Z2) continue;
+        const U3 good = near3(x, R.h.x, z2);
+        const U3 clamped = series5(x, R.h.x, rcp_approx(fmaxf(z2, MID_Z2)));
+        float a[3] = {0.f, 0.f, 0.f}, b[3] = {0.f, 0.f, 0.f};
+        add3(a, good, x, R);
+        add3(b, clamped, x, R);
+        atomicAdd(&s_core[0][p], a[0] - b[0]);
+        atomicAdd(&s_core[1][p], a[1] - b[1]);
+        atomicAdd(&s_core[2][p], a[2] - b[2]);
+      }
+    }
+    __syncthreads();
+  }
+
+  // level-1 node values (reduce the 16-thread groups) and Chebyshev coefficients
+#pragma unroll
+  for (int q = 0; q < 3; ++q) s_red[q][tid] = (double)sum1[q] - (double)comp1[q];
+  __syncthreads();
+  if (tid < 3 * MJ_K) {
+    const int q = tid / MJ_K, j = tid % MJ_K;
+    double f = 0.0;
+    for (int i = j; i < (int)blockDim.x; i += MJ_K) f += s_red[q][i];
+    s_red[q][j] = f;   // read back after the barrier, only entries < MJ_K
+  }
+  __syncthreads();
+  if (tid < 3 * MJ_K) {
+    const int q = tid / MJ_K, k = tid % MJ_K;
+    double c = 0.0;
+    for (int j = 0; j < MJ_K; ++j) c += s_red[q][j] * cospi((double)k * (2.0 * j + 1.0) / (2.0 * MJ_K));
+    s_c1[q][k] = use_l1 ? (float)(c * (2.0 / MJ_K)) : 0.f;
+  }
+  // level-2 node values of this warp: lanes j and j+16 hold halves of node j
+#pragma unroll
+  for (int q = 0; q < 3; ++q) {
+    float f2 = sum2[q] - comp2[q];
+    f2 += __shfl_xor_sync(0xffffffffu, f2, 16);
+    double c = 0.0;
+    for (int j = 0; j < MJ_K; ++j) {
+      const float fj = __shfl_sync(0xffffffffu, f2, j);
+      c += (double)fj * cospi((double)(lane & 15) * (2.0 * j + 1.0) / (2.0 * MJ_K));
+    }
+    if (lane < MJ_K) s_c2[warp][q][lane] = use_l2 ? (float)(c * (2.0 / MJ_K)) : 0.f;
+  }
+  __syncthreads();
+
+  const double T = t_layer[row];
+  const float inv_h1 = use_l1 ? 1.0f / H1 : 0.f, inv_h2 = use_l2 ? 1.0f / H2 : 0.f;
+  const double* g = g_tau ? g_tau + (long long)(row / n_lay) * n_nu : nullptr;
+  double pt = 0.0, pv = 0.0;
+#pragma unroll
+  for (int m = 0; m < P; ++m) {
+    const int pl = w0 + lane * P + m;
+    if (pl >= n_c) continue;
+    double v[3];
+#pragma unroll
+    for (int q = 0; q < 3; ++q) {
+      float s = s_core[q][pl];
+      if (use_l1) s += clenshaw_k(s_c1[q], ((float)pl - C1) * inv_h1);
+      if (use_l2) s += clenshaw_k(s_c2[warp][q], ((float)pl - C2w) * inv_h2);
+      v[q] = (double)acc[q][m] + (double)s;
+    }
+    const long long p = c0 + pl;
+    const double nu = grid_nu(nu_min, step, p);
+    const double hv = 0.5 * C2 * nu / T;
+    const double R = nu * tanh(hv);
+    const double ch = cosh(hv);
+    const double R_T = -nu * (hv / T) / (ch * ch);          // dR/dT
+    const double jt = R_T * v[0] + R * v[1], jv = R * v[2];
+    if (g) {                      // vector-Jacobian product with d loss / d tau
+      pt += g[p] * jt;
+      pv += g[p] * jv;
+    } else {
+      const long long o = (long long)row * n_nu + p;
+      od[o] = (float)(v[0] * R);
+      d_t[o] = (float)jt;
+      d_v[o] = (float)jv;
+    }
+  }
+  if (g) {
+    for (int o = 16; o > 0; o >>= 1) {
+      pt += __shfl_xor_sync(0xffffffffu, pt, o);
+      pv += __shfl_xor_sync(0xffffffffu, pv, o);
+    }
+    if (lane == 0) {
+      s_red[0][warp] = pt;
+      s_red[1][warp] = pv;
+    }
+    __syncthreads();
+    if (tid == 0) {
+      double a = 0.0, b = 0.0;
+      for (int w = 0; w < n_warps; ++w) {
+        a += s_red[0][w];
+        b += s_red[1][w];
+      }
+      atomicAdd(&vjp_t[row], a);
+      atomicAdd(&vjp_v[row], b);
+    }
+  }
+}
+
+}  // namespace lbl
+
+using namespace lbl;
+
+extern "C" int lbl_jacobian_ml_f32(const LineF32* prep, const LineJac* jprep, int n_lines, const int* ranges,
+                                   const double* t_layer, int n_rows, int n_lay, double nu_min, double step,
+                                   long long n_nu, int tile_samples, double cutoff, float* od, float* d_t,
+                                   float* d_v, const double* g_tau, double* vjp_t, double* vjp_v, void* stream) {
+  const bool vjp = g_tau != nullptr;
+  if (!prep || !jprep || !ranges || !t_layer || n_lines < 1 || n_rows < 1 || n_lay < 1 || n_rows % n_lay ||
+      n_rows > 65535 || n_nu < 1 || tile_samples < 1 || !(step > 0) || !(cutoff >= 0) ||
+      (vjp ? (!vjp_t || !vjp_v) : (!od || !d_t || !d_v)))
+    return lbl_set_error(LBL_EINVAL, "lbl_jacobian_ml_f32: bad arguments");
+  const int per_tile = tile_samples < MJ_CHUNK ? tile_samples : MJ_CHUNK;
+  const int threads = 32 * ((per_tile + MJ_WARP_PTS - 1) / MJ_WARP_PTS);
+  const int cp = threads * MJ_P;
+  const long long n_tiles = (n_nu + tile_samples - 1) / tile_samples;
+  const long long chunks = (tile_samples + cp - 1) / cp;
+  if (n_tiles * chunks > 0x7fffffffLL) return lbl_set_error(LBL_EINVAL, "lbl_jacobian_ml_f32: grid too large");
+  dim3 grid((unsigned)(n_tiles * chunks), (unsigned)n_rows);
+  jac_ml_kernel<<<grid, threads, 0, (cudaStream_t)stream>>>(prep, jprep, n_lines, (const int2*)ranges, t_layer,
+                                                             nu_min, step, n_nu, tile_samples, (int)chunks, cutoff,
+                                                             od, d_t, d_v, n_lay, g_tau, vjp_t, vjp_v);
+  return lbl_check_launch("lbl_jacobian_ml_f32");
+}

@@ -306,6 +306,86 @@ class Job:
         self.h2d_bytes += t.numel() * t.element_size()
         return t
 
+    def _device_lines(self, stream):
+        """Layers, per-(layer, group) records, band mask + sort, gather and tile ranges.
+
+        Returns (t_layer, layer_groups, lines, n_kept, ranges, n_grp), or None when
+        no line lies in the band.
+        """
+        torch, dev = self.torch, self.dev
+        grid = self.grid
+        n_prof, n_lay, n_nu = self.n_prof, self.n_lay, grid.n_nu
+        n_rows = n_prof * n_lay
+        n_gas = len(self.layers.gases)
+        if self.lv is not None:
+            lp, lt, lv = self.lv
+            p_atm = torch.empty((n_prof, n_lay), dtype=torch.float64, device=dev)
+            t_lay = torch.empty_like(p_atm)
+            v_lay = torch.empty((n_prof, n_gas, n_lay), dtype=torch.float64, device=dev)
+            col = torch.empty_like(v_lay)
+            _lib.call("lbl_build_layers", lp.data_ptr(), lt.data_ptr(), lv.data_ptr(), n_prof, n_lay + 1, n_gas,
+                      COLUMN_FACTOR, p_atm.data_ptr(), t_lay.data_ptr(), v_lay.data_ptr(), col.data_ptr(),
+                      stream)
+            self.launches += 1
+        else:
+            p_atm, t_lay, v_lay, col = self.lay
+        # per (layer, group)
+        n_grp = len(self.groups)
+        grp_gas, grp_mass, tips_off, tips_len, tips_t, tips_q = self.grp
+        lg = torch.empty((n_rows * n_grp * _lib.SIZEOF_LAYER_GROUP // 8,), dtype=torch.float64, device=dev)
+        _lib.call("lbl_layer_groups", t_lay.data_ptr(), p_atm.data_ptr(), v_lay.data_ptr(), col.data_ptr(),
+                  n_prof, n_lay, n_gas, n_grp, grp_gas.data_ptr(), grp_mass.data_ptr(), tips_off.data_ptr(),
+                  tips_len.data_ptr(), tips_t.data_ptr(), tips_q.data_ptr(), lg.data_ptr(), stream)
+        self.launches += 1
+        # lines: mask, sort, gather
+        d_nu0, d_sref, d_gair, d_gself, d_elow, d_nair, d_shift = self.lines_in
+        n_lines = self.n_lines
+        ws_bytes = _lib.load().lbl_sort_workspace_bytes(n_lines)
+        ws = torch.empty((ws_bytes + 7) // 8, dtype=torch.float64, device=dev)
+        order = torch.empty(n_lines, dtype=torch.int32, device=dev)
+        kept = torch.empty(1, dtype=torch.int32, device=dev)
+        max_sb = torch.empty(1, dtype=torch.float64, device=dev)
+        _lib.call("lbl_sort_lines", d_nu0.data_ptr(), d_shift.data_ptr(), self.gid.data_ptr(), n_lines,
+                  self.nu_first - self.cutoff, self.nu_last + self.cutoff, self.p_max, ws.data_ptr(), ws_bytes,
+                  order.data_ptr(), kept.data_ptr(), max_sb.data_ptr(), stream)
+        self.launches += sort_launches(n_lines)
+        self._kept = kept
+        n_kept = int(kept.item())                      # one small device->host read
+        if n_kept == 0:
+            return None
+        lines = torch.empty((n_kept * _lib.SIZEOF_LINE_IN // 8,), dtype=torch.float64, device=dev)
+        _lib.call("lbl_gather_lines", d_nu0.data_ptr(), d_sref.data_ptr(), d_gair.data_ptr(), d_gself.data_ptr(),
+                  d_elow.data_ptr(), d_nair.data_ptr(), d_shift.data_ptr(), self.gid.data_ptr(), order.data_ptr(),
+                  kept.data_ptr(), n_kept, lines.data_ptr(), stream)
+        n_tiles = (n_nu + grid.tile_samples - 1) // grid.tile_samples
+        ranges = torch.empty((n_tiles, 2), dtype=torch.int32, device=dev)
+        _lib.call("lbl_tile_ranges", lines.data_ptr(), kept.data_ptr(), grid.nu_min, grid.step, n_nu,
+                  grid.tile_samples, self.cutoff, self.pad, n_tiles, ranges.data_ptr(), stream)
+        self.launches += 2
+        return t_lay, lg, lines, n_kept, ranges, n_grp
+
+    def _raise_on_error(self, err, n_grp: int) -> None:
+        """FloatingPointError for the first failing (layer, group) of the device error word."""
+        key = int(err.item())
+        if key != INT_MAX:
+            row, g = divmod(key, n_grp + 1)
+            k = row % self.n_lay
+            if g < n_grp:
+                raise FloatingPointError(
+                    f"Layer {k}, gas '{self.groups[g].gas}': non-finite or negative line strength")
+            raise FloatingPointError(f"Layer {k}: non-finite optical depth after radiation term")
+
+    def jacobian(self, gas: str = "H2O", g_tau=None):
+        """Per-layer Jacobians of the float32 multi-level engine.
+
+        Returns device tensors (od, d tau/dT_layer, d tau/dlnVMR_layer of ``gas``),
+        each [n_prof, n_lay, n_nu] float32; with ``g_tau`` ([n_prof, n_nu]) returns
+        instead the vector-Jacobian products (sum_nu g dtau/dT, sum_nu g dtau/dlnVMR),
+        each [n_prof, n_lay] float64, without storing the Jacobian.
+        """
+        self.launches = 0
+        return _jacobian_impl(self, gas, g_tau)
+
     def run(self, precision: str = "fp32", mu: Optional[Sequence[float]] = None, want_od: bool = True,
             want_tau: bool = False, want_trans: bool = False, count_evals: bool = False,
             timer: Optional[dict] = None, channels: Optional[Tuple[int, int]] = None) -> EngineResult:
@@ -352,53 +432,11 @@ class Job:
 
         if self.empty:
             return finish(torch.zeros((n_prof, n_lay, n_nu), dtype=od_dtype, device=dev))
-
-        # layers
-        n_gas = len(self.layers.gases)
-        if self.lv is not None:
-            lp, lt, lv = self.lv
-            p_atm = torch.empty((n_prof, n_lay), dtype=torch.float64, device=dev)
-            t_lay = torch.empty_like(p_atm)
-            v_lay = torch.empty((n_prof, n_gas, n_lay), dtype=torch.float64, device=dev)
-            col = torch.empty_like(v_lay)
-            _lib.call("lbl_build_layers", lp.data_ptr(), lt.data_ptr(), lv.data_ptr(), n_prof, n_lay + 1, n_gas,
-                      COLUMN_FACTOR, p_atm.data_ptr(), t_lay.data_ptr(), v_lay.data_ptr(), col.data_ptr(),
-                      stream)
-            self.launches += 1
-        else:
-            p_atm, t_lay, v_lay, col = self.lay
-        # per (layer, group)
-        n_grp = len(self.groups)
-        grp_gas, grp_mass, tips_off, tips_len, tips_t, tips_q = self.grp
-        lg = torch.empty((n_rows * n_grp * _lib.SIZEOF_LAYER_GROUP // 8,), dtype=torch.float64, device=dev)
-        _lib.call("lbl_layer_groups", t_lay.data_ptr(), p_atm.data_ptr(), v_lay.data_ptr(), col.data_ptr(),
-                  n_prof, n_lay, n_gas, n_grp, grp_gas.data_ptr(), grp_mass.data_ptr(), tips_off.data_ptr(),
-                  tips_len.data_ptr(), tips_t.data_ptr(), tips_q.data_ptr(), lg.data_ptr(), stream)
-        self.launches += 1
-        # lines: mask, sort, gather
-        d_nu0, d_sref, d_gair, d_gself, d_elow, d_nair, d_shift = self.lines_in
-        n_lines = self.n_lines
-        ws_bytes = _lib.load().lbl_sort_workspace_bytes(n_lines)
-        ws = torch.empty((ws_bytes + 7) // 8, dtype=torch.float64, device=dev)
-        order = torch.empty(n_lines, dtype=torch.int32, device=dev)
-        kept = torch.empty(1, dtype=torch.int32, device=dev)
-        max_sb = torch.empty(1, dtype=torch.float64, device=dev)
-        _lib.call("lbl_sort_lines", d_nu0.data_ptr(), d_shift.data_ptr(), self.gid.data_ptr(), n_lines,
-                  self.nu_first - self.cutoff, self.nu_last + self.cutoff, self.p_max, ws.data_ptr(), ws_bytes,
-                  order.data_ptr(), kept.data_ptr(), max_sb.data_ptr(), stream)
-        self.launches += sort_launches(n_lines)
-        n_kept = int(kept.item())                      # one small device->host read
-        if n_kept == 0:
+        st = self._device_lines(stream)
+        if st is None:
             return finish(torch.zeros((n_prof, n_lay, n_nu), dtype=od_dtype, device=dev))
-        lines = torch.empty((n_kept * _lib.SIZEOF_LINE_IN // 8,), dtype=torch.float64, device=dev)
-        _lib.call("lbl_gather_lines", d_nu0.data_ptr(), d_sref.data_ptr(), d_gair.data_ptr(), d_gself.data_ptr(),
-                  d_elow.data_ptr(), d_nair.data_ptr(), d_shift.data_ptr(), self.gid.data_ptr(), order.data_ptr(),
-                  kept.data_ptr(), n_kept, lines.data_ptr(), stream)
-        n_tiles = (n_nu + grid.tile_samples - 1) // grid.tile_samples
-        ranges = torch.empty((n_tiles, 2), dtype=torch.int32, device=dev)
-        _lib.call("lbl_tile_ranges", lines.data_ptr(), kept.data_ptr(), grid.nu_min, grid.step, n_nu,
-                  grid.tile_samples, self.cutoff, self.pad, n_tiles, ranges.data_ptr(), stream)
-        self.launches += 2
+        t_lay, lg, lines, n_kept, ranges, n_grp = st
+        kept = self._kept
         # per (layer, line) prep and the Voigt sums
         err = torch.full((1,), INT_MAX, dtype=torch.int32, device=dev)
         evals = torch.zeros(4, dtype=torch.int64, device=dev) if count_evals else None
@@ -425,14 +463,7 @@ class Job:
             e1.record()
             timer.setdefault("tau_events", []).append((e0, e1))
         self.launches += 2
-        key = int(err.item())
-        if key != INT_MAX:
-            row, g = divmod(key, n_grp + 1)
-            k = row % n_lay
-            if g < n_grp:
-                raise FloatingPointError(
-                    f"Layer {k}, gas '{self.groups[g].gas}': non-finite or negative line strength")
-            raise FloatingPointError(f"Layer {k}: non-finite optical depth after radiation term")
+        self._raise_on_error(err, n_grp)
         if evals is not None:
             ev = evals.cpu().tolist()
             res.evals = int(ev[0])
@@ -442,6 +473,58 @@ class Job:
             else:
                 res.work = int(ev[0])
         return finish(od)
+
+
+def _jacobian_impl(job: Job, gas: str, g_tau=None):
+    """Device stages of Job.jacobian."""
+    torch, dev = job.torch, job.dev
+    stream = torch.cuda.current_stream().cuda_stream
+    grid = job.grid
+    n_prof, n_lay, n_nu = job.n_prof, job.n_lay, grid.n_nu
+    n_rows = n_prof * n_lay
+
+    def zeros():
+        if g_tau is not None:
+            z = torch.zeros((n_prof, n_lay), dtype=torch.float64, device=dev)
+            return z, z.clone()
+        z = torch.zeros((n_prof, n_lay, n_nu), dtype=torch.float32, device=dev)
+        return z, z.clone(), z.clone()
+
+    if job.empty:
+        return zeros()
+    st = job._device_lines(stream)
+    if st is None:
+        return zeros()
+    t_lay, lg, lines, n_kept, ranges, n_grp = st
+    err = torch.full((1,), INT_MAX, dtype=torch.int32, device=dev)
+    prep = torch.empty((n_rows * n_kept * _lib.SIZEOF_LINE_F32 // 8,), dtype=torch.float64, device=dev)
+    _lib.call("lbl_line_prep_f32", lines.data_ptr(), job._kept.data_ptr(), n_kept, lg.data_ptr(), n_rows, n_grp,
+              grid.nu_min, grid.step, prep.data_ptr(), err.data_ptr(), stream)
+    job._raise_on_error(err, n_grp)
+    mask = 0
+    for i, grp in enumerate(job.groups):
+        if grp.gas == gas:
+            mask |= 1 << i
+    _, _, tips_off, tips_len, tips_t, tips_q = job.grp
+    dlnq = torch.empty((n_rows * n_grp,), dtype=torch.float64, device=dev)
+    jprep = torch.empty((n_rows * n_kept * _lib.SIZEOF_LINE_JAC // 8,), dtype=torch.float64, device=dev)
+    _lib.call("lbl_line_prep_jac", lines.data_ptr(), n_kept, lg.data_ptr(), n_rows, n_grp, tips_off.data_ptr(),
+              tips_len.data_ptr(), tips_t.data_ptr(), tips_q.data_ptr(), mask, dlnq.data_ptr(), jprep.data_ptr(),
+              stream)
+    job.launches += 4
+    common = (prep.data_ptr(), jprep.data_ptr(), n_kept, ranges.data_ptr(), t_lay.data_ptr(), n_rows, n_lay,
+              grid.nu_min, grid.step, n_nu, grid.tile_samples, job.cutoff)
+    if g_tau is not None:
+        g = torch.as_tensor(g_tau).to(device=dev, dtype=torch.float64).reshape(n_prof, n_nu).contiguous()
+        vt = torch.zeros((n_prof, n_lay), dtype=torch.float64, device=dev)
+        vv = torch.zeros_like(vt)
+        _lib.call("lbl_jacobian_ml_f32", *common, 0, 0, 0, g.data_ptr(), vt.data_ptr(), vv.data_ptr(), stream)
+        return vt, vv
+    od = torch.empty((n_prof, n_lay, n_nu), dtype=torch.float32, device=dev)
+    d_t = torch.empty_like(od)
+    d_v = torch.empty_like(od)
+    _lib.call("lbl_jacobian_ml_f32", *common, od.data_ptr(), d_t.data_ptr(), d_v.data_ptr(), 0, 0, 0, stream)
+    return od, d_t, d_v
 
 
 def optical_depth(sd: SpectralData, layers: LayerInput, grid: Grid, cutoff: float,
