@@ -53,6 +53,7 @@ def parse():
     ap.add_argument("--precision", default="fp32", choices=["fp32", "fp32-direct", "fp64"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-adjoint", action="store_true", help="skip the Jacobian timing")
     ap.add_argument("--nu-min", type=float, default=600.0, help="grid start (smaller cases for profiling)")
     ap.add_argument("--nu-max", type=float, default=2500.0, help="grid end (smaller cases for profiling)")
     return ap.parse_args()
@@ -199,6 +200,38 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(sm)}
 
 
+def adjoint_timing(torch, steps: int = 3):
+    """Forward vs full per-layer Jacobian on one profile of the Jacobian workload.
+
+    Lines of the 200k-line set in 1000-1200 cm^-1, the 60-layer profile, grid
+    1000-1200 cm^-1 at 0.001, d/dT_layer and d/dlnVMR_layer(H2O). Times include
+    every device stage of each call (CUDA events, inputs resident).
+    """
+    from pylblrtm_b200 import engine, synthetic
+    sd = synthetic.restrict(synthetic.three_gas_lines(), 1000.0, 1200.0)
+    grid = engine.make_grid(1000.0, 1200.0, 0.001, 2.0)
+    job = engine.Job(sd, engine.layer_input_from_profile(synthetic.logp_profile()), grid, 25.0)
+    g = torch.ones((1, grid.n_nu), dtype=torch.float64, device="cuda")
+
+    def timed(fn):
+        fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(steps):
+            fn()
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / steps
+
+    fwd = timed(lambda: job.run("fp32", want_od=True))
+    jac = timed(lambda: job.jacobian("H2O"))
+    vjp = timed(lambda: job.jacobian("H2O", g_tau=g))
+    return {"workload": "lines 1000-1200 cm^-1 of the 200k-line set, 60 layers, grid 1000-1200 at 0.001",
+            "outputs": "od + d tau/dT_layer + d tau/dlnVMR_layer(H2O), [60, 200001] each",
+            "forward_ms": fwd, "jacobian_ms": jac, "vjp_ms": vjp, "jacobian_over_forward": jac / fwd}
+
+
 def fp32_peak(torch):
     """Measured float32 FMA throughput (TFLOP/s) of this GPU with lbl_probe_fma_f32."""
     from pylblrtm_b200 import _lib
@@ -298,6 +331,7 @@ def main():
             dist.destroy_process_group()
         return
     peak = fp32_peak(torch)
+    adj = None if (a.no_adjoint or world > 1) else adjoint_timing(torch)
     tau_avg = sum(tau_ms) / len(tau_ms)
     if a.precision == "fp32":
         nodes, l3, near = r0.work_split
@@ -337,6 +371,7 @@ def main():
         "clocks": clocks.summary(),
         "e2e": e2e,
         "cpu_baseline": cpu,
+        "adjoint": adj,
     }
     print(json.dumps(line), flush=True)
     if world > 1:
