@@ -206,6 +206,71 @@ int lbl_faddeeva_f64(const double* x, const double* y, long long n, double* re, 
 int lbl_faddeeva_f32(const float* x, const float* y, long long n, float* re, float* im, int mode,
                      void* stream);
 
+/* ---- surrogate network (no reference counterpart) ----
+ * The channel-transmittance surrogate (an MLP trained on this engine's own spectra)
+ * runs on one BF16 tensor-core GEMM, D[M, N] = A[M, K] . B[N, K]^T with A and B
+ * row-major bf16 (K contiguous) and float32 accumulation, whose epilogue is one of: */
+#define LBL_GEMM_F32 0          /* out_f32[z][m, n] = D (split z of n_split; partials summed by the consumer) */
+#define LBL_GEMM_BIAS_GELU 1    /* z = D + bias -> z_out (bf16); gelu(z) -> y and y_t (bf16) */
+#define LBL_GEMM_BIAS_SIGMOID 2 /* p = sigmoid(D + bias) -> out_f32; with target: dz = grad_scale * 2 (p - t) p (1 - p)
+                                   -> y and y_t (bf16, zero for n >= n_valid) and sum (p - t)^2 -> *loss */
+#define LBL_GEMM_DGELU 3        /* dz = D * gelu'(z_in) -> y and y_t (bf16) */
+
+/* Epilogue operands of lbl_gemm_bf16 (device pointers; NULL skips an optional output).
+ * Leading dimensions are in elements; y_t is written transposed ([N, M] row-major). */
+typedef struct {
+  int mode;
+  int n_valid;                  /* SIGMOID: columns >= n_valid are padding */
+  const float* bias;            /* [N] */
+  float* out_f32;               /* [M, ld_f32] (per split for LBL_GEMM_F32) */
+  long long ld_f32;
+  long long split_stride;       /* elements between split partials */
+  void* z_out;                  /* bf16 [M, ld_z] */
+  long long ld_z;
+  const void* z_in;             /* bf16 [M, ld_zin] */
+  long long ld_zin;
+  void* y;                      /* bf16 [M, ld_y] */
+  long long ld_y;
+  void* y_t;                    /* bf16 [N, ld_yt] */
+  long long ld_yt;
+  const float* target;          /* [M, ld_target] */
+  long long ld_target;
+  float grad_scale;
+  int pad0;
+  double* loss;                 /* accumulated sum of squared errors */
+} LblGemmEpilogue;
+
+/* Size of the opaque TMA descriptor (a CUtensorMap, 128 bytes). */
+size_t lbl_tensor_map_bytes(void);
+/* Encode (host call, no stream work) the TMA descriptor of a bf16 matrix [rows, cols]
+ * with row stride ld elements, for use as operand A or B of lbl_gemm_bf16. map_out is
+ * HOST memory of lbl_tensor_map_bytes(); base is device memory. rows must be a multiple
+ * of 128 and cols of 64. */
+int lbl_tensor_map_bf16(void* map_out, const void* base, long long rows, long long cols, long long ld);
+/* D = A . B^T through the maps (host memory) of A [M, K] and B [N, K]; M and N
+ * multiples of 128, K a multiple of 64 * n_split. err: device int raised to 1 if a
+ * pipeline wait timed out (the CTA's tile is then not written). */
+int lbl_gemm_bf16(const void* map_a, const void* map_b, int M, int N, int K, int n_split,
+                  const LblGemmEpilogue* ep, int* err, void* stream);
+/* Adam (bias-corrected, step >= 1) on float32 master weights w [rows, cols] (row stride
+ * ld) with moments m, v; the gradient is the in-order sum of n_split partials of g.
+ * Refreshes the bf16 copy w_bf16 [rows, ld] and its transpose wt_bf16 [cols, ld_t]
+ * when non-NULL. */
+int lbl_adam_step(float* w, float* m, float* v, const float* g, int n_split, long long split_stride, int rows,
+                  int cols, int ld, float lr, float b1, float b2, float eps, int step, void* w_bf16, void* wt_bf16,
+                  int ld_t, void* stream);
+/* out[r] = sum_c x[r, c] of a bf16 matrix (bias gradients). */
+int lbl_rowsum_bf16(const void* x, int rows, int cols, int ld, float* out, void* stream);
+/* Standardised bf16 network inputs: x[b, c] = (raw[b, c] - mean[c]) * inv_std[c] for
+ * c < cols, zero up to ld; the transposed copy x_t [ld, ld_t] when non-NULL. */
+int lbl_pack_inputs_bf16(const float* raw, int rows, int cols, const float* mean, const float* inv_std, void* x,
+                         int ld, void* x_t, int ld_t, void* stream);
+/* Ensemble gate: for each sample b, mean[b, c] over the n_mem members' predictions
+ * pred[m * member_stride + b * ld + c], est[b] = max_c of their standard deviation and
+ * flag[b] = (scale * est[b] > gate). */
+int lbl_ensemble_gate(const float* pred, int n_mem, long long member_stride, int n_samples, int ld, int n_ch,
+                      float scale, float gate, float* mean, float* est, int* flag, void* stream);
+
 /* Measurement probe (no reference counterpart): `blocks` CTAs of 256 threads
  * each run 8 chains of `iters` dependent float32 FMAs, i.e.
  * blocks * 256 * 8 * iters * 2 flops; the caller times the launch. */

@@ -27,6 +27,7 @@ _I = ctypes.c_int
 _L = ctypes.c_longlong
 _D = ctypes.c_double
 _S = ctypes.c_size_t
+_F = ctypes.c_float
 
 # name -> (restype, argtypes); every function of include/lblgpu.h
 SIGNATURES = {
@@ -53,7 +54,28 @@ SIGNATURES = {
     "lbl_faddeeva_f64": (_I, [_P, _P, _L, _P, _P, _P]),
     "lbl_faddeeva_f32": (_I, [_P, _P, _L, _P, _P, _I, _P]),
     "lbl_probe_fma_f32": (_I, [_P, _I, _I, _P]),
+    "lbl_tensor_map_bytes": (_S, []),
+    "lbl_tensor_map_bf16": (_I, [_P, _P, _L, _L, _L]),
+    "lbl_gemm_bf16": (_I, [_P, _P, _I, _I, _I, _I, _P, _P, _P]),
+    "lbl_adam_step": (_I, [_P, _P, _P, _P, _I, _L, _I, _I, _I, _F, _F, _F, _F, _I, _P, _P, _I, _P]),
+    "lbl_rowsum_bf16": (_I, [_P, _I, _I, _I, _P, _P]),
+    "lbl_pack_inputs_bf16": (_I, [_P, _I, _I, _P, _P, _P, _I, _P, _I, _P]),
+    "lbl_ensemble_gate": (_I, [_P, _I, _L, _I, _I, _I, _F, _F, _P, _P, _P, _P]),
 }
+
+# epilogue modes of lbl_gemm_bf16
+GEMM_F32, GEMM_BIAS_GELU, GEMM_BIAS_SIGMOID, GEMM_DGELU = 0, 1, 2, 3
+
+
+class GemmEpilogue(ctypes.Structure):
+    """LblGemmEpilogue of include/lblgpu.h (136 bytes)."""
+    _fields_ = [("mode", _I), ("n_valid", _I), ("bias", _P), ("out_f32", _P), ("ld_f32", _L),
+                ("split_stride", _L), ("z_out", _P), ("ld_z", _L), ("z_in", _P), ("ld_zin", _L),
+                ("y", _P), ("ld_y", _L), ("y_t", _P), ("ld_yt", _L), ("target", _P), ("ld_target", _L),
+                ("grad_scale", ctypes.c_float), ("pad0", _I), ("loss", _P)]
+
+
+SIZEOF_GEMM_EPILOGUE = 136
 
 _lock = threading.Lock()
 _lib = None

@@ -16,7 +16,7 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 PKG = os.path.dirname(HERE)
 ROOT = os.path.dirname(PKG)
-SOURCES = ["capi.cu", "prep.cu", "voigt.cu", "voigt_ml.cu", "voigt_ml_jac.cu"]
+SOURCES = ["capi.cu", "prep.cu", "voigt.cu", "voigt_ml.cu", "voigt_ml_jac.cu", "mlp.cu"]
 HEADERS = ["lbl_common.cuh", "faddeeva.cuh", "sum_common.cuh", "weideman_coeffs.h", os.path.join("..", "..", "include", "lblgpu.h")]
 LIB = os.path.join(PKG, "liblblgpu.so")
 HOST_LIB = os.path.join(PKG, "libfaddeeva_host.so")

@@ -46,6 +46,26 @@ def test_record_sizes_match_header():
     assert ctypes.sizeof(LineIn) == _lib.SIZEOF_LINE_IN
     assert ctypes.sizeof(LineF32) == _lib.SIZEOF_LINE_F32
     assert _lib.SIZEOF_LINE_F64 == 4 * 8
+    assert ctypes.sizeof(_lib.GemmEpilogue) == _lib.SIZEOF_GEMM_EPILOGUE
+
+
+def test_surrogate_host_checks():
+    lib = _lib.load()
+    assert lib.lbl_tensor_map_bytes() == 128
+    buf = ctypes.create_string_buffer(128)
+    # shape rules are checked before any driver call
+    with pytest.raises(RuntimeError, match="multiple of 128"):
+        _lib.call("lbl_tensor_map_bf16", ctypes.addressof(buf), 4096, 100, 64, 64)
+    ep = _lib.GemmEpilogue(mode=_lib.GEMM_F32)
+    with pytest.raises(RuntimeError, match="split-K needs the float32 epilogue"):
+        ep2 = _lib.GemmEpilogue(mode=_lib.GEMM_BIAS_GELU)
+        _lib.call("lbl_gemm_bf16", ctypes.addressof(buf), ctypes.addressof(buf), 128, 128, 128, 2,
+                  ctypes.addressof(ep2), 0, 0)
+    with pytest.raises(RuntimeError, match="epilogue buffers"):
+        _lib.call("lbl_gemm_bf16", ctypes.addressof(buf), ctypes.addressof(buf), 128, 128, 64, 1,
+                  ctypes.addressof(ep), 0, 0)
+    with pytest.raises(RuntimeError, match="bad arguments"):
+        _lib.call("lbl_adam_step", 0, 0, 0, 0, 1, 0, 1, 1, 1, 1e-3, 0.9, 0.999, 1e-8, 1, 0, 0, 0, 0)
 
 
 def test_host_queries_and_argument_errors():

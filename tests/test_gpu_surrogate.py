@@ -1,0 +1,268 @@
+"""Surrogate network on the device: the tcgen05 GEMM and its epilogues against torch
+float64, the training step's gradients and Adam update against the CPU oracle
+(oracle/mlp_ref.py), checkpoint/resume, the ensemble gate, and the trained gated
+surrogate against the engine it replaces."""
+
+import ctypes
+import time
+
+import numpy as np
+import pytest
+import torch
+
+from oracle import mlp_ref
+from pylblrtm_b200 import _lib, surrogate, synthetic
+
+pytestmark = pytest.mark.gpu
+
+
+def _bf(shape, gen, scale=1.0):
+    return (torch.randn(shape, generator=gen) * scale).to(torch.bfloat16).cuda()
+
+
+def _gemm(a, b, ep, n_split=1):
+    ma, mb = surrogate._Map(a), surrogate._Map(b)
+    err = torch.zeros(1, dtype=torch.int32, device="cuda")
+    _lib.call("lbl_gemm_bf16", ma.addr, mb.addr, a.shape[0], b.shape[0], a.shape[1], n_split,
+              ctypes.addressof(ep), err.data_ptr(), torch.cuda.current_stream().cuda_stream)
+    torch.cuda.synchronize()
+    assert err.item() == 0
+
+
+def _ref(a, b):
+    return a.double() @ b.double().T
+
+
+def _tol(a, b):
+    """Bound on float32 accumulation error: 2^-22 * sum_k |a_k b_k| per output."""
+    return 2.0 ** -22 * (a.double().abs() @ b.double().abs().T) + 1e-30
+
+
+@pytest.mark.parametrize("m,n,k,split", [(128, 128, 64, 1), (256, 384, 512, 1), (384, 256, 1024, 4),
+                                         (1024, 1024, 1024, 2)])
+def test_gemm_f32_matches_float64(cuda, m, n, k, split):
+    g = torch.Generator().manual_seed(m + n + k)
+    a, b = _bf((m, k), g), _bf((n, k), g)
+    out = torch.full((split, m, n), float("nan"), device="cuda")
+    ep = _lib.GemmEpilogue(mode=_lib.GEMM_F32, out_f32=out.data_ptr(), ld_f32=n, split_stride=m * n)
+    _gemm(a, b, ep, split)
+    got = out.double().sum(0)
+    assert torch.all(torch.abs(got - _ref(a, b)) <= split * _tol(a, b))
+
+
+def _bf_close(got, want, ulps=1):
+    """bf16 results equal up to `ulps` units in the last place of bf16."""
+    got, want = got.double(), want.double()
+    return bool(torch.all(torch.abs(got - want) <= ulps * 2.0 ** -7 * want.abs() + 1e-30))
+
+
+def test_gemm_bias_gelu_epilogue(cuda):
+    g = torch.Generator().manual_seed(11)
+    m, n, k = 256, 256, 256
+    a, b = _bf((m, k), g), _bf((n, k), g, 1 / 16)
+    bias = torch.randn(n, generator=g).cuda()
+    z = torch.empty((m, n), dtype=torch.bfloat16, device="cuda")
+    y = torch.empty_like(z)
+    yt = torch.empty((n, m), dtype=torch.bfloat16, device="cuda")
+    ep = _lib.GemmEpilogue(mode=_lib.GEMM_BIAS_GELU, bias=bias.data_ptr(), z_out=z.data_ptr(), ld_z=n,
+                           y=y.data_ptr(), ld_y=n, y_t=yt.data_ptr(), ld_yt=m)
+    _gemm(a, b, ep)
+    zr = (_ref(a, b) + bias.double()).float()
+    assert _bf_close(z, zr.to(torch.bfloat16))
+    assert _bf_close(y, torch.nn.functional.gelu(zr).to(torch.bfloat16), ulps=2)
+    assert torch.equal(yt, y.T)
+
+
+def test_gemm_sigmoid_loss_epilogue(cuda):
+    g = torch.Generator().manual_seed(12)
+    m, n, k, n_valid = 256, 256, 128, 200
+    a, b = _bf((m, k), g), _bf((n, k), g, 1 / 8)
+    bias = torch.randn(n, generator=g).cuda()
+    target = torch.rand((m, n_valid), generator=g).cuda()
+    p = torch.empty((m, n), device="cuda")
+    dz = torch.empty((m, n), dtype=torch.bfloat16, device="cuda")
+    dzt = torch.empty((n, m), dtype=torch.bfloat16, device="cuda")
+    loss = torch.zeros(1, dtype=torch.float64, device="cuda")
+    ep = _lib.GemmEpilogue(mode=_lib.GEMM_BIAS_SIGMOID, n_valid=n_valid, bias=bias.data_ptr(), out_f32=p.data_ptr(),
+                           ld_f32=n, target=target.data_ptr(), ld_target=n_valid, grad_scale=0.5,
+                           y=dz.data_ptr(), ld_y=n, y_t=dzt.data_ptr(), ld_yt=m, loss=loss.data_ptr())
+    _gemm(a, b, ep)
+    pr = torch.sigmoid(_ref(a, b) + bias.double())
+    assert torch.allclose(p.double(), pr, rtol=0, atol=2e-6)
+    d = pr[:, :n_valid] - target.double()
+    assert abs(loss.item() - (d * d).sum().item()) <= 1e-4 * (d * d).sum().item()
+    want = (0.5 * 2 * d * pr[:, :n_valid] * (1 - pr[:, :n_valid])).float().to(torch.bfloat16)
+    assert _bf_close(dz[:, :n_valid], want, ulps=2)
+    assert torch.count_nonzero(dz[:, n_valid:]) == 0
+    assert torch.equal(dzt, dz.T)
+
+
+def test_gemm_dgelu_epilogue(cuda):
+    g = torch.Generator().manual_seed(13)
+    m, n, k = 128, 256, 384
+    a, b = _bf((m, k), g, 1 / 4), _bf((n, k), g, 1 / 4)
+    zin = _bf((m, n), g)
+    dz = torch.empty((m, n), dtype=torch.bfloat16, device="cuda")
+    dzt = torch.empty((n, m), dtype=torch.bfloat16, device="cuda")
+    ep = _lib.GemmEpilogue(mode=_lib.GEMM_DGELU, z_in=zin.data_ptr(), ld_zin=n, y=dz.data_ptr(), ld_y=n,
+                           y_t=dzt.data_ptr(), ld_yt=m)
+    _gemm(a, b, ep)
+    zd = zin.double()
+    want = (_ref(a, b) * torch.from_numpy(mlp_ref.gelu_grad(zd.cpu().numpy())).cuda()).float().to(torch.bfloat16)
+    assert _bf_close(dz, want, ulps=2)
+    assert torch.equal(dzt, dz.T)
+
+
+def test_gemm_argument_errors(cuda):
+    a = torch.zeros((128, 64), dtype=torch.bfloat16, device="cuda")
+    ma = surrogate._Map(a)
+    ep = _lib.GemmEpilogue(mode=_lib.GEMM_F32)
+    with pytest.raises(RuntimeError, match="epilogue buffers"):
+        _lib.call("lbl_gemm_bf16", ma.addr, ma.addr, 128, 128, 64, 1, ctypes.addressof(ep), 0, 0)
+    with pytest.raises(RuntimeError, match="multiples of 128"):
+        _lib.call("lbl_gemm_bf16", ma.addr, ma.addr, 100, 128, 64, 1, ctypes.addressof(ep), 0, 0)
+    with pytest.raises(RuntimeError, match="rows must be a multiple of 128"):
+        surrogate._Map(torch.zeros((100, 64), dtype=torch.bfloat16, device="cuda"))
+
+
+def _small_net(seed=5):
+    net = surrogate.MLP(61, 200, hidden=256, depth=2, seed=seed)
+    rng = np.random.default_rng(seed)
+    raw = rng.standard_normal((256, 61)).astype(np.float32) * 3 + 1
+    target = rng.uniform(0, 1, (256, 200)).astype(np.float32)
+    net.set_normalisation(raw.mean(0), raw.std(0))
+    net.set_output_bias(target.mean(0))
+    return net, raw, target
+
+
+def _host_params(net):
+    w = [t[:nr, :kr].cpu().numpy() for t, (kr, nr) in zip(net.w, net.real)]
+    b = [t[:nr].cpu().numpy() for t, (_, nr) in zip(net.b, net.real)]
+    return w, b
+
+
+def test_training_gradients_match_oracle(cuda):
+    net, raw, target = _small_net()
+    w, b = _host_params(net)
+    loss, dw, db = net.gradients(torch.from_numpy(raw).cuda(), torch.from_numpy(target).cuda())
+    sse, p, dw_ref, db_ref = mlp_ref.forward_backward(raw, target, net.mean.cpu().numpy(), net.inv_std.cpu().numpy(),
+                                                      w, b, grad_scale=1.0 / 256)
+    assert abs(loss - sse / (256 * 200)) <= 1e-5 * sse / (256 * 200)
+    for l in range(len(dw)):
+        g, r = dw[l].double().cpu().numpy(), dw_ref[l]
+        assert np.linalg.norm(g - r) <= 2e-3 * np.linalg.norm(r), l
+        g, r = db[l].double().cpu().numpy(), db_ref[l]
+        assert np.linalg.norm(g - r) <= 2e-3 * np.linalg.norm(r), l
+    # inference output = the oracle's sigmoid output
+    out = net.predict(torch.from_numpy(raw).cuda()).double().cpu().numpy()
+    assert np.max(np.abs(out - p)) < 2e-5
+
+
+def test_adam_step_matches_oracle(cuda):
+    net, raw, target = _small_net(6)
+    w0, b0 = _host_params(net)
+    _, dw, db = net.gradients(torch.from_numpy(raw).cuda(), torch.from_numpy(target).cuda())
+    ws = net.workspace(256, True)
+    net._adam(ws, torch.cuda.current_stream().cuda_stream, 1e-3)
+    w1, b1 = _host_params(net)
+    for l in range(len(w0)):
+        wr, _, _ = mlp_ref.adam(w0[l], 0 * w0[l], 0 * w0[l], dw[l].cpu().numpy(), 1, 1e-3)
+        np.testing.assert_allclose(w1[l], wr, rtol=0, atol=1e-7)
+        br, _, _ = mlp_ref.adam(b0[l], 0 * b0[l], 0 * b0[l], db[l].cpu().numpy(), 1, 1e-3)
+        np.testing.assert_allclose(b1[l], br, rtol=0, atol=1e-7)
+        assert torch.equal(net.w_bf[l], net.w[l].to(torch.bfloat16))
+        assert torch.equal(net.wt_bf[l], net.w[l].T.to(torch.bfloat16))
+
+
+def _toy_data(n, seed=0):
+    rng = np.random.default_rng(seed)
+    x = rng.standard_normal((n, 61)).astype(np.float32)
+    a = rng.standard_normal((61, 200)) / 8
+    y = 1 / (1 + np.exp(-np.sin(x @ a) * 2))
+    return x, y.astype(np.float32)
+
+
+def test_training_reduces_loss_and_resume_is_exact(cuda):
+    x, y = _toy_data(4096)
+    cfg = surrogate.TrainConfig(batch=512, steps=300, lr=2e-3, warmup=20, seed=3)
+
+    def fresh():
+        net = surrogate.MLP(61, 200, hidden=256, depth=2, seed=1)
+        net.set_normalisation(x.mean(0), x.std(0))
+        net.set_output_bias(y.mean(0))
+        return net, surrogate.Trainer(net, x, y, cfg)
+
+    net, tr = fresh()
+    tr.run(40)
+    ck = tr.state_dict()
+    tr.run()
+    losses = tr.losses
+    assert np.mean(losses[-20:]) < 0.25 * np.mean(losses[:5])
+    net2, tr2 = fresh()
+    tr2.load_state_dict(ck)
+    tr2.run()
+    for a, b in zip(net.w, net2.w):
+        assert torch.equal(a, b)
+    assert tr2.losses[-10:] == losses[-10:]
+
+
+def test_ensemble_gate_matches_numpy(cuda):
+    g = torch.Generator().manual_seed(4)
+    n_mem, B, ld, n_ch = 4, 300, 256, 200
+    pred = torch.rand((n_mem, B, ld), generator=g).cuda()
+    pred[:, :150] = pred[0:1, :150] + 1e-4 * pred[:, :150]       # tight members for half the samples
+    mean = torch.empty((B, n_ch), device="cuda")
+    est = torch.empty(B, device="cuda")
+    flag = torch.empty(B, dtype=torch.int32, device="cuda")
+    _lib.call("lbl_ensemble_gate", pred.data_ptr(), n_mem, B * ld, B, ld, n_ch, 2.0, 1e-3, mean.data_ptr(),
+              est.data_ptr(), flag.data_ptr(), 0)
+    torch.cuda.synchronize()
+    p = pred[:, :, :n_ch].double().cpu().numpy()
+    np.testing.assert_allclose(mean.cpu().numpy(), p.mean(0), rtol=1e-6)
+    np.testing.assert_allclose(est.cpu().numpy(), p.std(0).max(1), rtol=1e-3, atol=1e-7)
+    np.testing.assert_array_equal(flag.cpu().numpy(), (2.0 * est.cpu().numpy() > 1e-3).astype(np.int32))
+    assert flag[:150].sum() == 0 and flag[150:].sum() == 150
+
+
+def test_gated_surrogate_against_engine(cuda):
+    """A small trained surrogate: accurate in distribution, OOD flagged, fallback exact, and faster."""
+    problem = surrogate.SurrogateProblem(nu_min=700.0, nu_max=720.0, step=0.001, channel_width=0.25)
+    sd = synthetic.restrict(synthetic.three_gas_lines(20_000), 675.0, 745.0)
+    train = surrogate.sample_profiles(4096, seed=1)
+    x = train.features()
+    y = surrogate.engine_channels(sd, train, problem, profiles_per_launch=256)
+    members = surrogate.train_ensemble(x, y, n_members=4, hidden=256, depth=2,
+                                       cfg=surrogate.TrainConfig(batch=512, steps=600, lr=2e-3, warmup=30, seed=7))
+    test_in = surrogate.sample_profiles(512, seed=2)
+    test_ood = surrogate.sample_profiles(512, seed=3, t_offset=25.0)
+    gate = surrogate.GatedSurrogate(members, gate=2e-3)
+    ref_in = surrogate.engine_channels(sd, test_in, problem)
+    ref_ood = surrogate.engine_channels(sd, test_ood, problem)
+    mean_in, est_in, flag_in = gate.ensemble(torch.from_numpy(test_in.features()).cuda())
+    _, est_ood, flag_ood = gate.ensemble(torch.from_numpy(test_ood.features()).cuda())
+    err_in = np.abs(mean_in.cpu().numpy() - ref_in).max(1)
+    # in distribution the surrogate is far better than the best input-independent guess
+    base = np.abs(y.mean(0)[None] - ref_in).max(1)
+    assert np.median(err_in) < 0.1 * np.median(base)
+    # out of distribution the ensemble disagrees more
+    assert np.median(est_ood.cpu().numpy()) > 2 * np.median(est_in.cpu().numpy())
+    assert flag_ood.float().mean() > flag_in.float().mean()
+    # the gated result equals the engine wherever it fell back
+    t = {}
+    out, _, flag = gate(sd, test_ood, problem, timings=t)
+    fb = flag.cpu().numpy()
+    assert fb.any()
+    np.testing.assert_array_equal(out.cpu().numpy()[fb], ref_ood[fb].astype(np.float32))
+    # speed: surrogate-only evaluation against the engine on the same 512 profiles
+    raw = torch.from_numpy(test_in.features()).cuda()
+    gate.ensemble(raw)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    gate.ensemble(raw)
+    torch.cuda.synchronize()
+    t_sur = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    surrogate.engine_channels(sd, test_in, problem, profiles_per_launch=512)
+    torch.cuda.synchronize()
+    t_eng = time.perf_counter() - t0
+    assert t_eng > 5 * t_sur, (t_eng, t_sur)
