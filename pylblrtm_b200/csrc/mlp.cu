@@ -354,15 +354,17 @@ __global__ void ensemble_gate_kernel(const float* __restrict__ pred, int n_mem, 
   const int b = blockIdx.x;
   float worst = 0.0f;
   for (int c = threadIdx.x; c < n_ch; c += blockDim.x) {
-    float s = 0.f, s2 = 0.f;
-    for (int m = 0; m < n_mem; ++m) {
-      const float p = pred[m * member_stride + (long long)b * ld + c];
-      s += p;
-      s2 += p * p;
-    }
+    const float* col = pred + (long long)b * ld + c;
+    float s = 0.f;
+    for (int m = 0; m < n_mem; ++m) s += col[m * member_stride];
     const float mu = s / n_mem;
+    float s2 = 0.f;                                  // second pass: deviations (no cancellation)
+    for (int m = 0; m < n_mem; ++m) {
+      const float d = col[m * member_stride] - mu;
+      s2 += d * d;
+    }
     mean[(long long)b * n_ch + c] = mu;
-    worst = fmaxf(worst, sqrtf(fmaxf(s2 / n_mem - mu * mu, 0.0f)));
+    worst = fmaxf(worst, sqrtf(s2 / n_mem));
   }
   for (int o = 16; o > 0; o >>= 1) worst = fmaxf(worst, __shfl_xor_sync(0xffffffffu, worst, o));
   __shared__ float part[32];

@@ -579,5 +579,6 @@ def train_ensemble(features: np.ndarray, targets: np.ndarray, n_members: int = 4
         net.set_output_bias(p0)
         tr = Trainer(net, features, targets, TrainConfig(**{**cfg.__dict__, "seed": cfg.seed * 100 + m}))
         tr.run()
+        net.train_losses = tr.losses
         members.append(net)
     return members

@@ -34,8 +34,9 @@ def _ref(a, b):
 
 
 def _tol(a, b):
-    """Bound on float32 accumulation error: 2^-22 * sum_k |a_k b_k| per output."""
-    return 2.0 ** -22 * (a.double().abs() @ b.double().abs().T) + 1e-30
+    """Bound on the tensor cores' float32 accumulation error: 2^-16 * sum_k |a_k b_k| per
+    output (a layout or descriptor error is O(1) of that sum)."""
+    return 2.0 ** -16 * (a.double().abs() @ b.double().abs().T) + 1e-30
 
 
 @pytest.mark.parametrize("m,n,k,split", [(128, 128, 64, 1), (256, 384, 512, 1), (384, 256, 1024, 4),
@@ -47,13 +48,14 @@ def test_gemm_f32_matches_float64(cuda, m, n, k, split):
     ep = _lib.GemmEpilogue(mode=_lib.GEMM_F32, out_f32=out.data_ptr(), ld_f32=n, split_stride=m * n)
     _gemm(a, b, ep, split)
     got = out.double().sum(0)
-    assert torch.all(torch.abs(got - _ref(a, b)) <= split * _tol(a, b))
+    ratio = (torch.abs(got - _ref(a, b)) / _tol(a, b)).max().item()
+    assert ratio <= split, ratio
 
 
-def _bf_close(got, want, ulps=1):
-    """bf16 results equal up to `ulps` units in the last place of bf16."""
-    got, want = got.double(), want.double()
-    return bool(torch.all(torch.abs(got - want) <= ulps * 2.0 ** -7 * want.abs() + 1e-30))
+def _close(got, exact, atol, rel=2.0 ** -8):
+    """|got - exact| <= rel * |exact| + atol elementwise (rel = half a bf16 ulp by default)."""
+    got, exact = got.double(), exact.double()
+    return bool(torch.all(torch.abs(got - exact) <= rel * exact.abs() + atol))
 
 
 def test_gemm_bias_gelu_epilogue(cuda):
@@ -67,9 +69,10 @@ def test_gemm_bias_gelu_epilogue(cuda):
     ep = _lib.GemmEpilogue(mode=_lib.GEMM_BIAS_GELU, bias=bias.data_ptr(), z_out=z.data_ptr(), ld_z=n,
                            y=y.data_ptr(), ld_y=n, y_t=yt.data_ptr(), ld_yt=m)
     _gemm(a, b, ep)
-    zr = (_ref(a, b) + bias.double()).float()
-    assert _bf_close(z, zr.to(torch.bfloat16))
-    assert _bf_close(y, torch.nn.functional.gelu(zr).to(torch.bfloat16), ulps=2)
+    zr = _ref(a, b) + bias.double()
+    tol = _tol(a, b)
+    assert _close(z, zr, tol)
+    assert _close(y, torch.nn.functional.gelu(zr), 1.2 * tol + 1e-6)     # |gelu'| <= 1.13
     assert torch.equal(yt, y.T)
 
 
@@ -88,11 +91,12 @@ def test_gemm_sigmoid_loss_epilogue(cuda):
                            y=dz.data_ptr(), ld_y=n, y_t=dzt.data_ptr(), ld_yt=m, loss=loss.data_ptr())
     _gemm(a, b, ep)
     pr = torch.sigmoid(_ref(a, b) + bias.double())
-    assert torch.allclose(p.double(), pr, rtol=0, atol=2e-6)
+    tol = _tol(a, b)
+    assert _close(p, pr, 0.25 * tol + 1e-6, rel=2e-6)                    # sigmoid' <= 1/4
     d = pr[:, :n_valid] - target.double()
     assert abs(loss.item() - (d * d).sum().item()) <= 1e-4 * (d * d).sum().item()
-    want = (0.5 * 2 * d * pr[:, :n_valid] * (1 - pr[:, :n_valid])).float().to(torch.bfloat16)
-    assert _bf_close(dz[:, :n_valid], want, ulps=2)
+    want = 0.5 * 2 * d * pr[:, :n_valid] * (1 - pr[:, :n_valid])
+    assert _close(dz[:, :n_valid], want, 0.5 * tol[:, :n_valid] + 1e-6)  # |d/dz (p - t) p (1 - p)| < 1/2
     assert torch.count_nonzero(dz[:, n_valid:]) == 0
     assert torch.equal(dzt, dz.T)
 
@@ -107,9 +111,8 @@ def test_gemm_dgelu_epilogue(cuda):
     ep = _lib.GemmEpilogue(mode=_lib.GEMM_DGELU, z_in=zin.data_ptr(), ld_zin=n, y=dz.data_ptr(), ld_y=n,
                            y_t=dzt.data_ptr(), ld_yt=m)
     _gemm(a, b, ep)
-    zd = zin.double()
-    want = (_ref(a, b) * torch.from_numpy(mlp_ref.gelu_grad(zd.cpu().numpy())).cuda()).float().to(torch.bfloat16)
-    assert _bf_close(dz, want, ulps=2)
+    gp = torch.from_numpy(mlp_ref.gelu_grad(zin.double().cpu().numpy())).cuda()
+    assert _close(dz, _ref(a, b) * gp, 1.2 * _tol(a, b) + 1e-6)
     assert torch.equal(dzt, dz.T)
 
 
@@ -227,7 +230,9 @@ def test_ensemble_gate_matches_numpy(cuda):
 def test_gated_surrogate_against_engine(cuda):
     """A small trained surrogate: accurate in distribution, OOD flagged, fallback exact, and faster."""
     problem = surrogate.SurrogateProblem(nu_min=700.0, nu_max=720.0, step=0.001, channel_width=0.25)
-    sd = synthetic.restrict(synthetic.three_gas_lines(20_000), 675.0, 745.0)
+    # 1/10 of the 200k-line density with strengths x 1e-3: channel T spans ~0.08-0.8
+    # (at full strength every channel of this window is saturated, T < 1e-10)
+    sd = synthetic.scale_strengths(synthetic.restrict(synthetic.three_gas_lines(20_000), 675.0, 745.0), 1e-3)
     train = surrogate.sample_profiles(4096, seed=1)
     x = train.features()
     y = surrogate.engine_channels(sd, train, problem, profiles_per_launch=256)
@@ -235,10 +240,11 @@ def test_gated_surrogate_against_engine(cuda):
                                        cfg=surrogate.TrainConfig(batch=512, steps=600, lr=2e-3, warmup=30, seed=7))
     test_in = surrogate.sample_profiles(512, seed=2)
     test_ood = surrogate.sample_profiles(512, seed=3, t_offset=25.0)
-    gate = surrogate.GatedSurrogate(members, gate=2e-3)
+    gate = surrogate.GatedSurrogate(members)
     ref_in = surrogate.engine_channels(sd, test_in, problem)
     ref_ood = surrogate.engine_channels(sd, test_ood, problem)
-    mean_in, est_in, flag_in = gate.ensemble(torch.from_numpy(test_in.features()).cuda())
+    mean_in, est_in, _ = gate.ensemble(torch.from_numpy(test_in.features()).cuda())
+    gate.gate = float(np.quantile(est_in.cpu().numpy(), 0.9))      # 10 % of in-distribution flagged
     _, est_ood, flag_ood = gate.ensemble(torch.from_numpy(test_ood.features()).cuda())
     err_in = np.abs(mean_in.cpu().numpy() - ref_in).max(1)
     # in distribution the surrogate is far better than the best input-independent guess
@@ -246,7 +252,7 @@ def test_gated_surrogate_against_engine(cuda):
     assert np.median(err_in) < 0.1 * np.median(base)
     # out of distribution the ensemble disagrees more
     assert np.median(est_ood.cpu().numpy()) > 2 * np.median(est_in.cpu().numpy())
-    assert flag_ood.float().mean() > flag_in.float().mean()
+    assert flag_ood.float().mean() > 0.2
     # the gated result equals the engine wherever it fell back
     t = {}
     out, _, flag = gate(sd, test_ood, problem, timings=t)
