@@ -54,6 +54,7 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-adjoint", action="store_true", help="skip the Jacobian timing")
+    ap.add_argument("--no-surrogate", action="store_true", help="skip the gated-surrogate timing")
     ap.add_argument("--nu-min", type=float, default=600.0, help="grid start (smaller cases for profiling)")
     ap.add_argument("--nu-max", type=float, default=2500.0, help="grid end (smaller cases for profiling)")
     return ap.parse_args()
@@ -232,6 +233,32 @@ def adjoint_timing(torch, steps: int = 3):
             "forward_ms": fwd, "jacobian_ms": jac, "vjp_ms": vjp, "jacobian_over_forward": jac / fwd}
 
 
+def surrogate_timing():
+    """Gated surrogate on the 20-layer, 650-1150 cm^-1, 2,000-channel workload, reduced.
+
+    Trains the 4-member 61 -> 1024x4 -> 2000 ensemble for 1,500 steps on 8,192
+    engine spectra (the full study uses 100,000 spectra and 20,000 steps:
+    ``python -m pylblrtm_b200.surrogate_study``), evaluates 4,096 fresh + 5 % OOD
+    (+25 K) profiles against the engine, and times surrogate-only inference on
+    68,813 profiles (65,536 + 5 %), the gated workload's batch.
+    """
+    from pylblrtm_b200 import surrogate_study
+    rep = surrogate_study.run(n_train=8192, n_eval=4096, ood=0.05, steps=1500, infer_batch=68813,
+                              log=lambda *_: None)
+    th, err = rep["throughput"], rep["errors"]
+    return {"workload": "20-layer profiles, 650-1150 cm^-1 at 0.001, 2000 channels of 0.25 cm^-1, "
+                        f"{rep['problem']['lines']} lines x {rep['problem']['strength_scale']:g} strength; "
+                        "reduced training (8192 spectra, 1500 steps/member)",
+            "engine_spectra_per_s": th["engine_spectra_per_s"],
+            "surrogate_only_spectra_per_s": th["infer_batch"]["spectra_per_s"],
+            "surrogate_only_tflops": th["infer_batch"]["tflops"],
+            "surrogate_only_speedup": th["infer_batch"]["spectra_per_s"] / th["engine_spectra_per_s"],
+            "blended_spectra_per_s": th["blended_spectra_per_s"], "blended_speedup": th["speedup_blended"],
+            "flagged_in": rep["gate"]["flagged_in"], "flagged_ood": rep["gate"]["flagged_ood"],
+            "max_channel_err_in": err["surrogate_in"], "max_channel_err_gated": err["gated_all"],
+            "train_steps_per_s": rep["training"]["steps_per_s"]}
+
+
 def fp32_peak(torch):
     """Measured float32 FMA throughput (TFLOP/s) of this GPU with lbl_probe_fma_f32."""
     from pylblrtm_b200 import _lib
@@ -332,6 +359,7 @@ def main():
         return
     peak = fp32_peak(torch)
     adj = None if (a.no_adjoint or world > 1) else adjoint_timing(torch)
+    sur = None if (a.no_surrogate or world > 1) else surrogate_timing()
     tau_avg = sum(tau_ms) / len(tau_ms)
     if a.precision == "fp32":
         nodes, l3, near = r0.work_split
@@ -372,6 +400,7 @@ def main():
         "e2e": e2e,
         "cpu_baseline": cpu,
         "adjoint": adj,
+        "surrogate": sur,
     }
     print(json.dumps(line), flush=True)
     if world > 1:

@@ -48,7 +48,9 @@ def line_list(n_lines: int, problem: surrogate.SurrogateProblem, strength_scale:
 def run(n_train: int = 100_000, n_eval: int = 65_536, ood: float = 0.05, steps: int = 20_000,
         members: int = 4, batch: int = 4096, hidden: int = 1024, depth: int = 4, lr: float = 1e-3,
         strength_scale: float = 1e-4, n_lines: int = 200_000, gate: float = 1e-3, seed: int = 0,
-        profiles_per_launch: int = 256, log=print) -> dict:
+        profiles_per_launch: int = 256, infer_batch: int = 0, log=print) -> dict:
+    """The study; ``infer_batch`` > 0 also times surrogate-only inference on that many
+    fresh profiles (features only, no engine reference)."""
     import torch
     problem = surrogate.SurrogateProblem()
     sd = line_list(n_lines, problem, strength_scale)
@@ -124,6 +126,21 @@ def run(n_train: int = 100_000, n_eval: int = 65_536, ood: float = 0.05, steps: 
         "gemm_flops_per_spectrum": 2 * sum(k * n for k, n in nets[0].dims) * members,
     }
     rep["throughput"]["surrogate_tflops"] = rep["throughput"]["gemm_flops_per_spectrum"] * len(ev) / t_sur / 1e12
+    if infer_batch:
+        big = torch.as_tensor(surrogate.sample_profiles(infer_batch, seed=seed + 4).features(), device=nets[0].dev)
+        gs.ensemble(big)
+        torch.cuda.synchronize()
+        reps = 5
+        e0.record()
+        for _ in range(reps):
+            gs.ensemble(big)
+        e1.record()
+        torch.cuda.synchronize()
+        t_big = e0.elapsed_time(e1) / 1e3 / reps
+        rep["throughput"]["infer_batch"] = {
+            "profiles": infer_batch, "seconds": t_big, "spectra_per_s": infer_batch / t_big,
+            "tflops": rep["throughput"]["gemm_flops_per_spectrum"] * infer_batch / t_big / 1e12,
+            "launches": gs.launches}
     rep["gate"] = {"gate": gate, "flagged_in": float(flag_h[~is_ood].mean()),
                    "flagged_ood": float(flag_h[is_ood].mean()) if n_ood else None,
                    "n_flagged": int(flag_h.sum()), "n_eval": len(ev)}
@@ -153,10 +170,11 @@ def main(argv=None) -> None:
     ap.add_argument("--lines", type=int, default=200_000)
     ap.add_argument("--gate", type=float, default=1e-3)
     ap.add_argument("--seed", type=int, default=0)
+    ap.add_argument("--infer-batch", type=int, default=0)
     ap.add_argument("--out", default=None)
     a = ap.parse_args(argv)
     rep = run(a.train, a.eval, a.ood, a.steps, a.members, a.batch, a.hidden, a.depth, a.lr, a.strength_scale,
-              a.lines, a.gate, a.seed)
+              a.lines, a.gate, a.seed, infer_batch=a.infer_batch)
     text = json.dumps(rep, indent=1)
     print(text)
     if a.out:
