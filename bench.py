@@ -361,6 +361,26 @@ def main():
     adj = None if (a.no_adjoint or world > 1) else adjoint_timing(torch)
     sur = None if (a.no_surrogate or world > 1) else surrogate_timing()
     tau_avg = sum(tau_ms) / len(tau_ms)
+    # HBM-bound stages: algorithmic bytes / CUDA-event time
+    hbm_peak = None
+    try:
+        with open(os.path.join(os.path.dirname(os.path.abspath(__file__)), "MEASURED_PEAKS.json")) as f:
+            hbm_peak = float(json.load(f)["hbm_gbs"])
+    except (OSError, KeyError, ValueError):
+        hbm_peak = 6650.0
+    n_rows_, n_kept_, n_grp_, rec_ = timer["prep_shape"]
+    prep_ms = sum(b.elapsed_time(c) for b, c in timer["prep_events"]) / len(timer["prep_events"])
+    sum_ms = sum(b.elapsed_time(c) for b, c in timer["sum_events"]) / len(timer["sum_events"])
+    prep_bytes = n_rows_ * n_kept_ * rec_ + n_kept_ * 64 + n_rows_ * n_grp_ * 48
+    sum_bytes = n_rows_ * grid.n_nu * (4 if a.precision != "fp64" else 8) + grid.n_nu * 8
+    hbm = {"peak_gbs": hbm_peak, "peak_source": "MEASURED_PEAKS.json hbm_gbs (copy, burst)",
+           "line_prep": {"ms": prep_ms, "bytes": prep_bytes, "gbs": prep_bytes / prep_ms / 1e6,
+                         "frac": prep_bytes / prep_ms / 1e6 / hbm_peak,
+                         "bytes_rule": "32-B record written per (layer, line) + 64-B line record read once "
+                                       "+ 48-B layer-group record per (layer, group)"},
+           "layer_sum_exp": {"ms": sum_ms, "bytes": sum_bytes, "gbs": sum_bytes / sum_ms / 1e6,
+                             "frac": sum_bytes / sum_ms / 1e6 / hbm_peak,
+                             "bytes_rule": "od read once (4 B x layers per point) + f64 T written"}}
     if a.precision == "fp32":
         nodes, l3, near = r0.work_split
         flops = nodes * FLOPS_NODE + l3 * FLOPS_L3 + near * FLOPS_NEAR + FLOPS_CHEB_PER_POINT * grid.n_nu * 60
@@ -399,6 +419,7 @@ def main():
         "clocks": clocks.summary(),
         "e2e": e2e,
         "cpu_baseline": cpu,
+        "hbm_kernels": hbm,
         "adjoint": adj,
         "surrogate": sur,
     }

@@ -424,8 +424,14 @@ class Job:
                 tau = torch.empty((n_prof, n_nu), dtype=torch.float64, device=dev) if want_tau else None
                 tr = torch.empty((n_prof, n_nu), dtype=torch.float64, device=dev) if want_trans else None
                 fn = "lbl_layer_sum_exp_f32" if od.dtype == torch.float32 else "lbl_layer_sum_exp_f64"
+                if timer is not None:
+                    s0, s1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                    s0.record()
                 _lib.call(fn, _lib.ptr(od), n_prof, n_lay, n_nu, _lib.ptr(mu_d), _lib.ptr(tr), _lib.ptr(tau),
                           stream)
+                if timer is not None:
+                    s1.record()
+                    timer.setdefault("sum_events", []).append((s0, s1))
                 self.launches += 1
                 res.tau, res.trans = tau, tr
             return res
@@ -443,6 +449,10 @@ class Job:
         od = torch.empty((n_prof, n_lay, n_nu), dtype=od_dtype, device=dev)
         rec = _lib.SIZEOF_LINE_F32 if single else _lib.SIZEOF_LINE_F64
         prep = torch.empty((n_rows * n_kept * rec // 8,), dtype=torch.float64, device=dev)
+        if timer is not None:
+            p0, p1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            p0.record()
+            timer["prep_shape"] = (n_rows, n_kept, n_grp, rec)
         if single:
             _lib.call("lbl_line_prep_f32", lines.data_ptr(), kept.data_ptr(), n_kept, lg.data_ptr(), n_rows, n_grp,
                       grid.nu_min, grid.step, prep.data_ptr(), err.data_ptr(), stream)
@@ -450,6 +460,8 @@ class Job:
             _lib.call("lbl_line_prep_f64", lines.data_ptr(), kept.data_ptr(), n_kept, lg.data_ptr(), n_rows, n_grp,
                       prep.data_ptr(), err.data_ptr(), stream)
         if timer is not None:
+            p1.record()
+            timer.setdefault("prep_events", []).append((p0, p1))
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             e0.record()
         common = (prep.data_ptr(), n_kept, ranges.data_ptr(), t_lay.data_ptr(), n_rows, grid.nu_min, grid.step,

@@ -240,7 +240,23 @@ class MLP:
         self.mean = torch.zeros((self.n_in,), dtype=torch.float32, device=self.dev)
         self.inv_std = torch.ones((self.n_in,), dtype=torch.float32, device=self.dev)
         self._ws: Dict[Tuple[int, bool], _Workspace] = {}
+        self.group = None                 # data-parallel process group (None: one process)
+        self.world = 1
         self.refresh_bf16()
+
+    def data_parallel(self, group=None) -> "MLP":
+        """Train data-parallel over the ranks of ``group``: rank 0's parameters and
+        normalisation are broadcast, each rank's loss is scaled by 1 / (batch x world)
+        and gradients are summed (all-reduce) before every Adam step."""
+        from . import shard
+        self.group = group
+        self.world, _ = shard.world_and_rank(group)
+        if self.world > 1:
+            import torch.distributed as dist
+            for t in self.w + self.b + [self.mean, self.inv_std]:
+                dist.broadcast(t, src=dist.get_global_rank(group, 0) if group is not None else 0, group=group)
+            self.refresh_bf16()
+        return self
 
     # -- state -------------------------------------------------------------
     def refresh_bf16(self) -> None:
@@ -320,7 +336,7 @@ class MLP:
                 ep.n_valid = self.n_out
                 if train:
                     ep.target, ep.ld_target = ws.target.data_ptr(), self.n_out
-                    ep.grad_scale = 1.0 / B
+                    ep.grad_scale = 1.0 / (B * self.world)
                     ep.y, ep.ld_y = ws.dz[li].data_ptr(), n
                     ep.y_t, ep.ld_yt = ws.dzt[li].data_ptr(), B
                     ep.loss = ws.loss.data_ptr()
@@ -365,7 +381,8 @@ class MLP:
     def train_step(self, raw, target, lr: Optional[float] = None, check: bool = False):
         """One Adam step on a batch (device tensors raw [B, n_in], target [B, n_out] float32).
 
-        Returns the device scalar of the batch's mean squared error (before the update).
+        Returns the device scalar of this rank's batch mean squared error (before the
+        update). Data-parallel (:meth:`data_parallel`): B is the local batch.
         """
         torch = self.torch
         B = raw.shape[0]
@@ -377,6 +394,9 @@ class MLP:
         ws.loss.zero_()
         self._forward(ws, stream, True)
         self._backward(ws, stream)
+        if self.world > 1:
+            from . import shard
+            shard.allreduce_gradients(ws.dw + ws.db, self.group)
         self._adam(ws, stream, self.lr if lr is None else float(lr))
         if check:
             self._check(ws)

@@ -171,10 +171,11 @@ def main(argv=None) -> None:
     ap.add_argument("--gate", type=float, default=1e-3)
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--infer-batch", type=int, default=0)
+    ap.add_argument("--profiles-per-launch", type=int, default=256)
     ap.add_argument("--out", default=None)
     a = ap.parse_args(argv)
     rep = run(a.train, a.eval, a.ood, a.steps, a.members, a.batch, a.hidden, a.depth, a.lr, a.strength_scale,
-              a.lines, a.gate, a.seed, infer_batch=a.infer_batch)
+              a.lines, a.gate, a.seed, profiles_per_launch=a.profiles_per_launch, infer_batch=a.infer_batch)
     text = json.dumps(rep, indent=1)
     print(text)
     if a.out:

@@ -161,6 +161,22 @@ def test_training_gradients_match_oracle(cuda):
     assert np.max(np.abs(out - p)) < 2e-5
 
 
+def test_data_parallel_gradient_scaling(cuda):
+    """Two ranks of 128 with scale 1/(128 x 2) sum to the 256-row batch gradient (what
+    shard.allreduce_gradients computes between backward and Adam)."""
+    net, raw, target = _small_net(7)
+    r, t = torch.from_numpy(raw).cuda(), torch.from_numpy(target).cuda()
+    _, dw, db = net.gradients(r, t)
+    net.world = 2
+    try:
+        _, dw_a, db_a = net.gradients(r[:128], t[:128])
+        _, dw_b, db_b = net.gradients(r[128:], t[128:])
+    finally:
+        net.world = 1
+    for full, a, b in zip(dw + db, dw_a + db_a, dw_b + db_b):
+        assert torch.linalg.norm(a + b - full) <= 1e-5 * torch.linalg.norm(full)
+
+
 def test_adam_step_matches_oracle(cuda):
     net, raw, target = _small_net(6)
     w0, b0 = _host_params(net)
