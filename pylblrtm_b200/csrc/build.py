@@ -20,6 +20,7 @@ SOURCES = ["capi.cu", "prep.cu", "voigt.cu", "voigt_ml.cu", "voigt_ml_jac.cu", "
 HEADERS = ["lbl_common.cuh", "faddeeva.cuh", "sum_common.cuh", "weideman_coeffs.h", os.path.join("..", "..", "include", "lblgpu.h")]
 LIB = os.path.join(PKG, "liblblgpu.so")
 HOST_LIB = os.path.join(PKG, "libfaddeeva_host.so")
+IO_LIB = os.path.join(PKG, "liblblio.so")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 
@@ -40,6 +41,8 @@ def _stale(target: str, deps) -> bool:
 def build(force: bool = False, verbose: bool = False) -> str:
     """Compile every .cu source for sm_100a and link liblblgpu.so; returns its path."""
     deps = SOURCES + HEADERS + ["build.py", "faddeeva_host.cpp"]
+    if force or _stale(IO_LIB, ["hitran_par.cpp", os.path.join("..", "..", "include", "lblio.h"), "build.py"]):
+        build_io()
     if not force and not _stale(LIB, deps):
         return LIB
     objdir = os.path.join(ROOT, "_build")
@@ -58,6 +61,15 @@ def build(force: bool = False, verbose: bool = False) -> str:
     os.replace(tmp, LIB)
     build_host_check()
     return LIB
+
+
+def build_io() -> str:
+    """Host (g++) build of the HITRAN text reader, liblblio.so (no CUDA)."""
+    tmp = IO_LIB + ".tmp"
+    subprocess.run(["g++", "-O2", "-std=c++17", "-fPIC", "-shared", os.path.join(HERE, "hitran_par.cpp"),
+                    "-o", tmp], check=True)
+    os.replace(tmp, IO_LIB)
+    return IO_LIB
 
 
 def build_host_check() -> str:
