@@ -1,5 +1,6 @@
 /*
- * lblio.h — C ABI of the host-side HITRAN text reader (liblblio.so; no CUDA).
+ * lblio.h — C ABI of the host-side helpers (liblblio.so; no CUDA): the HITRAN text
+ * reader and the line-list group scan.
  *
  * Replaces the line loop of pylblrtm/hitran_manager.py:816-872 (par_to_dict) with the
  * same semantics (see pylblrtm_b200/csrc/hitran_par.cpp); the Python layer
@@ -32,6 +33,17 @@ long long lbl_par_count_lines(const char* text, long long len);
  * ids [n, 2] (mol_id, iso_id), status [n]; cap must equal lbl_par_count_lines. */
 int lbl_par_parse(const char* text, long long len, long long cap, double* values, int* ids,
                   signed char* status);
+
+/* Group scan of the line list (replaces the pair discovery and band-mask counts of
+ * pylblrtm/forward.py:189-245): distinct (mol, iso) pairs in first-seen order
+ * (pair_mol, pair_iso [max_pairs]), the number of lines of each inside the band
+ * mask nu0 in [(nu_first - cutoff) - |shift| p_max, (nu_last + cutoff) + |shift| p_max]
+ * with lo_edge = nu_first - cutoff and hi_edge = nu_last + cutoff (pair_band), their
+ * count (n_pairs) and every line's pair (pair_index [n]). LBL_EINVAL when more than
+ * max_pairs pairs occur. */
+int lbl_line_pairs(const int* mol, const int* iso, const double* nu0, const double* shift, long long n,
+                   double lo_edge, double hi_edge, double p_max, int max_pairs, int* pair_mol, int* pair_iso,
+                   long long* pair_band, int* n_pairs, int* pair_index);
 
 #ifdef __cplusplus
 }

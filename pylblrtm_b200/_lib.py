@@ -77,8 +77,34 @@ class GemmEpilogue(ctypes.Structure):
 
 SIZEOF_GEMM_EPILOGUE = 136
 
+# host-side helpers (liblblio.so, include/lblio.h): no CUDA
+IO_LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "liblblio.so")
+HOST_SIGNATURES = {
+    "lbl_par_count_lines": (_L, [ctypes.c_char_p, _L]),
+    "lbl_par_parse": (_I, [ctypes.c_char_p, _L, _L, _P, _P, _P]),
+    "lbl_line_pairs": (_I, [_P, _P, _P, _P, _L, _D, _D, _D, _I, _P, _P, _P, _P, _P]),
+}
+
 _lock = threading.Lock()
 _lib = None
+_host = None
+
+
+def load_host() -> ctypes.CDLL:
+    """Load liblblio.so (host helpers) once and declare its signatures."""
+    global _host
+    with _lock:
+        if _host is None:
+            if not os.path.exists(IO_LIB_PATH):
+                raise EngineUnavailable(f"{IO_LIB_PATH} is missing; build it with "
+                                        "`python -m pylblrtm_b200.csrc.build`")
+            lib = ctypes.CDLL(IO_LIB_PATH)
+            for name, (res, args) in HOST_SIGNATURES.items():
+                fn = getattr(lib, name)
+                fn.restype = res
+                fn.argtypes = args
+            _host = lib
+    return _host
 
 
 class EngineUnavailable(RuntimeError):

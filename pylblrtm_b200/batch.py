@@ -113,4 +113,4 @@ def transmittance_batch(
         axis = grid.nu_min + (np.arange(n_ch) * width + 0.5 * (width - 1)) * grid.step
     else:
         axis = grid.nu
-    return axis, (out.cpu().numpy() if as_numpy else out)
+    return axis, (engine.to_host(out) if as_numpy else out)

@@ -125,18 +125,19 @@ def run_forward(spectral_data: SpectralData, profile: AtmosphericProfile,
     grid = engine.make_grid(float(sp["nu_min_cm1"]), float(sp["nu_max_cm1"]), float(sp["step_cm1"]),
                             float(ca["tile_width_cm1"]))
     mu = float(ca["mu_view"])
+    nu = engine.grid_async(grid)
     res = engine.optical_depth(
         spectral_data, engine.layer_input_from_profile(profile), grid, float(ca["line_cutoff_cm1"]),
         precision=cfg.get("engine", {}).get("precision", DEFAULT_PRECISION), mu=[mu],
         want_od=bool(out["optical_depth_layers"]), want_tau=bool(out["optical_depth"]),
         want_trans=bool(out["transmittance"]), warn_level=3)
-    result = ForwardResult(wavenumber_cm1=grid.nu, config=cfg)
+    result = ForwardResult(wavenumber_cm1=nu.result(), config=cfg)
     if out["transmittance"]:
-        result.transmittance = res.trans[0].cpu().numpy()
+        result.transmittance = engine.to_host(res.trans[0])
     if out["optical_depth"]:
-        result.optical_depth = res.tau[0].cpu().numpy()           # vertical, not divided by mu
+        result.optical_depth = engine.to_host(res.tau[0])        # vertical, not divided by mu
     if out["optical_depth_layers"]:
-        result.optical_depth_layers = res.od[0].double().cpu().numpy()
+        result.optical_depth_layers = engine.to_host(res.od[0].double())
     if out["save"]["enabled"]:
         result.save()
     return result

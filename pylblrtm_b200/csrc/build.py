@@ -41,7 +41,8 @@ def _stale(target: str, deps) -> bool:
 def build(force: bool = False, verbose: bool = False) -> str:
     """Compile every .cu source for sm_100a and link liblblgpu.so; returns its path."""
     deps = SOURCES + HEADERS + ["build.py", "faddeeva_host.cpp"]
-    if force or _stale(IO_LIB, ["hitran_par.cpp", os.path.join("..", "..", "include", "lblio.h"), "build.py"]):
+    if force or _stale(IO_LIB, ["hitran_par.cpp", "host_scan.cpp", os.path.join("..", "..", "include", "lblio.h"),
+                                "build.py"]):
         build_io()
     if not force and not _stale(LIB, deps):
         return LIB
@@ -64,10 +65,12 @@ def build(force: bool = False, verbose: bool = False) -> str:
 
 
 def build_io() -> str:
-    """Host (g++) build of the HITRAN text reader, liblblio.so (no CUDA)."""
+    """Host (g++) build of the HITRAN reader and line scan, liblblio.so (no CUDA); no
+    floating-point contraction, so host arithmetic rounds like NumPy's."""
     tmp = IO_LIB + ".tmp"
-    subprocess.run(["g++", "-O2", "-std=c++17", "-fPIC", "-shared", os.path.join(HERE, "hitran_par.cpp"),
-                    "-o", tmp], check=True)
+    subprocess.run(["g++", "-O2", "-std=c++17", "-ffp-contract=off", "-fPIC", "-shared",
+                    os.path.join(HERE, "hitran_par.cpp"), os.path.join(HERE, "host_scan.cpp"), "-o", tmp],
+                   check=True)
     os.replace(tmp, IO_LIB)
     return IO_LIB
 

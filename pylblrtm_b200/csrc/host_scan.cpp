@@ -1,0 +1,45 @@
+// One host pass over the line list for the group selection of pylblrtm/forward.py:189-245
+// (liblblio.so): the distinct (mol_id, iso_id) pairs, how many lines of each fall inside
+// the band mask of forward.py:190-191, and the pair index of every line. The band test
+// is evaluated in the reference's operation order,
+//     sb = |shift| * p_max;  in = (nu0 >= (nu_first - cutoff) - sb) & (nu0 <= (nu_last + cutoff) + sb)
+// and this file is compiled with floating-point contraction off, so every comparison
+// sees the same doubles as NumPy's.
+#include <math.h>
+
+#include "../../include/lblio.h"
+
+extern "C" int lbl_line_pairs(const int* mol, const int* iso, const double* nu0, const double* shift, long long n,
+                              double lo_edge, double hi_edge, double p_max, int max_pairs, int* pair_mol,
+                              int* pair_iso, long long* pair_band, int* n_pairs, int* pair_index) {
+  if (n < 0 || max_pairs < 1 || !n_pairs || (n > 0 && (!mol || !iso || !nu0 || !shift || !pair_index)) ||
+      !pair_mol || !pair_iso || !pair_band)
+    return LBL_EINVAL;
+  int np_ = 0, last = -1;
+  for (long long i = 0; i < n; ++i) {
+    const int m = mol[i], s = iso[i];
+    int k = last;
+    if (k < 0 || pair_mol[k] != m || pair_iso[k] != s) {
+      k = -1;
+      for (int j = 0; j < np_; ++j)
+        if (pair_mol[j] == m && pair_iso[j] == s) {
+          k = j;
+          break;
+        }
+      if (k < 0) {
+        if (np_ >= max_pairs) return LBL_EINVAL;
+        k = np_++;
+        pair_mol[k] = m;
+        pair_iso[k] = s;
+        pair_band[k] = 0;
+      }
+      last = k;
+    }
+    pair_index[i] = k;
+    const double sb = fabs(shift[i]) * p_max;
+    const double v = nu0[i];
+    if ((v >= lo_edge - sb) & (v <= hi_edge + sb)) ++pair_band[k];
+  }
+  *n_pairs = np_;
+  return LBL_OK;
+}

@@ -80,7 +80,7 @@ __device__ __forceinline__ float clenshaw16(const float* c, float t) {
   return fmaf(t, b1, 0.5f * c[0] - b2);
 }
 
-__global__ void __launch_bounds__(ML_THREADS, 2)
+__global__ void __launch_bounds__(ML_THREADS, 4)
 tau_ml_kernel(const LineF32* __restrict__ prep, int n_lines, const int2* __restrict__ ranges,
               const double* __restrict__ t_layer, double nu_min, double step, long long n_nu,
               int tile_samples, int chunks_per_tile, double cutoff, int n_grp, float* __restrict__ od,

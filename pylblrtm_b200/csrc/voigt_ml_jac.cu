@@ -140,7 +140,7 @@ __device__ __forceinline__ float clenshaw_k(const float* c, float t) {
   return fmaf(t, b1, 0.5f * c[0] - b2);
 }
 
-__global__ void __launch_bounds__(MJ_THREADS, 1)
+__global__ void __launch_bounds__(MJ_THREADS, 2)
 jac_ml_kernel(const LineF32* __restrict__ prep, const LineJac* __restrict__ jprep, int n_lines,
               const int2* __restrict__ ranges, const double* __restrict__ t_layer, double nu_min, double step,
               long long n_nu, int tile_samples, int chunks_per_tile, double cutoff, float* __restrict__ od,

@@ -20,6 +20,7 @@ the GPU. There is no CPU path.
 
 from __future__ import annotations
 
+import ctypes
 import math
 import warnings
 from dataclasses import dataclass, field
@@ -67,7 +68,10 @@ class Grid:
 
     @property
     def nu(self) -> np.ndarray:
-        return self.nu_min + np.arange(self.n_nu, dtype=np.float64) * self.step
+        nu = np.arange(self.n_nu, dtype=np.float64)      # nu_min + i * step, in place
+        nu *= self.step
+        nu += self.nu_min
+        return nu
 
     def nu_at(self, i: int) -> float:
         return float(self.nu_min + np.float64(i) * self.step)
@@ -117,31 +121,38 @@ def select_groups(sd: SpectralData, profile_gases: Sequence[str], nu_first: floa
     lines = sd.lines
     mol = np.asarray(lines["mol_id"])
     iso = np.asarray(lines["iso_id"])
-    nu0 = np.asarray(lines["nu0"], dtype=np.float64)
-    shift = np.asarray(lines["shift"], dtype=np.float64)
-    n = nu0.size
+    n = np.asarray(lines["nu0"]).size
     gid = np.full(n, -1, dtype=np.int32)
     if n == 0:
         return [], gid
-    mol64 = mol.astype(np.int64)
-    iso64 = iso.astype(np.int64)
-    small = (mol64.min() >= 0 and iso64.min() >= 0 and mol64.max() < 4096 and iso64.max() < 1024)
-    if small:
-        key = mol64 * 1024 + iso64
-        present = np.flatnonzero(np.bincount(key))
-        pairs = [(int(k // 1024), int(k % 1024)) for k in present]
-        inv = None
-    else:
-        key2 = np.stack([mol64, iso64], axis=1)
-        uniq, inv = np.unique(key2, axis=0, return_inverse=True)
-        pairs = [(int(a), int(b)) for a, b in uniq]
-        inv = inv.reshape(-1)
-    sb = np.abs(shift) * p_max                                         # forward.py:191
-    in_band = (nu0 >= nu_first - cutoff - sb) & (nu0 <= nu_last + cutoff + sb)
-    if small:
-        band_counts = np.bincount(key[in_band], minlength=int(key.max()) + 1)
-    else:
-        band_counts = np.bincount(inv[in_band], minlength=len(pairs))
+    # one native pass: distinct (mol, iso) pairs, band-mask counts (forward.py:190-191)
+    # and each line's pair; ids must fit int32 (HITRAN numbers are small)
+    for a in (mol, iso):
+        if a.dtype != np.int32 and (a.min() < -2 ** 31 or a.max() >= 2 ** 31):
+            raise ValueError("mol_id / iso_id values must fit a 32-bit integer")
+    c = lambda a, t: np.ascontiguousarray(a, dtype=t)
+    mol32, iso32 = c(mol, np.int32), c(iso, np.int32)
+    nu0, shift = c(lines["nu0"], np.float64), c(lines["shift"], np.float64)
+    pair_index = np.empty(n, dtype=np.int32)
+    host = _lib.load_host()
+    max_pairs = 256
+    while True:
+        pm = np.empty(max_pairs, np.int32)
+        pi_ = np.empty(max_pairs, np.int32)
+        pb = np.empty(max_pairs, np.int64)
+        n_pairs = ctypes.c_int(0)
+        rc = host.lbl_line_pairs(mol32.ctypes.data, iso32.ctypes.data, nu0.ctypes.data, shift.ctypes.data, n,
+                                 nu_first - cutoff, nu_last + cutoff, float(p_max), max_pairs, pm.ctypes.data,
+                                 pi_.ctypes.data, pb.ctypes.data, ctypes.byref(n_pairs), pair_index.ctypes.data)
+        if rc == 0:
+            break
+        if max_pairs >= n:
+            raise RuntimeError("lbl_line_pairs failed")
+        max_pairs = min(n, 16 * max_pairs)
+    k = n_pairs.value
+    order = np.lexsort((pi_[:k], pm[:k]))                               # sorted (mol_id, iso_id)
+    pairs = [(int(pm[j]), int(pi_[j])) for j in order]
+    band_counts = pb[:k][order]
     groups: List[Group] = []
     lut_pairs: Dict[int, int] = {}
     for pi, (m, i) in enumerate(pairs):
@@ -156,7 +167,7 @@ def select_groups(sd: SpectralData, profile_gases: Sequence[str], nu_first: floa
                 f"spectral data but not in the atmospheric profile vmr; "
                 f"its lines are skipped.", RuntimeWarning, stacklevel=warn_level)
             continue
-        cnt = band_counts[m * 1024 + i] if small else band_counts[pi]
+        cnt = band_counts[pi]
         if cnt == 0:
             continue
         mm = sd.molar_masses.get((int(m), int(i)))
@@ -172,20 +183,14 @@ def select_groups(sd: SpectralData, profile_gases: Sequence[str], nu_first: floa
         if np.asarray(t_arr).size == 0 or np.asarray(t_arr).size != np.asarray(q_arr).size:
             raise ValueError("array of sample points is empty" if np.asarray(t_arr).size == 0
                              else "fp and xp are not of the same length.")
-        lut_pairs[m * 1024 + i if small else pi] = len(groups)
+        lut_pairs[int(order[pi])] = len(groups)
         groups.append(Group(int(m), int(i), gas, float(mm), np.asarray(t_arr, np.float64),
                             np.asarray(q_arr, np.float64)))
     if groups:
-        if small:
-            lut = np.full(int(key.max()) + 1, -1, dtype=np.int32)
-            for k, g in lut_pairs.items():
-                lut[k] = g
-            gid = lut[key]
-        else:
-            lut = np.full(len(pairs), -1, dtype=np.int32)
-            for k, g in lut_pairs.items():
-                lut[k] = g
-            gid = lut[inv]
+        lut = np.full(k, -1, dtype=np.int32)
+        for j, g in lut_pairs.items():
+            lut[j] = g
+        gid = lut[pair_index]
     return groups, gid
 
 
@@ -229,6 +234,29 @@ class EngineResult:
     work: int = 0                  # Faddeeva evaluations actually performed (multi-level engine)
     work_split: tuple = ()         # (node evaluations, level-3 loop evaluations, near-zone points)
     groups: List[Group] = field(default_factory=list)
+
+
+_GRID_POOL = None
+
+
+def grid_async(grid: Grid):
+    """Future of ``grid.nu`` computed on a worker thread (NumPy releases the GIL), so the
+    host builds the returned grid while the device computes."""
+    global _GRID_POOL
+    if _GRID_POOL is None:
+        from concurrent.futures import ThreadPoolExecutor
+        _GRID_POOL = ThreadPoolExecutor(max_workers=1, thread_name_prefix="lbl-grid")
+    return _GRID_POOL.submit(lambda: grid.nu)
+
+
+def to_host(t) -> np.ndarray:
+    """Device tensor -> NumPy array through a pinned (page-locked) buffer from torch's
+    caching host allocator; the returned array owns that buffer."""
+    torch = _torch()
+    h = torch.empty(t.shape, dtype=t.dtype, pin_memory=True)
+    h.copy_(t, non_blocking=True)
+    torch.cuda.current_stream().synchronize()
+    return h.numpy()
 
 
 def _upload(torch, a, dtype, device):

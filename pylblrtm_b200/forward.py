@@ -51,10 +51,12 @@ def compute_transmittance(
     if not (0.0 < mu_view <= 1.0):
         raise ValueError("mu_view must be in (0, 1]")
     grid = engine.make_grid(nu_min_cm1, nu_max_cm1, step_cm1, tile_width_cm1)
+    nu = engine.grid_async(grid)
     res = engine.optical_depth(spectral_data, engine.layer_input_from_profile(profile), grid,
                                float(line_cutoff_cm1), precision=precision, mu=[float(mu_view)],
                                want_od=False, want_trans=True, warn_level=3)
-    return grid.nu, res.trans[0].cpu().numpy()
+    trans = engine.to_host(res.trans[0])
+    return nu.result(), trans
 
 
 def _build_optical_depth(
@@ -72,4 +74,4 @@ def _build_optical_depth(
     grid = engine.grid_from_array(nu, tile_width_cm1)
     res = engine.optical_depth(sd, engine.layer_input_from_layers(layers), grid, float(line_cutoff_cm1),
                                precision=precision, want_od=True, warn_level=4)
-    return res.od[0].to(dtype=__import__("torch").float64).cpu().numpy()
+    return engine.to_host(res.od[0].to(dtype=__import__("torch").float64))

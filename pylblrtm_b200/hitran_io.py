@@ -17,7 +17,6 @@ import ctypes
 import logging
 import os
 import re
-import threading
 from pathlib import Path
 from typing import Dict, Optional, Tuple, Union
 
@@ -28,14 +27,11 @@ from .spectral_data import SpectralData
 
 logger = logging.getLogger(__name__)
 
-IO_LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "liblblio.so")
 PAR_SHORT, PAR_NONASCII = -1, -2
 COLUMNS = ("mol_id", "iso_id", "nu0", "Sref", "g_air", "g_self", "Elow", "n_air", "shift")
 _SLICES = ((0, 2), (2, 3), (3, 15), (15, 25), (35, 40), (40, 45), (45, 55), (55, 59), (59, 67))
 _ID_TO_MOL = {v: k for k, v in MOLECULE_IDS.items()}
 
-_lock = threading.Lock()
-_io = None
 
 
 class HITRANDataError(ValueError):
@@ -43,19 +39,8 @@ class HITRANDataError(ValueError):
 
 
 def _lib() -> ctypes.CDLL:
-    global _io
-    with _lock:
-        if _io is None:
-            if not os.path.exists(IO_LIB_PATH):
-                raise RuntimeError(f"{IO_LIB_PATH} is missing; build it with `python -m pylblrtm_b200.csrc.build`")
-            lib = ctypes.CDLL(IO_LIB_PATH)
-            lib.lbl_par_count_lines.restype = ctypes.c_longlong
-            lib.lbl_par_count_lines.argtypes = [ctypes.c_char_p, ctypes.c_longlong]
-            lib.lbl_par_parse.restype = ctypes.c_int
-            lib.lbl_par_parse.argtypes = [ctypes.c_char_p, ctypes.c_longlong, ctypes.c_longlong, ctypes.c_void_p,
-                                          ctypes.c_void_p, ctypes.c_void_p]
-            _io = lib
-    return _io
+    from . import _lib as lib_mod
+    return lib_mod.load_host()
 
 
 def _python_fields(raw: str):

@@ -72,7 +72,9 @@ def run(n_train: int = 100_000, n_eval: int = 65_536, ood: float = 0.05, steps: 
                    "target_quantiles": [float(v) for v in np.quantile(y, [0, 0.1, 0.5, 0.9, 1])]}
     log(f"data: {n_train} spectra in {t_gen:.1f} s")
 
-    # 2. ensemble training
+    # 2. ensemble training (a training set smaller than one batch trains on all of it)
+    batch = max(128, min(batch, n_train // 128 * 128))
+    rep["network"]["batch"] = batch
     t0 = time.perf_counter()
     cfg = surrogate.TrainConfig(batch=batch, steps=steps, lr=lr, lr_final=lr * 1e-2, warmup=min(200, steps // 10),
                                 seed=seed + 1)
