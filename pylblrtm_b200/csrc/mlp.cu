@@ -4,21 +4,26 @@
 // and is trained on spectra produced by this library's own engine.
 //
 // D[M, N] = A[M, K] . B[N, K]^T, A and B bf16 row-major with K contiguous ("K-major"),
-// accumulated in float32 in tensor memory. One CTA (4 warps) computes a 128 x 128 tile:
-//   warp 0, lane 0  streams 128 x 64 tiles of A and B into a 3-stage shared-memory ring
-//                   with TMA (128-byte swizzle); each stage completes a "full" mbarrier;
-//   warp 1, lane 0  issues tcgen05.mma (M = 128, N = 128, K = 16) four times per stage
-//                   and frees the stage with tcgen05.commit on its "empty" mbarrier;
-//   all 4 warps     wait for the last commit, read their 32 accumulator rows with
-//                   tcgen05.ld and apply the epilogue.
-// Two CTAs fit on one SM (99 KB shared memory, 128 tensor-memory columns each), so one
-// CTA's epilogue overlaps the other's main loop. Split-K (grid.z > 1) is offered for the
-// float32 mode only: split z writes its partial sum to out_f32 + z * split_stride and the
-// consumer adds the partials in a fixed order (deterministic).
+// accumulated in float32 in tensor memory. The kernel is persistent (one CTA per SM,
+// each looping over 128 x BN output tiles, BN = 256 or 128) and warp-specialised:
+//   warp 0, lane 0   streams 128 x 64 tiles of A and BN x 64 tiles of B into a 4-stage
+//                    shared-memory ring with TMA (128-byte swizzle, no multicast);
+//                    each stage completes a "full" mbarrier;
+//   warp 1, lane 0   issues tcgen05.mma (M = 128, N = BN, K = 16) four times per stage
+//                    into one of two tensor-memory accumulators and frees the stage
+//                    with tcgen05.commit on its "empty" mbarrier; a finished tile is
+//                    signalled on the accumulator's "tmem_full" mbarrier;
+//   warps 2-5        (the epilogue) read their 32 accumulator rows each with
+//                    tcgen05.ld, apply the epilogue, store, and release the accumulator
+//                    ("tmem_empty", one arrival per warp), so the epilogue of one tile
+//                    overlaps the main loop of the next.
+// Split-K (n_split > 1) is offered for the float32 mode only: split z writes its partial
+// sum to out_f32 + z * split_stride and the consumer adds the partials in a fixed order
+// (deterministic).
 //
 // Every mbarrier wait is bounded by wall-clock time (globaltimer); a wait that runs out
-// marks the CTA failed, the CTA skips its epilogue, always frees its tensor memory and
-// raises the caller's error word.
+// marks the CTA failed, every role leaves its loop, the MMA warp drains its own
+// outstanding MMAs, tensor memory is always freed and the caller's error word is raised.
 #include <cuda.h>
 #include <cuda_bf16.h>
 #include <math.h>
@@ -29,11 +34,22 @@
 
 namespace lbl {
 
-constexpr int GM = 128, GN = 128, GK = 64, GSTAGES = 3;
-constexpr int G_TILE_BYTES = GM * GK * 2;                          // 16 KiB per operand tile
-constexpr int G_SMEM_BYTES = 2 * GSTAGES * G_TILE_BYTES + 1024 + 128;
+constexpr int GM = 128, GK = 64, GSTAGES = 4;
+constexpr int G_A_BYTES = GM * GK * 2;                             // 16 KiB A tile per stage
+constexpr int G_THREADS = 192;                                     // TMA, MMA, 4 epilogue warps
 constexpr unsigned long long G_WAIT_NS = 2000000000ull;            // 2 s per wait at most
-constexpr int G_TMEM_COLS = 128;
+
+template <int BN>
+struct GemmCfg {
+  static constexpr int B_BYTES = BN * GK * 2;
+  static constexpr int STAGE_BYTES = G_A_BYTES + B_BYTES;
+  static constexpr int TMEM_COLS = 2 * BN;                         // two float32 accumulators
+  static constexpr int SMEM = GSTAGES * STAGE_BYTES + 1024 + 256;  // ring + alignment + barriers
+  // kind::f16: D f32 (bits 4-5 = 1), A and B bf16 (bits 7-9, 10-12 = 1), both K-major
+  // (bits 15, 16 = 0), N >> 3 at bit 17, M >> 4 at bit 24.
+  static constexpr uint32_t IDESC =
+      (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(BN >> 3) << 17) | ((uint32_t)(GM >> 4) << 24);
+};
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
 
@@ -95,17 +111,17 @@ __device__ __forceinline__ uint64_t sw128_desc(uint32_t addr) {
   return d;
 }
 
-// Instruction descriptor of kind::f16: D f32 (bits 4-5 = 1), A and B bf16 (bits 7-9 and
-// 10-12 = 1), both K-major (bits 15, 16 = 0), N >> 3 at bit 17, M >> 4 at bit 24.
-constexpr uint32_t G_IDESC =
-    (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(GN >> 3) << 17) | ((uint32_t)(GM >> 4) << 24);
-
-__device__ __forceinline__ void umma_bf16(uint32_t tmem_d, uint64_t da, uint64_t db, uint32_t accumulate) {
+__device__ __forceinline__ void umma_bf16(uint32_t tmem_d, uint64_t da, uint64_t db, uint32_t idesc,
+                                          uint32_t accumulate) {
   asm volatile(
       "{\n\t.reg .pred p;\n\t"
       "setp.ne.b32 p, %4, 0;\n\t"
       "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem_d),
-      "l"(da), "l"(db), "r"(G_IDESC), "r"(accumulate));
+      "l"(da), "l"(db), "r"(idesc), "r"(accumulate));
+}
+
+__device__ __forceinline__ void mbar_arrive(uint32_t bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
 }
 
 __device__ __forceinline__ void umma_commit(uint32_t bar) {
@@ -158,134 +174,208 @@ __device__ __forceinline__ void load_row16(const __nv_bfloat16* src, float* v) {
   }
 }
 
-__global__ void __launch_bounds__(128, 2)
-gemm_bf16_kernel(const __grid_constant__ CUtensorMap map_a, const __grid_constant__ CUtensorMap map_b, int k_tiles,
-                 LblGemmEpilogue ep, int* err) {
+// Epilogue of one 16-column slice of one accumulator row (row, col = first column).
+__device__ __forceinline__ void epilogue16(const LblGemmEpilogue& ep, int split, int row, int col, float* v,
+                                           float& loss) {
+  if (ep.mode == LBL_GEMM_F32) {
+    float4* d = reinterpret_cast<float4*>(ep.out_f32 + (long long)split * ep.split_stride +
+                                          (long long)row * ep.ld_f32 + col);
+#pragma unroll
+    for (int i = 0; i < 4; ++i) d[i] = make_float4(v[4 * i], v[4 * i + 1], v[4 * i + 2], v[4 * i + 3]);
+    return;
+  }
+  if (ep.mode == LBL_GEMM_BIAS_GELU) {
+#pragma unroll
+    for (int i = 0; i < 16; ++i) v[i] += ep.bias[col + i];
+    if (ep.z_out) store_row16((__nv_bfloat16*)ep.z_out + (long long)row * ep.ld_z + col, v);
+#pragma unroll
+    for (int i = 0; i < 16; ++i) v[i] = gelu(v[i]);
+  } else if (ep.mode == LBL_GEMM_BIAS_SIGMOID) {
+    float p[16];
+#pragma unroll
+    for (int i = 0; i < 16; ++i) p[i] = 1.0f / (1.0f + __expf(-(v[i] + ep.bias[col + i])));
+    if (ep.out_f32) {
+      float4* d = reinterpret_cast<float4*>(ep.out_f32 + (long long)row * ep.ld_f32 + col);
+#pragma unroll
+      for (int i = 0; i < 4; ++i) d[i] = make_float4(p[4 * i], p[4 * i + 1], p[4 * i + 2], p[4 * i + 3]);
+    }
+    if (!ep.target) return;
+#pragma unroll
+    for (int i = 0; i < 16; ++i) {
+      if (col + i < ep.n_valid) {
+        const float d = p[i] - ep.target[(long long)row * ep.ld_target + col + i];
+        loss += d * d;
+        v[i] = ep.grad_scale * 2.0f * d * p[i] * (1.0f - p[i]);
+      } else {
+        v[i] = 0.0f;                               // padded outputs carry no gradient
+      }
+    }
+  } else {                                         // LBL_GEMM_DGELU
+    float z[16];
+    load_row16((const __nv_bfloat16*)ep.z_in + (long long)row * ep.ld_zin + col, z);
+#pragma unroll
+    for (int i = 0; i < 16; ++i) v[i] *= gelu_grad(z[i]);
+  }
+  if (ep.y) store_row16((__nv_bfloat16*)ep.y + (long long)row * ep.ld_y + col, v);
+  if (ep.y_t) {
+    __nv_bfloat16* yt = (__nv_bfloat16*)ep.y_t;
+#pragma unroll
+    for (int i = 0; i < 16; ++i) yt[(long long)(col + i) * ep.ld_yt + row] = __float2bfloat16(v[i]);
+  }
+}
+
+// Work unit u -> (split, m tile, n tile); n varies fastest so concurrent CTAs share A.
+struct GemmGrid {
+  int n_m, n_n, kt_per;
+  __device__ __forceinline__ void unit(int u, int& split, int& m0, int& n0, int bn) const {
+    split = u / (n_m * n_n);
+    const int r = u - split * n_m * n_n;
+    m0 = (r / n_n) * GM;
+    n0 = (r % n_n) * bn;
+  }
+};
+
+template <int BN>
+__global__ void __launch_bounds__(G_THREADS, 1)
+gemm_bf16_kernel(const __grid_constant__ CUtensorMap map_a, const __grid_constant__ CUtensorMap map_b,
+                 GemmGrid gg, int units, LblGemmEpilogue ep, int* err) {
+  using Cfg = GemmCfg<BN>;
   extern __shared__ unsigned char g_smem_raw[];
   unsigned char* smem = (unsigned char*)(((uintptr_t)g_smem_raw + 1023) & ~(uintptr_t)1023);
-  unsigned char* tiles_a = smem;
-  unsigned char* tiles_b = smem + GSTAGES * G_TILE_BYTES;
-  uint64_t* bars = (uint64_t*)(smem + 2 * GSTAGES * G_TILE_BYTES);  // full[S], empty[S], done
-  uint32_t* tmem_slot = (uint32_t*)(bars + 2 * GSTAGES + 1);
+  uint64_t* bars = (uint64_t*)(smem + GSTAGES * Cfg::STAGE_BYTES);
+  uint64_t* full = bars;                       // [GSTAGES], one producer arrival + TMA bytes
+  uint64_t* empty = bars + GSTAGES;            // [GSTAGES], one tcgen05.commit
+  uint64_t* tfull = bars + 2 * GSTAGES;        // [2], one tcgen05.commit
+  uint64_t* tempty = bars + 2 * GSTAGES + 2;   // [2], one arrival per epilogue warp
+  uint64_t* drain = bars + 2 * GSTAGES + 4;    // MMA warp's final commit
+  uint32_t* tmem_slot = (uint32_t*)(bars + 2 * GSTAGES + 5);
   volatile int* fail = (volatile int*)(tmem_slot + 1);
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int m0 = blockIdx.y * GM, n0 = blockIdx.x * GN;
-  const int kt0 = blockIdx.z * k_tiles;
-
   if (threadIdx.x == 0) {
     *fail = 0;
-    for (int s = 0; s < 2 * GSTAGES + 1; ++s) mbar_init(smem_u32(&bars[s]), 1);
+    for (int i = 0; i < GSTAGES; ++i) {
+      mbar_init(smem_u32(&full[i]), 1);
+      mbar_init(smem_u32(&empty[i]), 1);
+    }
+    for (int i = 0; i < 2; ++i) {
+      mbar_init(smem_u32(&tfull[i]), 1);
+      mbar_init(smem_u32(&tempty[i]), 4);
+    }
+    mbar_init(smem_u32(drain), 1);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   if (warp == 0) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
-                 "r"(G_TMEM_COLS));
+                 "r"(Cfg::TMEM_COLS));
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
   }
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   const uint32_t tmem = *tmem_slot;
+  float loss = 0.0f;
 
-  if (warp == 0 && lane == 0) {
-    for (int kt = 0; kt < k_tiles; ++kt) {
-      const int s = kt % GSTAGES;
-      if (kt >= GSTAGES && !mbar_wait(smem_u32(&bars[GSTAGES + s]), ((kt / GSTAGES) - 1) & 1)) {
-        *fail = 1;
-        break;
+  if (warp == 0) {
+    if (lane == 0) {                           // TMA producer
+      int g = 0;
+      for (int u = blockIdx.x; u < units && !*fail; u += gridDim.x) {
+        int split, m0, n0;
+        gg.unit(u, split, m0, n0, BN);
+        const int k0 = split * gg.kt_per;
+        for (int kt = 0; kt < gg.kt_per; ++kt, ++g) {
+          const int s = g % GSTAGES;
+          if (g >= GSTAGES && !mbar_wait(smem_u32(&empty[s]), ((g / GSTAGES) - 1) & 1)) {
+            *fail = 1;
+            break;
+          }
+          if (*fail) break;
+          unsigned char* st = smem + s * Cfg::STAGE_BYTES;
+          const uint32_t fb = smem_u32(&full[s]);
+          mbar_expect_tx(fb, Cfg::STAGE_BYTES);
+          tma_load_2d(smem_u32(st), &map_a, fb, (k0 + kt) * GK, m0);
+#pragma unroll
+          for (int h = 0; h < BN / 128; ++h)
+            tma_load_2d(smem_u32(st + G_A_BYTES + h * 128 * GK * 2), &map_b, fb, (k0 + kt) * GK, n0 + 128 * h);
+        }
       }
-      if (*fail) break;
-      const uint32_t full = smem_u32(&bars[s]);
-      mbar_expect_tx(full, 2 * G_TILE_BYTES);
-      tma_load_2d(smem_u32(tiles_a + s * G_TILE_BYTES), &map_a, full, (kt0 + kt) * GK, m0);
-      tma_load_2d(smem_u32(tiles_b + s * G_TILE_BYTES), &map_b, full, (kt0 + kt) * GK, n0);
+      // no copy may still be writing shared memory when the CTA ends (bounded wait)
+      for (int j = g > GSTAGES ? g - GSTAGES : 0; j < g; ++j)
+        if (!mbar_wait(smem_u32(&full[j % GSTAGES]), (j / GSTAGES) & 1)) *fail = 1;
     }
-  } else if (warp == 1 && lane == 0) {
-    for (int kt = 0; kt < k_tiles; ++kt) {
-      const int s = kt % GSTAGES;
-      if (!mbar_wait(smem_u32(&bars[s]), (kt / GSTAGES) & 1)) {
-        *fail = 1;
+  } else if (warp == 1) {
+    if (lane == 0) {                           // MMA issuer
+      int g = 0, i = 0;
+      for (int u = blockIdx.x; u < units && !*fail; u += gridDim.x, ++i) {
+        const int b = i & 1;
+        if (i >= 2 && !mbar_wait(smem_u32(&tempty[b]), ((i >> 1) - 1) & 1)) {
+          *fail = 1;
+          break;
+        }
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        const uint32_t acc = tmem + (uint32_t)(b * BN);
+        bool ok = true;
+        for (int kt = 0; kt < gg.kt_per; ++kt, ++g) {
+          const int s = g % GSTAGES;
+          if (!mbar_wait(smem_u32(&full[s]), (g / GSTAGES) & 1)) {
+            ok = false;
+            break;
+          }
+          asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+          const uint32_t a0 = smem_u32(smem + s * Cfg::STAGE_BYTES), b0 = a0 + G_A_BYTES;
+#pragma unroll
+          for (int kk = 0; kk < GK / 16; ++kk)
+            umma_bf16(acc, sw128_desc(a0 + kk * 32), sw128_desc(b0 + kk * 32), Cfg::IDESC,
+                      (kt > 0 || kk > 0) ? 1u : 0u);
+          umma_commit(smem_u32(&empty[s]));
+        }
+        if (!ok) {
+          *fail = 1;
+          break;
+        }
+        umma_commit(smem_u32(&tfull[b]));
+      }
+      umma_commit(smem_u32(drain));            // arrives once every MMA issued above has finished
+      if (!mbar_wait(smem_u32(drain), 0)) *fail = 1;
+    }
+  } else {                                     // epilogue warps 2..5: tensor-memory lanes 32 * (warp % 4)
+    const int q = warp & 3;
+    int i = 0;
+    for (int u = blockIdx.x; u < units; u += gridDim.x, ++i) {
+      const int b = i & 1;
+      bool ok = !*fail && mbar_wait(smem_u32(&tfull[b]), (i >> 1) & 1);
+      ok = __all_sync(0xffffffffu, ok);
+      if (!ok) {
+        if (lane == 0) *fail = 1;
         break;
       }
       asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-      const uint32_t a0 = smem_u32(tiles_a + s * G_TILE_BYTES), b0 = smem_u32(tiles_b + s * G_TILE_BYTES);
-#pragma unroll
-      for (int kk = 0; kk < GK / 16; ++kk)
-        umma_bf16(tmem, sw128_desc(a0 + kk * 32), sw128_desc(b0 + kk * 32), (kt > 0 || kk > 0) ? 1u : 0u);
-      umma_commit(smem_u32(&bars[GSTAGES + s]));
+      int split, m0, n0;
+      gg.unit(u, split, m0, n0, BN);
+      const int row = m0 + q * 32 + lane;
+      const uint32_t base = tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(b * BN);
+#pragma unroll 1
+      for (int c0 = 0; c0 < BN; c0 += 16) {
+        float v[16];
+        tmem_ld16(base + (uint32_t)c0, v);
+        epilogue16(ep, split, row, n0 + c0, v, loss);
+      }
+      asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+      __syncwarp();
+      if (lane == 0) mbar_arrive(smem_u32(&tempty[b]));
     }
-    umma_commit(smem_u32(&bars[2 * GSTAGES]));   // arrives once every MMA issued above has finished
+    if (ep.loss && ep.mode == LBL_GEMM_BIAS_SIGMOID && ep.target) {
+      double l = loss;
+      for (int o = 16; o > 0; o >>= 1) l += __shfl_xor_sync(0xffffffffu, l, o);
+      if (lane == 0 && l != 0.0) atomicAdd(ep.loss, l);
+    }
   }
   __syncwarp();
-  if (!mbar_wait(smem_u32(&bars[2 * GSTAGES]), 0)) *fail = 1;
-  __syncthreads();
-  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-  const bool ok = (*fail == 0);                   // CTA-uniform after the barrier
-
-  const int row = m0 + warp * 32 + lane;          // accumulator row = tensor-memory lane
-  float loss = 0.0f;
-  if (ok) {
-    for (int c0 = 0; c0 < GN; c0 += 16) {
-      float v[16];
-      tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0, v);
-      const int col = n0 + c0;
-      if (ep.mode == LBL_GEMM_F32) {
-        float4* d = reinterpret_cast<float4*>(ep.out_f32 + (long long)blockIdx.z * ep.split_stride +
-                                              (long long)row * ep.ld_f32 + col);
-#pragma unroll
-        for (int i = 0; i < 4; ++i) d[i] = make_float4(v[4 * i], v[4 * i + 1], v[4 * i + 2], v[4 * i + 3]);
-        continue;
-      }
-      if (ep.mode == LBL_GEMM_BIAS_GELU) {
-#pragma unroll
-        for (int i = 0; i < 16; ++i) v[i] += ep.bias[col + i];
-        if (ep.z_out) store_row16((__nv_bfloat16*)ep.z_out + (long long)row * ep.ld_z + col, v);
-#pragma unroll
-        for (int i = 0; i < 16; ++i) v[i] = gelu(v[i]);
-      } else if (ep.mode == LBL_GEMM_BIAS_SIGMOID) {
-        float p[16];
-#pragma unroll
-        for (int i = 0; i < 16; ++i) p[i] = 1.0f / (1.0f + __expf(-(v[i] + ep.bias[col + i])));
-        if (ep.out_f32) {
-          float4* d = reinterpret_cast<float4*>(ep.out_f32 + (long long)row * ep.ld_f32 + col);
-#pragma unroll
-          for (int i = 0; i < 4; ++i) d[i] = make_float4(p[4 * i], p[4 * i + 1], p[4 * i + 2], p[4 * i + 3]);
-        }
-        if (!ep.target) continue;
-#pragma unroll
-        for (int i = 0; i < 16; ++i) {
-          if (col + i < ep.n_valid) {
-            const float d = p[i] - ep.target[(long long)row * ep.ld_target + col + i];
-            loss += d * d;
-            v[i] = ep.grad_scale * 2.0f * d * p[i] * (1.0f - p[i]);
-          } else {
-            v[i] = 0.0f;                           // padded outputs carry no gradient
-          }
-        }
-      } else {                                     // LBL_GEMM_DGELU
-        float z[16];
-        load_row16((const __nv_bfloat16*)ep.z_in + (long long)row * ep.ld_zin + col, z);
-#pragma unroll
-        for (int i = 0; i < 16; ++i) v[i] *= gelu_grad(z[i]);
-      }
-      if (ep.y) store_row16((__nv_bfloat16*)ep.y + (long long)row * ep.ld_y + col, v);
-      if (ep.y_t) {
-        __nv_bfloat16* yt = (__nv_bfloat16*)ep.y_t;
-#pragma unroll
-        for (int i = 0; i < 16; ++i) yt[(long long)(col + i) * ep.ld_yt + row] = __float2bfloat16(v[i]);
-      }
-    }
-  }
-  if (ep.loss && ep.mode == LBL_GEMM_BIAS_SIGMOID && ep.target) {
-    double l = loss;
-    for (int o = 16; o > 0; o >>= 1) l += __shfl_xor_sync(0xffffffffu, l, o);
-    if (lane == 0 && l != 0.0) atomicAdd(ep.loss, l);
-  }
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();
-  if (threadIdx.x == 0 && !ok && err) atomicMax(err, 1);
-  if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(G_TMEM_COLS));
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  if (threadIdx.x == 0 && *fail && err) atomicMax(err, 1);
+  if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(Cfg::TMEM_COLS));
 }
 
 // ---------------------------------------------------------------------------
@@ -420,9 +510,35 @@ extern "C" int lbl_tensor_map_bf16(void* map_out, const void* base, long long ro
   return LBL_OK;
 }
 
+template <int BN>
+static int launch_gemm(const CUtensorMap& a, const CUtensorMap& b, int M, int N, int K, int n_split,
+                       const LblGemmEpilogue* ep, int* err, cudaStream_t stream) {
+  int dev = 0;
+  cudaGetDevice(&dev);
+  static int attr_set[64] = {0};
+  static int n_sm[64] = {0};
+  if (dev < 0 || dev >= 64) return lbl_set_error(LBL_EINVAL, "lbl_gemm_bf16: device index out of range");
+  if (!attr_set[dev]) {
+    if (cudaFuncSetAttribute(gemm_bf16_kernel<BN>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             GemmCfg<BN>::SMEM) != cudaSuccess)
+      return lbl_check_launch("lbl_gemm_bf16 (shared memory attribute)");
+    cudaDeviceGetAttribute(&n_sm[dev], cudaDevAttrMultiProcessorCount, dev);
+    attr_set[dev] = 1;
+  }
+  GemmGrid gg;
+  gg.n_m = M / GM;
+  gg.n_n = N / BN;
+  gg.kt_per = K / GK / n_split;
+  const long long units = (long long)gg.n_m * gg.n_n * n_split;
+  if (units > 0x7fffffffLL) return lbl_set_error(LBL_EINVAL, "lbl_gemm_bf16: too many tiles");
+  const int grid = (int)(units < n_sm[dev] ? units : n_sm[dev]);
+  gemm_bf16_kernel<BN><<<grid, G_THREADS, GemmCfg<BN>::SMEM, stream>>>(a, b, gg, (int)units, *ep, err);
+  return lbl_check_launch("lbl_gemm_bf16");
+}
+
 extern "C" int lbl_gemm_bf16(const void* map_a, const void* map_b, int M, int N, int K, int n_split,
                              const LblGemmEpilogue* ep, int* err, void* stream) {
-  if (!map_a || !map_b || !ep || M < GM || N < GN || K < GK || M % GM || N % GN || K % GK || n_split < 1 ||
+  if (!map_a || !map_b || !ep || M < GM || N < 128 || K < GK || M % GM || N % 128 || K % GK || n_split < 1 ||
       (K / GK) % n_split || ep->mode < LBL_GEMM_F32 || ep->mode > LBL_GEMM_DGELU)
     return lbl_set_error(LBL_EINVAL, "lbl_gemm_bf16: M, N must be multiples of 128, K of 64 * n_split");
   if (n_split > 1 && ep->mode != LBL_GEMM_F32)
@@ -436,21 +552,11 @@ extern "C" int lbl_gemm_bf16(const void* map_a, const void* map_b, int M, int N,
       (ep->y_t && ep->ld_yt < M) || (ep->mode == LBL_GEMM_BIAS_SIGMOID && ep->out_f32 && ep->ld_f32 % 4) ||
       (ep->mode == LBL_GEMM_BIAS_SIGMOID && ep->target && ep->ld_target < ep->n_valid))
     return lbl_set_error(LBL_EINVAL, "lbl_gemm_bf16: epilogue buffers missing or strides too small/unaligned");
-  int dev = 0;
-  cudaGetDevice(&dev);
-  static int attr_set[64] = {0};
-  if (dev >= 0 && dev < 64 && !attr_set[dev]) {
-    if (cudaFuncSetAttribute(gemm_bf16_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, G_SMEM_BYTES) !=
-        cudaSuccess)
-      return lbl_check_launch("lbl_gemm_bf16 (shared memory attribute)");
-    attr_set[dev] = 1;
-  }
   CUtensorMap a, b;
   memcpy(&a, map_a, sizeof(a));
   memcpy(&b, map_b, sizeof(b));
-  dim3 grid((unsigned)(N / GN), (unsigned)(M / GM), (unsigned)n_split);
-  gemm_bf16_kernel<<<grid, 128, G_SMEM_BYTES, (cudaStream_t)stream>>>(a, b, K / GK / n_split, *ep, err);
-  return lbl_check_launch("lbl_gemm_bf16");
+  if (N % 256 == 0) return launch_gemm<256>(a, b, M, N, K, n_split, ep, err, (cudaStream_t)stream);
+  return launch_gemm<128>(a, b, M, N, K, n_split, ep, err, (cudaStream_t)stream);
 }
 
 extern "C" int lbl_adam_step(float* w, float* m, float* v, const float* g, int n_split, long long split_stride,

@@ -158,12 +158,14 @@ class _Map:
         _lib.call("lbl_tensor_map_bf16", self.addr, t.data_ptr(), t.shape[0], t.shape[1], t.stride(0))
 
 
-def _split_for(m: int, n: int, k: int, target_ctas: int = 296) -> int:
-    """Split-K factor for a float32 GEMM: enough CTAs for two per SM, >= 4 k-tiles each."""
+def _split_for(m: int, n: int, k: int, target_units: int = 148) -> int:
+    """Split-K factor for a float32 GEMM: at least one tile per SM of the persistent
+    kernel (tiles are 128 x 256, or 128 x 128 when n is not a multiple of 256), keeping
+    >= 8 k-tiles of 64 per split."""
     k_tiles = k // 64
-    tiles = (m // 128) * (n // 128)
+    tiles = (m // 128) * (n // (256 if n % 256 == 0 else 128))
     s = 1
-    while tiles * s < target_ctas and k_tiles % (2 * s) == 0 and k_tiles // (2 * s) >= 4:
+    while tiles * s < target_units and k_tiles % (2 * s) == 0 and k_tiles // (2 * s) >= 8:
         s *= 2
     return s
 

@@ -40,7 +40,10 @@ def _tol(a, b):
 
 
 @pytest.mark.parametrize("m,n,k,split", [(128, 128, 64, 1), (256, 384, 512, 1), (384, 256, 1024, 4),
-                                         (1024, 1024, 1024, 2)])
+                                         (1024, 1024, 1024, 2),
+                                         # more tiles than SMs: each persistent CTA reuses both accumulators
+                                         (4096, 2048, 512, 1), (8192, 384, 256, 1), (38400, 256, 128, 1),
+                                         (1024, 1024, 4096, 8)])
 def test_gemm_f32_matches_float64(cuda, m, n, k, split):
     g = torch.Generator().manual_seed(m + n + k)
     a, b = _bf((m, k), g), _bf((n, k), g)
