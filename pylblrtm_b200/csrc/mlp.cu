@@ -13,10 +13,10 @@
 //                    into one of two tensor-memory accumulators and frees the stage
 //                    with tcgen05.commit on its "empty" mbarrier; a finished tile is
 //                    signalled on the accumulator's "tmem_full" mbarrier;
-//   warps 2-5        (the epilogue) read their 32 accumulator rows each with
-//                    tcgen05.ld, apply the epilogue, store, and release the accumulator
-//                    ("tmem_empty", one arrival per warp), so the epilogue of one tile
-//                    overlaps the main loop of the next.
+//   warps 2-9        (the epilogue, two per SM sub-partition) each read 32 accumulator
+//                    rows x half the columns with tcgen05.ld, apply the epilogue, store,
+//                    and release the accumulator ("tmem_empty", one arrival per warp), so
+//                    the epilogue of one tile overlaps the main loop of the next.
 // Split-K (n_split > 1) is offered for the float32 mode only: split z writes its partial
 // sum to out_f32 + z * split_stride and the consumer adds the partials in a fixed order
 // (deterministic).
@@ -36,7 +36,9 @@ namespace lbl {
 
 constexpr int GM = 128, GK = 64, GSTAGES = 4;
 constexpr int G_A_BYTES = GM * GK * 2;                             // 16 KiB A tile per stage
-constexpr int G_THREADS = 192;                                     // TMA, MMA, 4 epilogue warps
+constexpr int G_EPI_WARPS = 8;                                     // 2 per SM sub-partition
+constexpr int G_EPI_GROUPS = G_EPI_WARPS / 4;                      // column groups of a tile
+constexpr int G_THREADS = 64 + 32 * G_EPI_WARPS;                   // TMA warp, MMA warp, epilogue
 constexpr unsigned long long G_WAIT_NS = 2000000000ull;            // 2 s per wait at most
 
 template <int BN>
@@ -193,7 +195,7 @@ __device__ __forceinline__ void epilogue16(const LblGemmEpilogue& ep, int split,
   } else if (ep.mode == LBL_GEMM_BIAS_SIGMOID) {
     float p[16];
 #pragma unroll
-    for (int i = 0; i < 16; ++i) p[i] = 1.0f / (1.0f + __expf(-(v[i] + ep.bias[col + i])));
+    for (int i = 0; i < 16; ++i) p[i] = __fdividef(1.0f, 1.0f + __expf(-(v[i] + ep.bias[col + i])));
     if (ep.out_f32) {
       float4* d = reinterpret_cast<float4*>(ep.out_f32 + (long long)row * ep.ld_f32 + col);
 #pragma unroll
@@ -260,7 +262,7 @@ gemm_bf16_kernel(const __grid_constant__ CUtensorMap map_a, const __grid_constan
     }
     for (int i = 0; i < 2; ++i) {
       mbar_init(smem_u32(&tfull[i]), 1);
-      mbar_init(smem_u32(&tempty[i]), 4);
+      mbar_init(smem_u32(&tempty[i]), G_EPI_WARPS);
     }
     mbar_init(smem_u32(drain), 1);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
@@ -338,8 +340,10 @@ gemm_bf16_kernel(const __grid_constant__ CUtensorMap map_a, const __grid_constan
       umma_commit(smem_u32(drain));            // arrives once every MMA issued above has finished
       if (!mbar_wait(smem_u32(drain), 0)) *fail = 1;
     }
-  } else {                                     // epilogue warps 2..5: tensor-memory lanes 32 * (warp % 4)
+  } else {  // epilogue warps: tensor-memory lanes 32 * (warp % 4), column group (warp - 2) / 4
     const int q = warp & 3;
+    const int cg = (warp - 2) >> 2;
+    constexpr int CW = BN / G_EPI_GROUPS;      // columns per group
     int i = 0;
     for (int u = blockIdx.x; u < units; u += gridDim.x, ++i) {
       const int b = i & 1;
@@ -355,7 +359,7 @@ gemm_bf16_kernel(const __grid_constant__ CUtensorMap map_a, const __grid_constan
       const int row = m0 + q * 32 + lane;
       const uint32_t base = tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(b * BN);
 #pragma unroll 1
-      for (int c0 = 0; c0 < BN; c0 += 16) {
+      for (int c0 = cg * CW; c0 < (cg + 1) * CW; c0 += 16) {
         float v[16];
         tmem_ld16(base + (uint32_t)c0, v);
         epilogue16(ep, split, row, n0 + c0, v, loss);

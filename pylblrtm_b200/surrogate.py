@@ -317,7 +317,9 @@ class MLP:
                   ws.err.data_ptr(), stream)
         self.launches += 1
 
-    def _forward(self, ws: _Workspace, stream, train: bool) -> None:
+    def _forward(self, ws: _Workspace, stream, train: bool, out=None) -> None:
+        """Forward pass; inference writes the sigmoid output to ``out`` (float32
+        [B, n_out padded], row stride n_out padded) or to the workspace."""
         B = ws.batch
         L = len(self.dims)
         _lib.call("lbl_pack_inputs_bf16", ws.raw.data_ptr(), B, self.n_in, self.mean.data_ptr(),
@@ -343,7 +345,7 @@ class MLP:
                     ep.y_t, ep.ld_yt = ws.dzt[li].data_ptr(), B
                     ep.loss = ws.loss.data_ptr()
                 else:
-                    ep.out_f32, ep.ld_f32 = ws.out.data_ptr(), n
+                    ep.out_f32, ep.ld_f32 = (ws.out if out is None else out).data_ptr(), n
             self._gemm(ws.map_x[li], self.map_w[li], B, n, k, ep, ws, stream)
 
     def _backward(self, ws: _Workspace, stream) -> None:
@@ -467,8 +469,7 @@ class GatedSurrogate:
             ws.raw[:B].copy_(raw)
             if Bp > B:
                 ws.raw[B:].zero_()
-            net._forward(ws, stream, False)
-            pred[m].copy_(ws.out)
+            net._forward(ws, stream, False, out=pred[m])
             self.launches += net.launches
         mean = torch.empty((B, net0.n_out), dtype=torch.float32, device=net0.dev)
         est = torch.empty((B,), dtype=torch.float32, device=net0.dev)

@@ -157,6 +157,33 @@ def run(n_train: int = 100_000, n_eval: int = 65_536, ood: float = 0.05, steps: 
     return rep
 
 
+def infer_only(batch: int, members: int = 4, hidden: int = 1024, depth: int = 4, reps: int = 5,
+               seed: int = 0) -> dict:
+    """Surrogate-only inference timing with randomly initialised members (no engine, no
+    training): the cost of the ensemble and gate on ``batch`` profiles."""
+    import torch
+    problem = surrogate.SurrogateProblem()
+    nets = [surrogate.MLP(61, problem.n_channels, hidden=hidden, depth=depth, seed=seed + m)
+            for m in range(members)]
+    feats = surrogate.sample_profiles(batch, seed=seed).features()
+    for n in nets:
+        n.set_normalisation(feats.mean(0), feats.std(0))
+    gs = surrogate.GatedSurrogate(nets)
+    raw = torch.as_tensor(feats, device=nets[0].dev)
+    gs.ensemble(raw)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(reps):
+        gs.ensemble(raw)
+    e1.record()
+    torch.cuda.synchronize()
+    t = e0.elapsed_time(e1) / 1e3 / reps
+    flops = 2 * sum(k * n for k, n in nets[0].dims) * members * batch
+    return {"profiles": batch, "members": members, "seconds": t, "spectra_per_s": batch / t,
+            "tflops": flops / t / 1e12, "launches": gs.launches}
+
+
 def main(argv=None) -> None:
     ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
     ap.add_argument("--train", type=int, default=100_000)
@@ -174,8 +201,14 @@ def main(argv=None) -> None:
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--infer-batch", type=int, default=0)
     ap.add_argument("--profiles-per-launch", type=int, default=256)
+    ap.add_argument("--infer-only", action="store_true",
+                    help="only time surrogate inference on --infer-batch profiles (random weights)")
     ap.add_argument("--out", default=None)
     a = ap.parse_args(argv)
+    if a.infer_only:
+        rep = infer_only(a.infer_batch or 65536, a.members, a.hidden, a.depth, seed=a.seed)
+        print(json.dumps(rep))
+        return
     rep = run(a.train, a.eval, a.ood, a.steps, a.members, a.batch, a.hidden, a.depth, a.lr, a.strength_scale,
               a.lines, a.gate, a.seed, profiles_per_launch=a.profiles_per_launch, infer_batch=a.infer_batch)
     text = json.dumps(rep, indent=1)
