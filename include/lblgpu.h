@@ -221,7 +221,7 @@ int lbl_faddeeva_f32(const float* x, const float* y, long long n, float* re, flo
 typedef struct {
   int mode;
   int n_valid;                  /* SIGMOID: columns >= n_valid are padding */
-  const float* bias;            /* [N] */
+  const float* bias;            /* [N], 16-byte aligned */
   float* out_f32;               /* [M, ld_f32] (per split for LBL_GEMM_F32) */
   long long ld_f32;
   long long split_stride;       /* elements between split partials */

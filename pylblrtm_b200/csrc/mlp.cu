@@ -186,16 +186,28 @@ __device__ __forceinline__ void epilogue16(const LblGemmEpilogue& ep, int split,
     for (int i = 0; i < 4; ++i) d[i] = make_float4(v[4 * i], v[4 * i + 1], v[4 * i + 2], v[4 * i + 3]);
     return;
   }
+  float bias[16];
+  if (ep.mode == LBL_GEMM_BIAS_GELU || ep.mode == LBL_GEMM_BIAS_SIGMOID) {   // four 16-byte loads (broadcast)
+    const float4* b4 = reinterpret_cast<const float4*>(ep.bias + col);
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      const float4 t = __ldg(b4 + i);
+      bias[4 * i] = t.x;
+      bias[4 * i + 1] = t.y;
+      bias[4 * i + 2] = t.z;
+      bias[4 * i + 3] = t.w;
+    }
+  }
   if (ep.mode == LBL_GEMM_BIAS_GELU) {
 #pragma unroll
-    for (int i = 0; i < 16; ++i) v[i] += ep.bias[col + i];
+    for (int i = 0; i < 16; ++i) v[i] += bias[i];
     if (ep.z_out) store_row16((__nv_bfloat16*)ep.z_out + (long long)row * ep.ld_z + col, v);
 #pragma unroll
     for (int i = 0; i < 16; ++i) v[i] = gelu(v[i]);
   } else if (ep.mode == LBL_GEMM_BIAS_SIGMOID) {
     float p[16];
 #pragma unroll
-    for (int i = 0; i < 16; ++i) p[i] = __fdividef(1.0f, 1.0f + __expf(-(v[i] + ep.bias[col + i])));
+    for (int i = 0; i < 16; ++i) p[i] = __fdividef(1.0f, 1.0f + __expf(-(v[i] + bias[i])));
     if (ep.out_f32) {
       float4* d = reinterpret_cast<float4*>(ep.out_f32 + (long long)row * ep.ld_f32 + col);
 #pragma unroll
@@ -550,7 +562,7 @@ extern "C" int lbl_gemm_bf16(const void* map_a, const void* map_b, int M, int N,
   const bool needs_f32 = ep->mode == LBL_GEMM_F32;
   if ((needs_f32 && (!ep->out_f32 || ep->ld_f32 < N || ep->ld_f32 % 4 ||
                      (n_split > 1 && ep->split_stride < (long long)M * ep->ld_f32))) ||
-      (ep->mode != LBL_GEMM_F32 && ep->mode != LBL_GEMM_DGELU && !ep->bias) ||
+      (ep->mode != LBL_GEMM_F32 && ep->mode != LBL_GEMM_DGELU && (!ep->bias || ((uintptr_t)ep->bias) % 16)) ||
       (ep->mode == LBL_GEMM_DGELU && (!ep->z_in || ep->ld_zin < N || ep->ld_zin % 8)) ||
       (ep->z_out && (ep->ld_z < N || ep->ld_z % 8)) || (ep->y && (ep->ld_y < N || ep->ld_y % 8)) ||
       (ep->y_t && ep->ld_yt < M) || (ep->mode == LBL_GEMM_BIAS_SIGMOID && ep->out_f32 && ep->ld_f32 % 4) ||
