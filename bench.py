@@ -55,6 +55,7 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-adjoint", action="store_true", help="skip the Jacobian timing")
     ap.add_argument("--no-surrogate", action="store_true", help="skip the gated-surrogate timing")
+    ap.add_argument("--no-accuracy", action="store_true", help="skip the accuracy checks")
     ap.add_argument("--nu-min", type=float, default=600.0, help="grid start (smaller cases for profiling)")
     ap.add_argument("--nu-max", type=float, default=2500.0, help="grid end (smaller cases for profiling)")
     return ap.parse_args()
@@ -233,6 +234,42 @@ def adjoint_timing(torch, steps: int = 3):
             "forward_ms": fwd, "jacobian_ms": jac, "vjp_ms": vjp, "jacobian_over_forward": jac / fwd}
 
 
+def _errors(torch, t_test, t_ref, tau_test, tau_ref):
+    """max |dT|, max and median relative tau error (points with tau_ref > 1e-12)."""
+    t_test, t_ref = torch.as_tensor(t_test).double().cuda(), torch.as_tensor(t_ref).double().cuda()
+    tau_test, tau_ref = torch.as_tensor(tau_test).double().cuda(), torch.as_tensor(tau_ref).double().cuda()
+    m = tau_ref > 1e-12
+    rel = (tau_test[m] - tau_ref[m]).abs() / tau_ref[m]
+    return {"max_abs_dT": float((t_test - t_ref).abs().max()), "max_rel_tau": float(rel.max()),
+            "median_rel_tau": float(rel.median()), "points": int(t_ref.numel())}
+
+
+def accuracy(torch, job):
+    """Accuracy of the engines: the float32 engine against the float64 engine on the full
+    200k-line spectrum, and both against the reference's own outputs (golden vectors made
+    by running the reference) for the 2,000-line CO2 band at full strength (saturated) and
+    x 1e-3."""
+    from pylblrtm_b200 import engine, synthetic
+    r64 = job.run("fp64", mu=[0.8], want_od=False, want_tau=True, want_trans=True)
+    r32 = job.run("fp32", mu=[0.8], want_od=False, want_tau=True, want_trans=True)
+    out = {"three_gas_200k_fp32_vs_fp64": _errors(torch, r32.trans[0], r64.trans[0], r32.tau[0], r64.tau[0])}
+    gold_dir = os.path.join(os.path.dirname(os.path.abspath(__file__)), "tests", "golden")
+    for name, scale in (("co2_band_full", 1.0), ("co2_band_mid", 1e-3)):
+        g = np.load(os.path.join(gold_dir, f"{name}.npz"))
+        sd = synthetic.co2_band()
+        if scale != 1.0:
+            sd = synthetic.scale_strengths(sd, scale)
+        grid = engine.make_grid(float(g["nu_min"]), float(g["nu_max"]), float(g["step"]), float(g["tile"]))
+        j = engine.Job(sd, engine.layer_input_from_profile(synthetic.us_standard_atmosphere(["CO2"])), grid,
+                       float(g["cutoff"]))
+        res = {}
+        for prec in ("fp32", "fp64"):
+            r = j.run(prec, mu=[float(g["mu"])], want_od=False, want_tau=True, want_trans=True)
+            res[prec] = _errors(torch, r.trans[0], g["T"], r.tau[0], g["tau"])
+        out[f"{name}_vs_reference"] = res
+    return out
+
+
 def surrogate_timing():
     """Gated surrogate on the 20-layer, 650-1150 cm^-1, 2,000-channel workload, reduced.
 
@@ -360,6 +397,7 @@ def main():
     peak = fp32_peak(torch)
     adj = None if (a.no_adjoint or world > 1) else adjoint_timing(torch)
     sur = None if (a.no_surrogate or world > 1) else surrogate_timing()
+    acc = None if (a.no_accuracy or world > 1 or (a.nu_min, a.nu_max) != (600.0, 2500.0)) else accuracy(torch, job)
     tau_avg = sum(tau_ms) / len(tau_ms)
     # HBM-bound stages: algorithmic bytes / CUDA-event time
     hbm_peak = None
@@ -419,6 +457,7 @@ def main():
         "clocks": clocks.summary(),
         "e2e": e2e,
         "cpu_baseline": cpu,
+        "accuracy": acc,
         "hbm_kernels": hbm,
         "adjoint": adj,
         "surrogate": sur,

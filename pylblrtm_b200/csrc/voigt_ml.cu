@@ -287,8 +287,10 @@ tau_ml_kernel(const LineF32* __restrict__ prep, int n_lines, const int2* __restr
       }
       if (tid == 0) n_near_items += (unsigned long long)n_near;
     }
-    __syncthreads();
+    // No barrier here: the next round writes the staging arrays only after its first
+    // barrier, which every warp reaches after finishing this round.
   }
+  __syncthreads();   // near-pass atomics of the last round complete
 
   // ---- level-1 node values: reduce the 16-thread groups, then Chebyshev coefficients
   s_red[tid] = (double)sum1 - (double)comp1;

@@ -349,8 +349,10 @@ jac_ml_kernel(const LineF32* __restrict__ prep, const LineJac* __restrict__ jpre
         atomicAdd(&s_core[2][p], a[2] - b[2]);
       }
     }
-    __syncthreads();
+    // No barrier here: the next round writes the staging arrays only after its first
+    // barrier, which every warp reaches after finishing this round.
   }
+  __syncthreads();   // every warp is done with s1 (aliased by s_red) and the near-pass atomics
 
   // level-1 node values (reduce the 16-thread groups) and Chebyshev coefficients
 #pragma unroll
