@@ -44,6 +44,13 @@ FLOPS_CHEB_PER_POINT = 128   # two 16-term Clenshaw sums per point and layer
 CPU_SAMPLE = (1000.0, 1000.5)  # sub-window timed on the host (all 60 layers)
 
 
+# DRAM traffic of one tau_ml_kernel launch on the default workload (200k lines, 60 layers,
+# 600-2500 cm^-1), from a single-pass ncu capture of that launch
+# (dram__bytes_read.sum 386.22 MB + dram__bytes_write.sum 419.19 MB): the 384 MB of line
+# records read once and the 456 MB optical-depth output, part of which stays in L2.
+TAU_ML_DRAM_BYTES = 386.22e6 + 419.19e6
+
+
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -340,6 +347,7 @@ def main():
     # evaluation count of one spectrum (the reference tile rule), from the kernel's own counter
     r0 = job.run(a.precision, mu=[0.8], want_od=False, want_trans=True, count_evals=True)
     evals_per_step = r0.evals
+    r0_lines_bytes = int(getattr(job, "last_prep_bytes", 0))
     work_per_step = r0.work          # Faddeeva evaluations the kernel actually performs
     launches_per_step = job.launches
 
@@ -446,7 +454,13 @@ def main():
                    "grid_points": grid.n_nu, "parallelism": f"replicas{world}" if world > 1 else "single",
                    "l2": "inputs and outputs larger than L2 (line records 384 MB, od 456 MB)"},
         "roofline": {"bound": "fp32", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
-                     "frac": achieved / peak, "traffic": None,
+                     "frac": achieved / peak,
+                     "traffic": TAU_ML_DRAM_BYTES if (a.precision == "fp32" and (a.nu_min, a.nu_max) ==
+                                                      (600.0, 2500.0)) else None,
+                     "traffic_unit": "bytes per launch (ncu dram__bytes_read.sum + dram__bytes_write.sum)",
+                     "algorithmic_bytes": r0_lines_bytes + job.n_prof * job.n_lay * grid.n_nu * 4,
+                     "algorithmic_bytes_rule": "32-B prepared line record per (layer, line) read once + "
+                                               "float32 od written once per (layer, point)",
                      "kernel": {"fp32": "tau_ml_kernel", "fp32-direct": "tau_f32_kernel",
                                 "fp64": "tau_f64_kernel"}[a.precision],
                      "faddeeva_evals_per_launch": work_per_step,

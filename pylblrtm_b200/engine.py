@@ -477,6 +477,7 @@ class Job:
         od = torch.empty((n_prof, n_lay, n_nu), dtype=od_dtype, device=dev)
         rec = _lib.SIZEOF_LINE_F32 if single else _lib.SIZEOF_LINE_F64
         prep = torch.empty((n_rows * n_kept * rec // 8,), dtype=torch.float64, device=dev)
+        self.last_prep_bytes = n_rows * n_kept * rec          # prepared line records of the summation
         if timer is not None:
             p0, p1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             p0.record()
