@@ -106,6 +106,7 @@ tau_ml_kernel(const LineF32* __restrict__ prep, int n_lines, const int2* __restr
   const long long c0 = t0 + (long long)chunk * (blockDim.x * P);
   if (c0 >= t1) return;
   const int n_c = (int)(min(c0 + (long long)(blockDim.x * P), t1) - c0);
+  const int c0i = (int)c0;
   const double wlo = __dsub_rn(grid_nu(nu_min, step, t0), cutoff);
   const double whi = __dadd_rn(grid_nu(nu_min, step, t1 - 1), cutoff);
   const int2 rng = ranges[tile];
@@ -145,12 +146,13 @@ tau_ml_kernel(const LineF32* __restrict__ prep, int n_lines, const int2* __restr
     const bool have = base + tid < rng.y;
     if (base + blockDim.x + tid < rng.y) nxt = lp[base + blockDim.x + tid];
     const bool pass = have && (L.nuc >= wlo) && (L.nuc <= whi);
-    const float jf = (float)((long long)L.j0 - c0);
+    const float jf = (float)(L.j0 - c0i);           // |j0 - c0| < 1.5e9 (grid index span check)
     const bool lev1 = pass && use_l1 && (fabsf(jf - C1) - H1 > H1 + 1.f);
     const bool inner = pass && !lev1;
     // near range (points with possibly |z|^2 < MID_Z2) of an inner line, clipped to the chunk
     const float y2 = L.y * L.y;
-    const float hw = (y2 >= MID_Z2 && L.y >= 0.f) ? -1.0f : sqrtf(fmaxf(MID_Z2 - y2, 0.f)) / L.a + 1.0f;
+    float hw = -1.0f;                               // near half-width in points (inner lines only)
+    if (inner && !(y2 >= MID_Z2 && L.y >= 0.f)) hw = sqrtf(fmaxf(MID_Z2 - y2, 0.f)) / L.a + 1.0f;
     int near_lo = 0, near_n = 0;
     unsigned l3mask = 0;
     if (inner) {
@@ -194,7 +196,8 @@ tau_ml_kernel(const LineF32* __restrict__ prep, int n_lines, const int2* __restr
     if (pass) {
       MlLine r;
       r.g = make_float4(lev1 ? C1 - jf : jf, L.a, L.b, L.amp_far);
-      const float clamp_val = L.amp_far * mid_clamped_term(0.f, y2);   // r = 1/MID_Z2 when y2 < MID_Z2
+      float clamp_val = 0.f;                          // used by level 3 only
+      if (!lev1) clamp_val = L.amp_far * mid_clamped_term(0.f, y2);   // r = 1/MID_Z2 when y2 < MID_Z2
       r.h = make_float4(L.y, y2, L.amp, clamp_val);
       const unsigned lt = (1u << lane) - 1u;
       if (lev1) {
@@ -270,9 +273,12 @@ tau_ml_kernel(const LineF32* __restrict__ prep, int n_lines, const int2* __restr
     // |z|^2 < MID_Z2 there; x is formed exactly as in the loop, so the clamped value
     // cancels. Consecutive threads take consecutive points of a line.
     {
-      int l = 0;
       for (int i = tid; i < n_near; i += blockDim.x) {
-        while (s_seg_start[l + 1] <= i) ++l;
+        int l = 0, hi = n2;                               // largest l with s_seg_start[l] <= i
+        while (hi - l > 1) {
+          const int mid = (l + hi) >> 1;
+          if (s_seg_start[mid] <= i) l = mid; else hi = mid;
+        }
         const int p = s_seg_lo[l] + (i - s_seg_start[l]);
         if (!((s_seg_mask[l] >> (p >> 8)) & 1u)) continue;   // level 2 for the owning warp
         const MlLine R = s2[l];
@@ -358,7 +364,7 @@ extern "C" int lbl_tau_tiles_ml_f32(const LineF32* prep, int n_lines, const int*
                                     double cutoff, int n_grp, float* od, int* err, unsigned long long* evals,
                                     unsigned long long* work, void* stream) {
   if (!prep || !ranges || !t_layer || !od || n_lines < 1 || n_rows < 1 || n_rows > 65535 || n_nu < 1 ||
-      tile_samples < 1 || !(step > 0) || !(cutoff >= 0) || n_grp < 1)
+      n_nu > 1500000000LL || tile_samples < 1 || !(step > 0) || !(cutoff >= 0) || n_grp < 1)
     return lbl_set_error(LBL_EINVAL, "lbl_tau_tiles_ml_f32: bad arguments");
   const int per_tile = tile_samples < ML_CHUNK ? tile_samples : ML_CHUNK;
   const int threads = 32 * ((per_tile + ML_WARP_PTS - 1) / ML_WARP_PTS);
