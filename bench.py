@@ -209,36 +209,50 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(sm)}
 
 
-def adjoint_timing(torch, steps: int = 3):
-    """Forward vs full per-layer Jacobian on one profile of the Jacobian workload.
+def adjoint_timing(torch, steps: int = 3, n_batch: int = 256, chunk: int = 32):
+    """Forward vs full per-layer Jacobians on the Jacobian workload.
 
-    Lines of the 200k-line set in 1000-1200 cm^-1, the 60-layer profile, grid
-    1000-1200 cm^-1 at 0.001, d/dT_layer and d/dlnVMR_layer(H2O). Times include
-    every device stage of each call (CUDA events, inputs resident).
+    Lines of the 200k-line set in 1000-1200 cm^-1, grid 1000-1200 cm^-1 at 0.001, mu 0.8;
+    d/dT_layer and d/dlnVMR_layer(H2O). (1) one profile (the 60-layer base), every device
+    stage of each call; (2) the batch of 256 profiles (base + correlated N(0, 5 K)
+    temperature perturbations, H2O x exp(N(0, 0.3))) through the public batched APIs in
+    chunks of 32 profiles: transmittance only vs transmittance + Jacobians. CUDA events,
+    inputs on the host (the batched calls include their uploads).
     """
-    from pylblrtm_b200 import engine, synthetic
+    from pylblrtm_b200 import adjoint, batch, engine, synthetic
     sd = synthetic.restrict(synthetic.three_gas_lines(), 1000.0, 1200.0)
     grid = engine.make_grid(1000.0, 1200.0, 0.001, 2.0)
     job = engine.Job(sd, engine.layer_input_from_profile(synthetic.logp_profile()), grid, 25.0)
     g = torch.ones((1, grid.n_nu), dtype=torch.float64, device="cuda")
 
-    def timed(fn):
+    def timed(fn, reps=steps):
         fn()
         torch.cuda.synchronize()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record()
-        for _ in range(steps):
+        for _ in range(reps):
             fn()
         e1.record()
         torch.cuda.synchronize()
-        return e0.elapsed_time(e1) / steps
+        return e0.elapsed_time(e1) / reps
 
     fwd = timed(lambda: job.run("fp32", want_od=True))
     jac = timed(lambda: job.jacobian("H2O"))
     vjp = timed(lambda: job.jacobian("H2O", g_tau=g))
+    lv = synthetic.perturbed_levels(synthetic.logp_levels(), n_batch, seed=4242)
+    gases = ("H2O", "CO2", "O3")
+    vmr = {k: lv[k] for k in gases}
+    bf = timed(lambda: batch.transmittance_batch(sd, lv["p"], lv["t"], vmr, 1000.0, 1200.0, mu_view=0.8,
+                                                 profiles_per_launch=chunk, as_numpy=False), reps=1)
+    bj = timed(lambda: adjoint.layer_jacobians_batch(sd, lv["p"], lv["t"], vmr, 1000.0, 1200.0, mu_view=0.8,
+                                                     profiles_per_launch=chunk, on_chunk=lambda sl, out: None),
+               reps=1)
     return {"workload": "lines 1000-1200 cm^-1 of the 200k-line set, 60 layers, grid 1000-1200 at 0.001",
-            "outputs": "od + d tau/dT_layer + d tau/dlnVMR_layer(H2O), [60, 200001] each",
-            "forward_ms": fwd, "jacobian_ms": jac, "vjp_ms": vjp, "jacobian_over_forward": jac / fwd}
+            "outputs": "od + d tau/dT_layer + d tau/dlnVMR_layer(H2O), [60, 200001] each per profile",
+            "forward_ms": fwd, "jacobian_ms": jac, "vjp_ms": vjp, "jacobian_over_forward": jac / fwd,
+            "batch": {"profiles": n_batch, "chunk": chunk, "forward_ms": bf, "jacobian_ms": bj,
+                      "jacobian_over_forward": bj / bf, "forward_profiles_per_s": n_batch / bf * 1e3,
+                      "jacobian_profiles_per_s": n_batch / bj * 1e3}}
 
 
 def _errors(torch, t_test, t_ref, tau_test, tau_ref):

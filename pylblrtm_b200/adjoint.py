@@ -14,7 +14,7 @@ recomputes the Voigt values instead of storing the Jacobian.
 from __future__ import annotations
 
 from dataclasses import dataclass
-from typing import Dict, Sequence
+from typing import Dict, Optional, Sequence
 
 import numpy as np
 
@@ -46,6 +46,71 @@ def layer_jacobians(spectral_data: SpectralData, profile: AtmosphericProfile, nu
     if as_numpy:
         out = {k: (v if isinstance(v, np.ndarray) else v.double().cpu().numpy()) for k, v in out.items()}
     return out
+
+
+def layer_jacobians_batch(spectral_data: SpectralData, pressure_hpa, temperature_k, vmr: Dict[str, object],
+                          nu_min_cm1: float, nu_max_cm1: float, *, step_cm1: float = 0.001,
+                          line_cutoff_cm1: float = 25.0, tile_width_cm1: float = 2.0, gas: str = "H2O",
+                          mu_view=1.0, profiles_per_launch: int = 32, on_chunk=None) -> Optional[Dict[str, object]]:
+    """Transmittance and per-layer Jacobians of a batch of level profiles.
+
+    ``pressure_hpa``, ``temperature_k`` and every ``vmr[gas]`` are ``[n, n_levels]``
+    (TOA first, validated like ``transmittance_batch``); ``mu_view`` is a scalar or one
+    value per profile. For each chunk of ``profiles_per_launch`` profiles the device
+    computes ``od``, ``dtau_dT`` and ``dtau_dlnvmr`` ``[m, n_layers, n_nu]`` (float32)
+    and ``trans`` ``[m, n_nu]`` = exp(-sum_k od_k / mu) (float64). With ``on_chunk``
+    each chunk is handed to ``on_chunk(profile_slice, outputs)`` as device tensors and
+    nothing is kept (for batches whose Jacobians exceed device memory); otherwise the
+    chunks are concatenated on the device and returned with ``nu``.
+    """
+    import torch
+    from .batch import _validate_levels
+    if not isinstance(spectral_data, SpectralData):
+        raise TypeError("spectral_data must be a SpectralData instance")
+    p = np.atleast_2d(np.asarray(pressure_hpa, dtype=np.float64))
+    t = np.atleast_2d(np.asarray(temperature_k, dtype=np.float64))
+    gases = list(vmr.keys())
+    v = {g: np.atleast_2d(np.asarray(vmr[g], dtype=np.float64)) for g in gases}
+    _validate_levels(p, t, v)
+    if gas not in v:
+        raise ValueError(f"gas '{gas}' is not in vmr")
+    if nu_min_cm1 >= nu_max_cm1:
+        raise ValueError("nu_min_cm1 must be strictly less than nu_max_cm1")
+    if step_cm1 <= 0:
+        raise ValueError("step_cm1 must be positive")
+    n = p.shape[0]
+    mu = np.broadcast_to(np.asarray(mu_view, dtype=np.float64), (n,)).copy()
+    if not np.all((mu > 0.0) & (mu <= 1.0)):
+        raise ValueError("mu_view must be in (0, 1]")
+    if profiles_per_launch < 1:
+        raise ValueError("profiles_per_launch must be >= 1")
+    grid = engine.make_grid(nu_min_cm1, nu_max_cm1, step_cm1, tile_width_cm1)
+    vmr_all = np.stack([v[g] for g in gases], axis=1)
+    keep = []
+    for b0 in range(0, n, profiles_per_launch):
+        sl = slice(b0, min(n, b0 + profiles_per_launch))
+        li = engine.LayerInput(gases=gases, levels_p=p[sl], levels_t=t[sl], levels_vmr=vmr_all[sl])
+        job = engine.Job(spectral_data, li, grid, float(line_cutoff_cm1), warn_level=3)
+        od, d_t, d_v = job.jacobian(gas)
+        m = od.shape[0]
+        trans = torch.empty((m, grid.n_nu), dtype=torch.float64, device=od.device)
+        mu_d = torch.as_tensor(mu[sl], device=od.device)
+        if od.shape[1] > 0:
+            from . import _lib
+            _lib.call("lbl_layer_sum_exp_f32", od.data_ptr(), m, od.shape[1], grid.n_nu, mu_d.data_ptr(),
+                      trans.data_ptr(), 0, torch.cuda.current_stream().cuda_stream)
+        else:
+            trans.fill_(1.0)
+        out = {"od": od, "dtau_dT": d_t, "dtau_dlnvmr": d_v, "trans": trans}
+        if on_chunk is not None:
+            on_chunk(sl, out)
+        else:
+            keep.append(out)
+    if on_chunk is not None:
+        return None
+    res = {k: torch.cat([c[k] for c in keep]) for k in keep[0]}
+    res["nu"] = grid.nu
+    return res
 
 
 @dataclass
