@@ -8,7 +8,8 @@ Steps (all on one GPU):
      float32 line-by-line engine: the training targets;
   2. train a 4-member ensemble (61 -> 1024 x 4 -> 2000, BF16, Adam, batch 4096);
   3. draw ``--eval`` fresh profiles plus a fraction ``--ood`` shifted by +25 K, compute
-     their engine spectra (the judge of the surrogate and the engine's own spectra/s),
+     their engine spectra (the reference values for the surrogate's errors, and the engine's
+     own spectra/s),
      run the ensemble (surrogate-only spectra/s), and the gated path that recomputes
      flagged profiles with the engine (blended spectra/s);
   4. report per-profile maximum channel errors (quantiles, fraction <= 1e-3) for the
