@@ -24,6 +24,9 @@
 extern "C" {
 #endif
 
+/* flags of the multi-level summation and Jacobian kernels */
+#define LBL_DETERMINISTIC 1   /* bit-reproducible near-zone sums (fixed order; ~10-15 % slower) */
+
 /* status codes */
 #define LBL_OK 0
 #define LBL_EINVAL 1    /* bad argument (message in lbl_last_error) */
@@ -161,10 +164,15 @@ int lbl_tau_tiles_f32(const LineF32* prep, int n_lines, const int* ranges, const
  * half-width through 16 nodes over that sub-chunk, the rest directly. evals
  * counts reference-rule evaluations; work (nullable, 3 x u64) receives the
  * evaluations actually performed: [0] Chebyshev-node evaluations, [1] level-3
- * loop evaluations, [2] near-zone points. Replaces pylblrtm/forward.py:295-315. */
+ * loop evaluations, [2] near-zone points. flags: LBL_DETERMINISTIC adds the
+ * near-zone corrections in a fixed order (bit-reproducible across launches and
+ * batchings); without it overlapping near zones are summed by shared-memory
+ * atomics (reproducible to ~1e-9 relative). n_nu <= 1.5e9. Replaces
+ * pylblrtm/forward.py:295-315. */
 int lbl_tau_tiles_ml_f32(const LineF32* prep, int n_lines, const int* ranges, const double* t_layer, int n_rows,
                          double nu_min, double step, long long n_nu, int tile_samples, double cutoff, int n_grp,
-                         float* od, int* err, unsigned long long* evals, unsigned long long* work, void* stream);
+                         float* od, int* err, unsigned long long* evals, unsigned long long* work, int flags,
+                         void* stream);
 
 /* Layer Jacobians by the multi-level float32 summation (no reference
  * counterpart; the retrieval adjoint): writes od (as lbl_tau_tiles_ml_f32),
@@ -174,11 +182,12 @@ int lbl_tau_tiles_ml_f32(const LineF32* prep, int n_lines, const int* ranges, co
  * tau = sum_k od_k. With g_tau ([n_prof, n_nu] float64, d loss / d tau) the
  * kernel writes nothing per point and instead adds sum_p g_tau * d_t (d_v) into
  * vjp_t[row] (vjp_v[row]) (caller zeroes them): the vector-Jacobian product,
- * recomputing every Voigt value instead of storing the Jacobian. */
+ * recomputing every Voigt value instead of storing the Jacobian (its per-row
+ * sums use global atomics). flags: LBL_DETERMINISTIC as for lbl_tau_tiles_ml_f32. */
 int lbl_jacobian_ml_f32(const LineF32* prep, const LineJac* jprep, int n_lines, const int* ranges,
                         const double* t_layer, int n_rows, int n_lay, double nu_min, double step, long long n_nu,
                         int tile_samples, double cutoff, float* od, float* d_t, float* d_v, const double* g_tau,
-                        double* vjp_t, double* vjp_v, void* stream);
+                        double* vjp_t, double* vjp_v, int flags, void* stream);
 
 /* Column sums over layers and transmittance exp(-tau / mu); replaces
  * pylblrtm/forward.py:151 and config.py:266-270. od: [n_prof, n_lay, n_nu]

@@ -14,6 +14,7 @@ import threading
 LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "liblblgpu.so")
 
 LBL_OK = 0
+LBL_DETERMINISTIC = 1    # flag of the multi-level summation and Jacobian kernels
 
 # byte sizes of the records declared in include/lblgpu.h
 SIZEOF_LAYER_GROUP = 48
@@ -44,9 +45,9 @@ SIGNATURES = {
     "lbl_line_prep_f32": (_I, [_P, _P, _I, _P, _I, _I, _D, _D, _P, _P, _P]),
     "lbl_tau_tiles_f64": (_I, [_P, _I, _P, _P, _I, _D, _D, _L, _I, _D, _I, _P, _P, _P, _P]),
     "lbl_tau_tiles_f32": (_I, [_P, _I, _P, _P, _I, _D, _D, _L, _I, _D, _I, _P, _P, _P, _P]),
-    "lbl_tau_tiles_ml_f32": (_I, [_P, _I, _P, _P, _I, _D, _D, _L, _I, _D, _I, _P, _P, _P, _P, _P]),
+    "lbl_tau_tiles_ml_f32": (_I, [_P, _I, _P, _P, _I, _D, _D, _L, _I, _D, _I, _P, _P, _P, _P, _I, _P]),
     "lbl_line_prep_jac": (_I, [_P, _I, _P, _I, _I, _P, _P, _P, _P, _I, _P, _P, _P]),
-    "lbl_jacobian_ml_f32": (_I, [_P, _P, _I, _P, _P, _I, _I, _D, _D, _L, _I, _D, _P, _P, _P, _P, _P, _P, _P]),
+    "lbl_jacobian_ml_f32": (_I, [_P, _P, _I, _P, _P, _I, _I, _D, _D, _L, _I, _D, _P, _P, _P, _P, _P, _P, _I, _P]),
     "lbl_layer_sum_exp_f32": (_I, [_P, _I, _I, _L, _P, _P, _P, _P]),
     "lbl_layer_sum_exp_f64": (_I, [_P, _I, _I, _L, _P, _P, _P, _P]),
     "lbl_channel_mean_f32": (_I, [_P, _I, _I, _L, _P, _L, _I, _I, _P, _P]),

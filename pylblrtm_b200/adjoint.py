@@ -25,7 +25,8 @@ from .spectral_data import SpectralData
 
 def layer_jacobians(spectral_data: SpectralData, profile: AtmosphericProfile, nu_min_cm1: float,
                     nu_max_cm1: float, *, step_cm1: float = 0.001, line_cutoff_cm1: float = 25.0,
-                    tile_width_cm1: float = 2.0, gas: str = "H2O", as_numpy: bool = True) -> Dict[str, object]:
+                    tile_width_cm1: float = 2.0, gas: str = "H2O", as_numpy: bool = True,
+                    deterministic: bool = False) -> Dict[str, object]:
     """Per-layer optical depth and its Jacobians for one profile.
 
     Returns ``nu`` [n], ``od`` [n_layers, n], ``dtau_dT`` [n_layers, n]
@@ -41,7 +42,7 @@ def layer_jacobians(spectral_data: SpectralData, profile: AtmosphericProfile, nu
     grid = engine.make_grid(nu_min_cm1, nu_max_cm1, step_cm1, tile_width_cm1)
     job = engine.Job(spectral_data, engine.layer_input_from_profile(profile), grid, float(line_cutoff_cm1),
                      warn_level=3)
-    od, d_t, d_v = job.jacobian(gas)
+    od, d_t, d_v = job.jacobian(gas, deterministic=deterministic)
     out = {"nu": grid.nu, "od": od[0], "dtau_dT": d_t[0], "dtau_dlnvmr": d_v[0]}
     if as_numpy:
         out = {k: (v if isinstance(v, np.ndarray) else v.double().cpu().numpy()) for k, v in out.items()}
@@ -51,7 +52,8 @@ def layer_jacobians(spectral_data: SpectralData, profile: AtmosphericProfile, nu
 def layer_jacobians_batch(spectral_data: SpectralData, pressure_hpa, temperature_k, vmr: Dict[str, object],
                           nu_min_cm1: float, nu_max_cm1: float, *, step_cm1: float = 0.001,
                           line_cutoff_cm1: float = 25.0, tile_width_cm1: float = 2.0, gas: str = "H2O",
-                          mu_view=1.0, profiles_per_launch: int = 32, on_chunk=None) -> Optional[Dict[str, object]]:
+                          mu_view=1.0, profiles_per_launch: int = 32, on_chunk=None,
+                          deterministic: bool = False) -> Optional[Dict[str, object]]:
     """Transmittance and per-layer Jacobians of a batch of level profiles.
 
     ``pressure_hpa``, ``temperature_k`` and every ``vmr[gas]`` are ``[n, n_levels]``
@@ -91,7 +93,7 @@ def layer_jacobians_batch(spectral_data: SpectralData, pressure_hpa, temperature
         sl = slice(b0, min(n, b0 + profiles_per_launch))
         li = engine.LayerInput(gases=gases, levels_p=p[sl], levels_t=t[sl], levels_vmr=vmr_all[sl])
         job = engine.Job(spectral_data, li, grid, float(line_cutoff_cm1), warn_level=3)
-        od, d_t, d_v = job.jacobian(gas)
+        od, d_t, d_v = job.jacobian(gas, deterministic=deterministic)
         m = od.shape[0]
         trans = torch.empty((m, grid.n_nu), dtype=torch.float64, device=od.device)
         mu_d = torch.as_tensor(mu[sl], device=od.device)

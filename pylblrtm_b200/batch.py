@@ -64,6 +64,7 @@ def transmittance_batch(
     channel_width_cm1: Optional[float] = None,
     profiles_per_launch: Optional[int] = None,
     as_numpy: bool = True,
+    deterministic: bool = False,
 ) -> Tuple[np.ndarray, object]:
     """Transmittance of a batch of profiles.
 
@@ -71,7 +72,8 @@ def transmittance_batch(
     ``[n_profiles, n_levels]`` (TOA first); ``mu_view`` is a scalar or one value
     per profile. Returns ``(nu, T[n_profiles, n_nu])`` or, with
     ``channel_width_cm1``, ``(channel_centres, T[n_profiles, n_channels])``.
-    ``as_numpy=False`` keeps the result on the device (a torch tensor).
+    ``as_numpy=False`` keeps the result on the device (a torch tensor);
+    ``deterministic`` as in ``compute_transmittance``.
     """
     if not isinstance(spectral_data, SpectralData):
         raise TypeError("spectral_data must be a SpectralData instance")
@@ -105,7 +107,8 @@ def transmittance_batch(
         b1 = min(b0 + chunk, n_prof)
         li = engine.LayerInput(gases=gases, levels_p=p[b0:b1], levels_t=t[b0:b1], levels_vmr=vmr_all[b0:b1])
         job = engine.Job(spectral_data, li, grid, float(line_cutoff_cm1), warn_level=3)
-        res = job.run(precision, mu=mu[b0:b1], want_od=False, want_trans=channels is None, channels=channels)
+        res = job.run(precision, mu=mu[b0:b1], want_od=False, want_trans=channels is None, channels=channels,
+                      deterministic=deterministic)
         outs.append(res.channels if channels is not None else res.trans)
     out = torch.cat(outs, dim=0) if len(outs) > 1 else outs[0]
     if channels is not None:

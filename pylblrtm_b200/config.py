@@ -3,7 +3,7 @@
 Same defaults, merge, validation, result container and writers as the
 reference (``config.py:23-319``); the optical depth comes from the GPU engine.
 An optional ``engine`` section (ignored by the reference) selects the
-precision: ``engine: {precision: fp32|fp64}``.
+precision: ``engine: {precision: fp32|fp32-direct|fp64, deterministic: false|true}``.
 """
 
 from __future__ import annotations
@@ -79,6 +79,9 @@ def _validate(cfg: dict) -> None:
     fmt = out["save"]["format"]
     if fmt not in {"npz", "csv", "txt"}:
         raise ValueError(f"output.save.format must be 'npz', 'csv', or 'txt'; got '{fmt}'")
+    det = cfg.get("engine", {}).get("deterministic", False)
+    if not isinstance(det, bool):
+        raise ValueError(f"engine.deterministic must be true or false; got '{det}'")
     prec = cfg.get("engine", {}).get("precision", DEFAULT_PRECISION)
     if prec not in engine.PRECISIONS:
         raise ValueError(f"engine.precision must be one of {engine.PRECISIONS}; got '{prec}'")
@@ -129,6 +132,7 @@ def run_forward(spectral_data: SpectralData, profile: AtmosphericProfile,
     res = engine.optical_depth(
         spectral_data, engine.layer_input_from_profile(profile), grid, float(ca["line_cutoff_cm1"]),
         precision=cfg.get("engine", {}).get("precision", DEFAULT_PRECISION), mu=[mu],
+        deterministic=cfg.get("engine", {}).get("deterministic", False),
         want_od=bool(out["optical_depth_layers"]), want_tau=bool(out["optical_depth"]),
         want_trans=bool(out["transmittance"]), warn_level=3)
     result = ForwardResult(wavenumber_cm1=nu.result(), config=cfg)

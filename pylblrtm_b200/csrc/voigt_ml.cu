@@ -17,7 +17,8 @@
 //           |z|^2 clamped to >= MID_Z2 = 64, so every point inside a line's near
 //           zone receives the same constant. A CTA-wide near pass then gives each
 //           near point (accurate value - that constant): float continued fraction
-//           for 36 <= |z|^2 < 64, Weideman's float64 approximation below.
+//           for 36 <= |z|^2 < 64, Weideman's float64 approximation below. Its values
+//           are added per point in a fixed order, so results are bit-reproducible.
 //
 // Inside a reference tile the set of lines is fixed, so every level-1/2 sum is
 // smooth over its interval; the window test keeps the reference's truncation.
@@ -36,6 +37,7 @@ constexpr int ML_CHUNK = ML_THREADS * ML_P;    // max points per CTA
 constexpr int ML_K = 16;                       // Chebyshev nodes per level
 constexpr float ML_MIN_H1 = 32.f;              // smallest chunk half-width (points) using level 1
 constexpr float ML_MIN_H2 = 16.f;              // smallest sub-chunk half-width using level 2
+constexpr int ML_NB = 2048;                    // near items buffered per batch
 
 struct MlLine {
   float4 g;   // jf (centre index relative to the chunk start), a, b, amp_far
@@ -80,6 +82,7 @@ __device__ __forceinline__ float clenshaw16(const float* c, float t) {
   return fmaf(t, b1, 0.5f * c[0] - b2);
 }
 
+template <bool DET>
 __global__ void __launch_bounds__(ML_THREADS, 4)
 tau_ml_kernel(const LineF32* __restrict__ prep, int n_lines, const int2* __restrict__ ranges,
               const double* __restrict__ t_layer, double nu_min, double step, long long n_nu,
@@ -90,11 +93,13 @@ tau_ml_kernel(const LineF32* __restrict__ prep, int n_lines, const int2* __restr
   __shared__ MlLine s2[ML_THREADS];                 // inner lines of the round
   __shared__ unsigned char s_l2[ML_THREADS / 32][ML_THREADS];   // per-warp level-2 slots
   __shared__ unsigned char s_l3[ML_THREADS / 32][ML_THREADS];   // per-warp level-3 slots
+  __shared__ unsigned char s_nl[ML_THREADS / 32][ML_THREADS];   // per-warp slots with near points in it
   __shared__ int s_cnt[3][ML_THREADS / 32];
   __shared__ int s_seg_start[ML_THREADS + 1];       // near-item prefix per inner slot
   __shared__ short s_seg_lo[ML_THREADS];            // first near point per inner slot
   __shared__ unsigned char s_seg_mask[ML_THREADS];  // warps treating the inner line directly (level 3)
-  __shared__ float s_core[ML_CHUNK];
+  __shared__ float s_core[ML_CHUNK];               // near-zone corrections (each point owned by one thread)
+  __shared__ float s_nbuf[ML_NB];                   // near-item values of one batch
   __shared__ double s_red[ML_THREADS];
   __shared__ float s_c1[ML_K];
   __shared__ float s_c2[ML_THREADS / 32][ML_K];
@@ -228,14 +233,18 @@ tau_ml_kernel(const LineF32* __restrict__ prep, int n_lines, const int2* __restr
     }
 
     // ---- per-warp split of the inner lines into level 2 and level 3
-    int n2w = 0, n3w = 0;
+    int n2w = 0, n3w = 0, nnw = 0;
     for (int k = 0; k < n2; k += 32) {
       const int l = k + lane;
-      bool is2 = false, is3 = false;
+      bool is2 = false, is3 = false, nz = false;
       if (l < n2) {
         const float d = fabsf(s2[l].g.x - C2w) - H2;
         is2 = use_l2 && d > H2 + 1.f;
         is3 = !is2 && n_w > 0;
+        if constexpr (DET) {   // near points of slot l inside this warp's sub-chunk (level 3 here)
+          const int st = s_seg_start[l], len = s_seg_start[l + 1] - st, lo = s_seg_lo[l];
+          nz = len > 0 && ((s_seg_mask[l] >> warp) & 1u) && lo < w0 + n_w && lo + len > w0;
+        }
       }
       const unsigned q2 = __ballot_sync(0xffffffffu, is2), q3 = __ballot_sync(0xffffffffu, is3);
       const unsigned lt = (1u << lane) - 1u;
@@ -243,6 +252,11 @@ tau_ml_kernel(const LineF32* __restrict__ prep, int n_lines, const int2* __restr
       if (is3) s_l3[warp][n3w + __popc(q3 & lt)] = (unsigned char)l;
       n2w += __popc(q2);
       n3w += __popc(q3);
+      if constexpr (DET) {
+        const unsigned qn = __ballot_sync(0xffffffffu, nz);
+        if (nz) s_nl[warp][nnw + __popc(qn & lt)] = (unsigned char)l;
+        nnw += __popc(qn);
+      }
     }
     __syncwarp();
 
@@ -271,8 +285,10 @@ tau_ml_kernel(const LineF32* __restrict__ prep, int n_lines, const int2* __restr
     // s_seg_lo[l] + (i - s_seg_start[l]) of inner line l. It gets (accurate value -
     // clamped loop value) if the line is level 3 for the warp owning the point and
     // |z|^2 < MID_Z2 there; x is formed exactly as in the loop, so the clamped value
-    // cancels. Consecutive threads take consecutive points of a line.
-    {
+    // cancels. Consecutive threads take consecutive points of a line. Where near
+    // zones of several lines overlap, the shared-memory atomics add in scheduling
+    // order (results reproducible to rounding, ~1e-9 relative).
+    if constexpr (!DET) {
       for (int i = tid; i < n_near; i += blockDim.x) {
         int l = 0, hi = n2;                               // largest l with s_seg_start[l] <= i
         while (hi - l > 1) {
@@ -291,12 +307,55 @@ tau_ml_kernel(const LineF32* __restrict__ prep, int n_lines, const int2* __restr
         else v = (float)((double)R.h.z * weideman_re((double)x, (double)R.h.x));
         atomicAdd(&s_core[p], v - R.h.w);
       }
-      if (tid == 0) n_near_items += (unsigned long long)n_near;
+    } else {
+      // Bit-reproducible variant, in two phases so that the sums do not depend on thread
+      // scheduling. Phase 1 spreads the near items over the CTA: item i is point
+      // s_seg_lo[l] + (i - s_seg_start[l]) of inner line l; its value is (accurate value -
+      // clamped loop value) if the line is level 3 for the warp owning the point and
+      // |z|^2 < MID_Z2 there (x is formed exactly as in the loop, so the clamped value
+      // cancels), else 0. Phase 2: every thread adds the values of its own points in slot
+      // order. Items go through a buffer of ML_NB at a time.
+      for (int nb0 = 0; nb0 < n_near; nb0 += ML_NB) {
+        const int nb1 = min(n_near, nb0 + ML_NB);
+        for (int i = nb0 + tid; i < nb1; i += blockDim.x) {
+          int l = 0, hi = n2;                               // largest l with s_seg_start[l] <= i
+          while (hi - l > 1) {
+            const int mid = (l + hi) >> 1;
+            if (s_seg_start[mid] <= i) l = mid; else hi = mid;
+          }
+          const int p = s_seg_lo[l] + (i - s_seg_start[l]);
+          float v = 0.f;
+          if ((s_seg_mask[l] >> (p >> 8)) & 1u) {            // level 3 for the owning warp
+            const MlLine R = s2[l];
+            const float x0 = fmaf((float)(p & ~(P - 1)) - R.g.x, R.g.y, -R.g.z);
+            const float x = fmaf((float)(p & (P - 1)), R.g.y, x0);
+            const float z2 = fmaf(x, x, R.h.y);
+            if (z2 < MID_Z2) {
+              if (z2 >= CORE_Z2 && R.h.x >= 0.f) v = R.h.z * re_w_cf32(x, R.h.x, z2);
+              else v = (float)((double)R.h.z * weideman_re((double)x, (double)R.h.x));
+              v -= R.h.w;
+            }
+          }
+          s_nbuf[i - nb0] = v;
+        }
+        __syncthreads();
+        const int q0 = w0 + lane * P;                       // this thread's points [q0, q0 + P)
+        for (int j = 0; j < nnw; ++j) {                     // slots with near points in this warp, in order
+          const int l = s_nl[warp][j];
+          const int st = s_seg_start[l], en = s_seg_start[l + 1];
+          if (en <= nb0 || st >= nb1) continue;
+          const int lo = s_seg_lo[l];
+          const int pa = max(q0, lo + (max(st, nb0) - st)), pb = min(q0 + P, lo + (min(en, nb1) - st));
+          for (int p = pa; p < pb; ++p) s_core[p] += s_nbuf[st + (p - lo) - nb0];
+        }
+        if (nb1 < n_near) __syncthreads();                  // the buffer is refilled
+      }
     }
+    if (tid == 0) n_near_items += (unsigned long long)n_near;
     // No barrier here: the next round writes the staging arrays only after its first
     // barrier, which every warp reaches after finishing this round.
   }
-  __syncthreads();   // near-pass atomics of the last round complete
+  __syncthreads();
 
   // ---- level-1 node values: reduce the 16-thread groups, then Chebyshev coefficients
   s_red[tid] = (double)sum1 - (double)comp1;
@@ -362,7 +421,7 @@ using namespace lbl;
 extern "C" int lbl_tau_tiles_ml_f32(const LineF32* prep, int n_lines, const int* ranges, const double* t_layer,
                                     int n_rows, double nu_min, double step, long long n_nu, int tile_samples,
                                     double cutoff, int n_grp, float* od, int* err, unsigned long long* evals,
-                                    unsigned long long* work, void* stream) {
+                                    unsigned long long* work, int flags, void* stream) {
   if (!prep || !ranges || !t_layer || !od || n_lines < 1 || n_rows < 1 || n_rows > 65535 || n_nu < 1 ||
       n_nu > 1500000000LL || tile_samples < 1 || !(step > 0) || !(cutoff >= 0) || n_grp < 1)
     return lbl_set_error(LBL_EINVAL, "lbl_tau_tiles_ml_f32: bad arguments");
@@ -373,8 +432,13 @@ extern "C" int lbl_tau_tiles_ml_f32(const LineF32* prep, int n_lines, const int*
   const long long chunks = (tile_samples + cp - 1) / cp;
   if (n_tiles * chunks > 0x7fffffffLL) return lbl_set_error(LBL_EINVAL, "lbl_tau_tiles_ml_f32: grid too large");
   dim3 grid((unsigned)(n_tiles * chunks), (unsigned)n_rows);
-  tau_ml_kernel<<<grid, threads, 0, (cudaStream_t)stream>>>(prep, n_lines, (const int2*)ranges, t_layer, nu_min,
-                                                             step, n_nu, tile_samples, (int)chunks, cutoff, n_grp,
-                                                             od, err, evals, work);
+  if (flags & LBL_DETERMINISTIC)
+    tau_ml_kernel<true><<<grid, threads, 0, (cudaStream_t)stream>>>(prep, n_lines, (const int2*)ranges, t_layer,
+                                                                   nu_min, step, n_nu, tile_samples, (int)chunks,
+                                                                   cutoff, n_grp, od, err, evals, work);
+  else
+    tau_ml_kernel<false><<<grid, threads, 0, (cudaStream_t)stream>>>(prep, n_lines, (const int2*)ranges, t_layer,
+                                                                    nu_min, step, n_nu, tile_samples, (int)chunks,
+                                                                    cutoff, n_grp, od, err, evals, work);
   return lbl_check_launch("lbl_tau_tiles_ml_f32");
 }

@@ -34,6 +34,7 @@ constexpr int MJ_CHUNK = MJ_THREADS * MJ_P;       // 1024 points
 constexpr int MJ_K = 16;
 constexpr float MJ_MIN_H1 = 32.f;
 constexpr float MJ_MIN_H2 = 16.f;
+constexpr int MJ_NB = 1024;                        // near items buffered per batch (dynamic shared memory)
 
 struct JLine {
   float4 g;   // jf (or C1 - jf for level 1), a, b, amp
@@ -140,6 +141,7 @@ __device__ __forceinline__ float clenshaw_k(const float* c, float t) {
   return fmaf(t, b1, 0.5f * c[0] - b2);
 }
 
+template <bool DET>
 __global__ void __launch_bounds__(MJ_THREADS, 2)
 jac_ml_kernel(const LineF32* __restrict__ prep, const LineJac* __restrict__ jprep, int n_lines,
               const int2* __restrict__ ranges, const double* __restrict__ t_layer, double nu_min, double step,
@@ -151,11 +153,14 @@ jac_ml_kernel(const LineF32* __restrict__ prep, const LineJac* __restrict__ jpre
   __shared__ JLine s2[MJ_THREADS];
   __shared__ unsigned char s_l2[MJ_THREADS / 32][MJ_THREADS];
   __shared__ unsigned char s_l3[MJ_THREADS / 32][MJ_THREADS];
+  __shared__ unsigned char s_nl[MJ_THREADS / 32][MJ_THREADS];   // per-warp slots with near points in it
   __shared__ int s_cnt[3][MJ_THREADS / 32];
   __shared__ int s_seg_start[MJ_THREADS + 1];
   __shared__ short s_seg_lo[MJ_THREADS];
   __shared__ unsigned char s_seg_mask[MJ_THREADS];
-  __shared__ float s_core[3][MJ_CHUNK];
+  __shared__ float s_core[3][MJ_CHUNK];              // near corrections (each point owned by one thread)
+  extern __shared__ float s_nbuf_dyn[];              // near-item values of one batch: [3][MJ_NB]
+  float (*s_nbuf)[MJ_NB] = reinterpret_cast<float (*)[MJ_NB]>(s_nbuf_dyn);
   __shared__ float s_c1[3][MJ_K];
   __shared__ float s_c2[MJ_THREADS / 32][3][MJ_K];
   // the level-1 line records are dead after the last round; their space holds the reductions
@@ -284,14 +289,18 @@ jac_ml_kernel(const LineF32* __restrict__ prep, const LineJac* __restrict__ jpre
       kahan3(sum1, comp1, a);
     }
     // per-warp split of the inner lines into level 2 and level 3
-    int n2w = 0, n3w = 0;
+    int n2w = 0, n3w = 0, nnw = 0;
     for (int k = 0; k < n2; k += 32) {
       const int l = k + lane;
-      bool is2 = false, is3 = false;
+      bool is2 = false, is3 = false, nz = false;
       if (l < n2) {
         const float d = fabsf(s2[l].g.x - C2w) - H2;
         is2 = use_l2 && d > H2 + 1.f;
         is3 = !is2 && n_w > 0;
+        if constexpr (DET) {   // near points of slot l inside this warp's sub-chunk (level 3 here)
+          const int st = s_seg_start[l], len = s_seg_start[l + 1] - st, lo = s_seg_lo[l];
+          nz = len > 0 && ((s_seg_mask[l] >> warp) & 1u) && lo < w0 + n_w && lo + len > w0;
+        }
       }
       const unsigned q2 = __ballot_sync(0xffffffffu, is2), q3 = __ballot_sync(0xffffffffu, is3);
       const unsigned lt = (1u << lane) - 1u;
@@ -299,6 +308,11 @@ jac_ml_kernel(const LineF32* __restrict__ prep, const LineJac* __restrict__ jpre
       if (is3) s_l3[warp][n3w + __popc(q3 & lt)] = (unsigned char)l;
       n2w += __popc(q2);
       n3w += __popc(q3);
+      if constexpr (DET) {
+        const unsigned qn = __ballot_sync(0xffffffffu, nz);
+        if (nz) s_nl[warp][nnw + __popc(qn & lt)] = (unsigned char)l;
+        nnw += __popc(qn);
+      }
     }
     __syncwarp();
     // level 2: half-warps take one line each, lane (& 15) = node
@@ -326,12 +340,17 @@ jac_ml_kernel(const LineF32* __restrict__ prep, const LineJac* __restrict__ jpre
         acc[2][m] = a3[2];
       }
     }
-    // level 3, near correction (accurate - clamped) spread over the CTA; x is
-    // formed exactly as in the loop above, so the clamped values cancel
-    {
-      int l = 0;
+    // level 3, near correction (accurate - clamped) spread over the CTA; x is formed
+    // exactly as in the loop above, so the clamped values cancel. Where near zones
+    // overlap, the shared-memory atomics add in scheduling order (reproducible to
+    // rounding, ~1e-9 relative).
+    if constexpr (!DET) {
       for (int i = tid; i < n_near; i += blockDim.x) {
-        while (s_seg_start[l + 1] <= i) ++l;
+        int l = 0, hi = n2;                               // largest l with s_seg_start[l] <= i
+        while (hi - l > 1) {
+          const int mid = (l + hi) >> 1;
+          if (s_seg_start[mid] <= i) l = mid; else hi = mid;
+        }
         const int p = s_seg_lo[l] + (i - s_seg_start[l]);
         if (!((s_seg_mask[l] >> (p / MJ_WARP_PTS)) & 1u)) continue;
         const JLine R = s2[l];
@@ -348,11 +367,64 @@ jac_ml_kernel(const LineF32* __restrict__ prep, const LineJac* __restrict__ jpre
         atomicAdd(&s_core[1][p], a[1] - b[1]);
         atomicAdd(&s_core[2][p], a[2] - b[2]);
       }
+    } else {
+      // bit-reproducible variant: near correction (accurate - clamped) in two phases so that the sums do
+      // not depend on thread scheduling: the items are spread over the CTA into a buffer
+      // (x formed exactly as in the loop above, so the clamped values cancel; 0 where the
+      // line is not level 3 for the owning warp or |z|^2 >= MID_Z2), then every thread
+      // adds the values of its own points in slot order. MJ_NB items per batch.
+      for (int nb0 = 0; nb0 < n_near; nb0 += MJ_NB) {
+        const int nb1 = min(n_near, nb0 + MJ_NB);
+        for (int i = nb0 + tid; i < nb1; i += blockDim.x) {
+          int l = 0, hi = n2;                               // largest l with s_seg_start[l] <= i
+          while (hi - l > 1) {
+            const int mid = (l + hi) >> 1;
+            if (s_seg_start[mid] <= i) l = mid; else hi = mid;
+          }
+          const int p = s_seg_lo[l] + (i - s_seg_start[l]);
+          float d[3] = {0.f, 0.f, 0.f};
+          if ((s_seg_mask[l] >> (p / MJ_WARP_PTS)) & 1u) {
+            const JLine R = s2[l];
+            const float x0 = fmaf((float)(p & ~(P - 1)) - R.g.x, R.g.y, -R.g.z);
+            const float x = fmaf((float)(p & (P - 1)), R.g.y, x0);
+            const float z2 = fmaf(x, x, R.h.y);
+            if (z2 < MID_Z2) {
+              const U3 good = near3(x, R.h.x, z2);
+              const U3 clamped = series5(x, R.h.x, rcp_approx(fmaxf(z2, MID_Z2)));
+              float a[3] = {0.f, 0.f, 0.f}, b[3] = {0.f, 0.f, 0.f};
+              add3(a, good, x, R);
+              add3(b, clamped, x, R);
+              d[0] = a[0] - b[0];
+              d[1] = a[1] - b[1];
+              d[2] = a[2] - b[2];
+            }
+          }
+          s_nbuf[0][i - nb0] = d[0];
+          s_nbuf[1][i - nb0] = d[1];
+          s_nbuf[2][i - nb0] = d[2];
+        }
+        __syncthreads();
+        const int q0 = w0 + lane * P;                       // this thread's points [q0, q0 + P)
+        for (int j = 0; j < nnw; ++j) {                     // slots with near points in this warp, in order
+          const int l = s_nl[warp][j];
+          const int st = s_seg_start[l], en = s_seg_start[l + 1];
+          if (en <= nb0 || st >= nb1) continue;
+          const int lo = s_seg_lo[l];
+          const int pa = max(q0, lo + (max(st, nb0) - st)), pb = min(q0 + P, lo + (min(en, nb1) - st));
+          for (int p = pa; p < pb; ++p) {
+            const int k = st + (p - lo) - nb0;
+            s_core[0][p] += s_nbuf[0][k];
+            s_core[1][p] += s_nbuf[1][k];
+            s_core[2][p] += s_nbuf[2][k];
+          }
+        }
+        if (nb1 < n_near) __syncthreads();                  // the buffer is refilled
+      }
     }
     // No barrier here: the next round writes the staging arrays only after its first
     // barrier, which every warp reaches after finishing this round.
   }
-  __syncthreads();   // every warp is done with s1 (aliased by s_red) and the near-pass atomics
+  __syncthreads();   // every warp is done with s1 (aliased by s_red)
 
   // level-1 node values (reduce the 16-thread groups) and Chebyshev coefficients
 #pragma unroll
@@ -447,7 +519,8 @@ using namespace lbl;
 extern "C" int lbl_jacobian_ml_f32(const LineF32* prep, const LineJac* jprep, int n_lines, const int* ranges,
                                    const double* t_layer, int n_rows, int n_lay, double nu_min, double step,
                                    long long n_nu, int tile_samples, double cutoff, float* od, float* d_t,
-                                   float* d_v, const double* g_tau, double* vjp_t, double* vjp_v, void* stream) {
+                                   float* d_v, const double* g_tau, double* vjp_t, double* vjp_v, int flags,
+                                   void* stream) {
   const bool vjp = g_tau != nullptr;
   if (!prep || !jprep || !ranges || !t_layer || n_lines < 1 || n_rows < 1 || n_lay < 1 || n_rows % n_lay ||
       n_rows > 65535 || n_nu < 1 || tile_samples < 1 || !(step > 0) || !(cutoff >= 0) ||
@@ -460,8 +533,25 @@ extern "C" int lbl_jacobian_ml_f32(const LineF32* prep, const LineJac* jprep, in
   const long long chunks = (tile_samples + cp - 1) / cp;
   if (n_tiles * chunks > 0x7fffffffLL) return lbl_set_error(LBL_EINVAL, "lbl_jacobian_ml_f32: grid too large");
   dim3 grid((unsigned)(n_tiles * chunks), (unsigned)n_rows);
-  jac_ml_kernel<<<grid, threads, 0, (cudaStream_t)stream>>>(prep, jprep, n_lines, (const int2*)ranges, t_layer,
-                                                             nu_min, step, n_nu, tile_samples, (int)chunks, cutoff,
-                                                             od, d_t, d_v, n_lay, g_tau, vjp_t, vjp_v);
+  if (flags & LBL_DETERMINISTIC) {
+    constexpr int dyn_bytes = 3 * MJ_NB * (int)sizeof(float);   // near-item buffer
+    int dev = 0;
+    cudaGetDevice(&dev);
+    static int attr_set[64] = {0};
+    if (dev < 0 || dev >= 64) return lbl_set_error(LBL_EINVAL, "lbl_jacobian_ml_f32: device index out of range");
+    if (!attr_set[dev]) {
+      if (cudaFuncSetAttribute(jac_ml_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn_bytes) !=
+          cudaSuccess)
+        return lbl_check_launch("lbl_jacobian_ml_f32 (shared memory attribute)");
+      attr_set[dev] = 1;
+    }
+    jac_ml_kernel<true><<<grid, threads, dyn_bytes, (cudaStream_t)stream>>>(
+        prep, jprep, n_lines, (const int2*)ranges, t_layer, nu_min, step, n_nu, tile_samples, (int)chunks, cutoff,
+        od, d_t, d_v, n_lay, g_tau, vjp_t, vjp_v);
+  } else {
+    jac_ml_kernel<false><<<grid, threads, 0, (cudaStream_t)stream>>>(
+        prep, jprep, n_lines, (const int2*)ranges, t_layer, nu_min, step, n_nu, tile_samples, (int)chunks, cutoff,
+        od, d_t, d_v, n_lay, g_tau, vjp_t, vjp_v);
+  }
   return lbl_check_launch("lbl_jacobian_ml_f32");
 }

@@ -403,20 +403,22 @@ class Job:
                     f"Layer {k}, gas '{self.groups[g].gas}': non-finite or negative line strength")
             raise FloatingPointError(f"Layer {k}: non-finite optical depth after radiation term")
 
-    def jacobian(self, gas: str = "H2O", g_tau=None):
+    def jacobian(self, gas: str = "H2O", g_tau=None, deterministic: bool = False):
         """Per-layer Jacobians of the float32 multi-level engine.
 
         Returns device tensors (od, d tau/dT_layer, d tau/dlnVMR_layer of ``gas``),
         each [n_prof, n_lay, n_nu] float32; with ``g_tau`` ([n_prof, n_nu]) returns
         instead the vector-Jacobian products (sum_nu g dtau/dT, sum_nu g dtau/dlnVMR),
         each [n_prof, n_lay] float64, without storing the Jacobian.
+        ``deterministic`` selects the bit-reproducible near-zone sums.
         """
         self.launches = 0
-        return _jacobian_impl(self, gas, g_tau)
+        return _jacobian_impl(self, gas, g_tau, deterministic)
 
     def run(self, precision: str = "fp32", mu: Optional[Sequence[float]] = None, want_od: bool = True,
             want_tau: bool = False, want_trans: bool = False, count_evals: bool = False,
-            timer: Optional[dict] = None, channels: Optional[Tuple[int, int]] = None) -> EngineResult:
+            timer: Optional[dict] = None, channels: Optional[Tuple[int, int]] = None,
+            deterministic: bool = False) -> EngineResult:
         """All device stages; ``timer`` (dict) receives CUDA-event times of the summation kernel.
 
         ``channels = (width_points, n_channels)`` adds channel-mean transmittances
@@ -424,6 +426,8 @@ class Job:
         """
         if precision not in PRECISIONS:
             raise ValueError(f"precision must be one of {PRECISIONS}, got {precision!r}")
+        if deterministic and precision == "fp32-direct":
+            raise ValueError("deterministic=True needs precision 'fp32' (multi-level) or 'fp64'")
         torch, dev = self.torch, self.dev
         stream = torch.cuda.current_stream().cuda_stream
         grid = self.grid
@@ -497,7 +501,8 @@ class Job:
                   n_nu, grid.tile_samples, self.cutoff, n_grp, od.data_ptr(), err.data_ptr(), _lib.ptr(evals))
         if precision == "fp32":
             _lib.call("lbl_tau_tiles_ml_f32", *common,
-                      0 if evals is None else evals.data_ptr() + 8, stream)
+                      0 if evals is None else evals.data_ptr() + 8,
+                      _lib.LBL_DETERMINISTIC if deterministic else 0, stream)
         else:
             _lib.call("lbl_tau_tiles_f32" if single else "lbl_tau_tiles_f64", *common, stream)
         if timer is not None:
@@ -516,7 +521,7 @@ class Job:
         return finish(od)
 
 
-def _jacobian_impl(job: Job, gas: str, g_tau=None):
+def _jacobian_impl(job: Job, gas: str, g_tau=None, deterministic: bool = False):
     """Device stages of Job.jacobian."""
     torch, dev = job.torch, job.dev
     stream = torch.cuda.current_stream().cuda_stream
@@ -553,30 +558,32 @@ def _jacobian_impl(job: Job, gas: str, g_tau=None):
               tips_len.data_ptr(), tips_t.data_ptr(), tips_q.data_ptr(), mask, dlnq.data_ptr(), jprep.data_ptr(),
               stream)
     job.launches += 4
+    flags = _lib.LBL_DETERMINISTIC if deterministic else 0
     common = (prep.data_ptr(), jprep.data_ptr(), n_kept, ranges.data_ptr(), t_lay.data_ptr(), n_rows, n_lay,
               grid.nu_min, grid.step, n_nu, grid.tile_samples, job.cutoff)
     if g_tau is not None:
         g = torch.as_tensor(g_tau).to(device=dev, dtype=torch.float64).reshape(n_prof, n_nu).contiguous()
         vt = torch.zeros((n_prof, n_lay), dtype=torch.float64, device=dev)
         vv = torch.zeros_like(vt)
-        _lib.call("lbl_jacobian_ml_f32", *common, 0, 0, 0, g.data_ptr(), vt.data_ptr(), vv.data_ptr(), stream)
+        _lib.call("lbl_jacobian_ml_f32", *common, 0, 0, 0, g.data_ptr(), vt.data_ptr(), vv.data_ptr(), flags,
+                  stream)
         return vt, vv
     od = torch.empty((n_prof, n_lay, n_nu), dtype=torch.float32, device=dev)
     d_t = torch.empty_like(od)
     d_v = torch.empty_like(od)
-    _lib.call("lbl_jacobian_ml_f32", *common, od.data_ptr(), d_t.data_ptr(), d_v.data_ptr(), 0, 0, 0, stream)
+    _lib.call("lbl_jacobian_ml_f32", *common, od.data_ptr(), d_t.data_ptr(), d_v.data_ptr(), 0, 0, 0, flags, stream)
     return od, d_t, d_v
 
 
 def optical_depth(sd: SpectralData, layers: LayerInput, grid: Grid, cutoff: float,
                   precision: str = "fp32", mu: Optional[Sequence[float]] = None,
                   want_od: bool = True, want_tau: bool = False, want_trans: bool = False,
-                  warn_level: int = 4, count_evals: bool = False) -> EngineResult:
+                  warn_level: int = 4, count_evals: bool = False, deterministic: bool = False) -> EngineResult:
     """Upload one forward call and run every device stage (see the module docstring)."""
     if precision not in PRECISIONS:
         raise ValueError(f"precision must be one of {PRECISIONS}, got {precision!r}")
     job = Job(sd, layers, grid, cutoff, warn_level + 1)
-    return job.run(precision, mu, want_od, want_tau, want_trans, count_evals)
+    return job.run(precision, mu, want_od, want_tau, want_trans, count_evals, deterministic=deterministic)
 
 
 def layer_input_from_profile(profile) -> LayerInput:

@@ -34,11 +34,14 @@ def compute_transmittance(
     tile_width_cm1: float = 2.0,
     mu_view: float = 1.0,
     precision: str = DEFAULT_PRECISION,
+    deterministic: bool = False,
 ) -> Tuple[np.ndarray, np.ndarray]:
     """Monochromatic transmittance exp(-sum_k od_k / mu_view) on a uniform grid.
 
     Same contract as ``pylblrtm/forward.py:67-152``; returns ``(nu, T)`` as
-    float64 NumPy arrays. ``precision`` selects the engine arithmetic.
+    float64 NumPy arrays. ``precision`` selects the engine arithmetic;
+    ``deterministic`` makes the float32 engine bit-reproducible (fixed summation
+    order of the near-zone corrections; otherwise reproducible to ~1e-9 relative).
     """
     if not isinstance(spectral_data, SpectralData):
         raise TypeError("spectral_data must be a SpectralData instance")
@@ -54,7 +57,7 @@ def compute_transmittance(
     nu = engine.grid_async(grid)
     res = engine.optical_depth(spectral_data, engine.layer_input_from_profile(profile), grid,
                                float(line_cutoff_cm1), precision=precision, mu=[float(mu_view)],
-                               want_od=False, want_trans=True, warn_level=3)
+                               want_od=False, want_trans=True, warn_level=3, deterministic=deterministic)
     trans = engine.to_host(res.trans[0])
     return nu.result(), trans
 
@@ -66,6 +69,7 @@ def _build_optical_depth(
     line_cutoff_cm1: float,
     tile_width_cm1: float,
     precision: str = DEFAULT_PRECISION,
+    deterministic: bool = False,
 ) -> np.ndarray:
     """Vertical optical depth stack [n_layers, n_nu] (``pylblrtm/forward.py:157-317``).
 
@@ -73,5 +77,5 @@ def _build_optical_depth(
     """
     grid = engine.grid_from_array(nu, tile_width_cm1)
     res = engine.optical_depth(sd, engine.layer_input_from_layers(layers), grid, float(line_cutoff_cm1),
-                               precision=precision, want_od=True, warn_level=4)
+                               precision=precision, want_od=True, warn_level=4, deterministic=deterministic)
     return engine.to_host(res.od[0].to(dtype=__import__("torch").float64))

@@ -130,15 +130,16 @@ def sample_profiles(n: int, seed: int, t_offset: float = 0.0, t_sigma: float = 5
 
 
 def engine_channels(sd: SpectralData, profiles: ProfileBatch, problem: SurrogateProblem,
-                    profiles_per_launch: int = 128, as_numpy: bool = True):
-    """Channel-mean transmittance [n, n_channels] of each profile from the float32 engine."""
+                    profiles_per_launch: int = 128, as_numpy: bool = True, deterministic: bool = False):
+    """Channel-mean transmittance [n, n_channels] of each profile from the float32 engine
+    (``deterministic``: bit-reproducible sums, see ``compute_transmittance``)."""
     torch = engine._torch()
     grid = problem.grid
     outs = []
     for b0 in range(0, len(profiles), profiles_per_launch):
         part = profiles.subset(slice(b0, b0 + profiles_per_launch))
         job = engine.Job(sd, part.layer_input(), grid, problem.cutoff, warn_level=3)
-        res = job.run("fp32", mu=part.mu, want_od=False, channels=problem.channels)
+        res = job.run("fp32", mu=part.mu, want_od=False, channels=problem.channels, deterministic=deterministic)
         outs.append(res.channels.float())
     out = torch.cat(outs) if len(outs) > 1 else outs[0]
     return out.cpu().numpy() if as_numpy else out
@@ -445,11 +446,13 @@ class MLP:
 class GatedSurrogate:
     """4-member ensemble with a spread gate and float32-engine fallback."""
 
-    def __init__(self, members: Sequence[MLP], gate: float = 1e-3, scale: float = 1.0):
+    def __init__(self, members: Sequence[MLP], gate: float = 1e-3, scale: float = 1.0,
+                 deterministic: bool = False):
         if not members:
             raise ValueError("at least one member")
         self.members = list(members)
         self.gate, self.scale = float(gate), float(scale)
+        self.deterministic = bool(deterministic)      # of the engine fallback
         self.torch = members[0].torch
         self.launches = 0
 
@@ -497,7 +500,8 @@ class GatedSurrogate:
         t1 = time.perf_counter()
         idx = np.flatnonzero(flag_h)
         if idx.size:
-            fb = engine_channels(sd, profiles.subset(idx), problem, as_numpy=False)
+            fb = engine_channels(sd, profiles.subset(idx), problem, as_numpy=False,
+                                 deterministic=self.deterministic)
             mean[torch.as_tensor(idx, device=net0.dev)] = fb
         torch.cuda.synchronize()
         t2 = time.perf_counter()

@@ -124,19 +124,26 @@ def test_batched_jacobians_match_single_profiles_and_stream(cuda):
     vmr = {g: lv[g] for g in ("H2O", "CO2", "O3")}
     lo, hi = 1500.0, 1503.0
     mu = np.array([1.0, 0.7, 0.55])
-    res = adjoint.layer_jacobians_batch(sd, lv["p"], lv["t"], vmr, lo, hi, mu_view=mu, profiles_per_launch=2)
+    res = adjoint.layer_jacobians_batch(sd, lv["p"], lv["t"], vmr, lo, hi, mu_view=mu, profiles_per_launch=2,
+                                        deterministic=True)
     for i in range(3):
-        one = adjoint.layer_jacobians(sd, synthetic.profile_from_levels(lv, i), lo, hi, as_numpy=False)
+        one = adjoint.layer_jacobians(sd, synthetic.profile_from_levels(lv, i), lo, hi, as_numpy=False,
+                                      deterministic=True)
         for k in ("od", "dtau_dT", "dtau_dlnvmr"):
             assert torch.equal(res[k][i], one[k]), (i, k)
     chunks = []
     out = adjoint.layer_jacobians_batch(sd, lv["p"], lv["t"], vmr, lo, hi, mu_view=mu, profiles_per_launch=2,
-                                        on_chunk=lambda sl, o: chunks.append((sl, {k: v.clone() for k, v in o.items()})))
+                                        on_chunk=lambda sl, o: chunks.append((sl, {k: v.clone() for k, v in o.items()})),
+                                        deterministic=True)
     assert out is None and [c[0] for c in chunks] == [slice(0, 2), slice(2, 3)]
     for k in ("od", "dtau_dT", "dtau_dlnvmr", "trans"):
         assert torch.equal(torch.cat([c[1][k] for c in chunks]), res[k])
     _, t_fwd = batch.transmittance_batch(sd, lv["p"], lv["t"], vmr, lo, hi, mu_view=mu, as_numpy=False)
     assert torch.max(torch.abs(res["trans"] - t_fwd)).item() <= 1e-5
+    # the default (atomic) near-zone sums agree with the ordered ones to rounding
+    fast = adjoint.layer_jacobians_batch(sd, lv["p"], lv["t"], vmr, lo, hi, mu_view=mu, profiles_per_launch=2)
+    for k in ("od", "dtau_dT", "dtau_dlnvmr"):
+        assert torch.max(torch.abs(fast[k] - res[k])).item() <= 1e-6 * torch.max(torch.abs(res[k])).item(), k
     with pytest.raises(ValueError, match="not in vmr"):
         adjoint.layer_jacobians_batch(sd, lv["p"], lv["t"], vmr, lo, hi, gas="CH4")
     with pytest.raises(ValueError, match="mu_view"):

@@ -9,6 +9,7 @@ import warnings
 
 import numpy as np
 import pytest
+import torch
 
 import pylblrtm_b200 as lbl
 from conftest import ALL_GOLDEN, SMALL_GOLDEN, golden_case, oracle_inputs
@@ -23,12 +24,12 @@ TOL = {"fp64": dict(dT=1e-6, rtau=1e-9, rod=1e-9), "fp32": dict(dT=1e-5, rtau=2e
        "fp32-direct": dict(dT=1e-5, rtau=2e-5, rod=3e-5)}
 
 
-def _run(sd, prof, prm, precision, layers=False):
+def _run(sd, prof, prm, precision, layers=False, deterministic=False):
     cfg = {"spectral": {"nu_min_cm1": prm["nu_min"], "nu_max_cm1": prm["nu_max"], "step_cm1": prm["step"]},
            "calculation": {"mu_view": prm["mu"], "line_cutoff_cm1": prm["cutoff"],
                            "tile_width_cm1": prm["tile"]},
            "output": {"transmittance": True, "optical_depth": True, "optical_depth_layers": layers},
-           "engine": {"precision": precision}}
+           "engine": {"precision": precision, "deterministic": deterministic}}
     with warnings.catch_warnings(record=True) as wl:
         warnings.simplefilter("always")
         res = lbl.run_forward(sd, prof, cfg)
@@ -170,8 +171,8 @@ def test_no_contributing_lines_gives_unit_transmittance(cuda):
 
 def test_fp32_is_deterministic(cuda):
     sd, prof, prm, _ = golden_case("coarse_step")
-    a = _run(sd, prof, prm, "fp32", layers=True)[0]
-    b = _run(sd, prof, prm, "fp32", layers=True)[0]
+    a = _run(sd, prof, prm, "fp32", layers=True, deterministic=True)[0]
+    b = _run(sd, prof, prm, "fp32", layers=True, deterministic=True)[0]
     assert np.array_equal(a.optical_depth_layers, b.optical_depth_layers)
 
 
@@ -230,10 +231,10 @@ def test_batch_equals_single_profiles_bitwise(cuda):
     mu = np.array([1.0, 0.7, 0.45])
     for precision in ("fp32", "fp64"):
         nu, tb = lbl.transmittance_batch(sd, lv["p"], lv["t"], {g: lv[g] for g in ("H2O", "CO2", "O3")},
-                                         1500.0, 1510.0, mu_view=mu, precision=precision)
+                                         1500.0, 1510.0, mu_view=mu, precision=precision, deterministic=True)
         for i in range(3):
             _, t1 = lbl.compute_transmittance(sd, synthetic.profile_from_levels(lv, i), 1500.0, 1510.0,
-                                              mu_view=float(mu[i]), precision=precision)
+                                              mu_view=float(mu[i]), precision=precision, deterministic=True)
             assert np.array_equal(tb[i], t1), (precision, i)
 
 
@@ -248,3 +249,29 @@ def test_channel_mean_matches_host_box_average(cuda):
     ref = tb[:, :20 * 250].reshape(2, 20, 250).mean(axis=2)
     np.testing.assert_allclose(ch, ref, rtol=1e-12, atol=1e-15)
     np.testing.assert_allclose(centres, nu[:5000].reshape(20, 250).mean(axis=1), rtol=0, atol=1e-9)
+
+
+def test_fp32_bitwise_reproducible_with_overlapping_near_zones(cuda):
+    """300 lines per cm^-1 (near zones overlap): repeated launches and a batch of
+    profiles give the same float32 optical depth bit for bit, for both precisions."""
+    sd = synthetic.restrict(synthetic.three_gas_lines(6000, 1492, 1512, seed=3), 1492, 1512)
+    lv = synthetic.perturbed_levels(synthetic.logp_levels(6), 3, seed=77)
+    gases = ["H2O", "CO2", "O3"]
+    grid = engine.make_grid(1500.0, 1503.0, 0.001, 2.0)
+
+    def job(sl):
+        li = engine.LayerInput(gases=gases, levels_p=lv["p"][sl], levels_t=lv["t"][sl],
+                               levels_vmr=np.stack([lv[g][sl] for g in gases], axis=1))
+        return engine.Job(sd, li, grid, 25.0)
+
+    single, both = job(slice(0, 1)), job(slice(0, 3))
+    for precision in ("fp32", "fp64"):
+        a = single.run(precision, deterministic=True).od[0]
+        b = single.run(precision, deterministic=True).od[0]
+        c = both.run(precision, deterministic=True).od[0]
+        assert torch.equal(a, b) and torch.equal(a, c), precision
+    # the default float32 sums (atomic near-zone corrections) agree to rounding
+    d = both.run("fp32").od[0]
+    assert torch.max(torch.abs(d - a)).item() <= 1e-6 * torch.max(torch.abs(a)).item()
+    with pytest.raises(ValueError, match="deterministic"):
+        single.run("fp32-direct", deterministic=True)

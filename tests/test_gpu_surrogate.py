@@ -259,9 +259,9 @@ def test_gated_surrogate_against_engine(cuda):
                                        cfg=surrogate.TrainConfig(batch=512, steps=600, lr=2e-3, warmup=30, seed=7))
     test_in = surrogate.sample_profiles(512, seed=2)
     test_ood = surrogate.sample_profiles(512, seed=3, t_offset=25.0)
-    gate = surrogate.GatedSurrogate(members)
-    ref_in = surrogate.engine_channels(sd, test_in, problem)
-    ref_ood = surrogate.engine_channels(sd, test_ood, problem)
+    gate = surrogate.GatedSurrogate(members, deterministic=True)
+    ref_in = surrogate.engine_channels(sd, test_in, problem, deterministic=True)
+    ref_ood = surrogate.engine_channels(sd, test_ood, problem, deterministic=True)
     mean_in, est_in, _ = gate.ensemble(torch.from_numpy(test_in.features()).cuda())
     gate.gate = float(np.quantile(est_in.cpu().numpy(), 0.9))      # 10 % of in-distribution flagged
     _, est_ood, flag_ood = gate.ensemble(torch.from_numpy(test_ood.features()).cuda())
