@@ -39,11 +39,12 @@ int lbl_par_parse(const char* text, long long len, long long cap, double* values
  * (pair_mol, pair_iso [max_pairs]), the number of lines of each inside the band
  * mask nu0 in [(nu_first - cutoff) - |shift| p_max, (nu_last + cutoff) + |shift| p_max]
  * with lo_edge = nu_first - cutoff and hi_edge = nu_last + cutoff (pair_band), their
- * count (n_pairs) and every line's pair (pair_index [n]). LBL_EINVAL when more than
- * max_pairs pairs occur. */
+ * count (n_pairs), every line's pair (pair_index [n]) and the largest finite |shift|
+ * (*max_abs_shift; -1 when there is none). LBL_EINVAL when more than max_pairs pairs
+ * occur. */
 int lbl_line_pairs(const int* mol, const int* iso, const double* nu0, const double* shift, long long n,
                    double lo_edge, double hi_edge, double p_max, int max_pairs, int* pair_mol, int* pair_iso,
-                   long long* pair_band, int* n_pairs, int* pair_index);
+                   long long* pair_band, int* n_pairs, int* pair_index, double* max_abs_shift);
 
 #ifdef __cplusplus
 }

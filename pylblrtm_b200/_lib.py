@@ -83,7 +83,7 @@ IO_LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "liblblio
 HOST_SIGNATURES = {
     "lbl_par_count_lines": (_L, [ctypes.c_char_p, _L]),
     "lbl_par_parse": (_I, [ctypes.c_char_p, _L, _L, _P, _P, _P]),
-    "lbl_line_pairs": (_I, [_P, _P, _P, _P, _L, _D, _D, _D, _I, _P, _P, _P, _P, _P]),
+    "lbl_line_pairs": (_I, [_P, _P, _P, _P, _L, _D, _D, _D, _I, _P, _P, _P, _P, _P, _P]),
 }
 
 _lock = threading.Lock()

@@ -11,11 +11,13 @@
 
 extern "C" int lbl_line_pairs(const int* mol, const int* iso, const double* nu0, const double* shift, long long n,
                               double lo_edge, double hi_edge, double p_max, int max_pairs, int* pair_mol,
-                              int* pair_iso, long long* pair_band, int* n_pairs, int* pair_index) {
+                              int* pair_iso, long long* pair_band, int* n_pairs, int* pair_index,
+                              double* max_abs_shift) {
   if (n < 0 || max_pairs < 1 || !n_pairs || (n > 0 && (!mol || !iso || !nu0 || !shift || !pair_index)) ||
-      !pair_mol || !pair_iso || !pair_band)
+      !pair_mol || !pair_iso || !pair_band || !max_abs_shift)
     return LBL_EINVAL;
   int np_ = 0, last = -1;
+  double smax = -1.0;                               // largest finite |shift| (-1: none)
   for (long long i = 0; i < n; ++i) {
     const int m = mol[i], s = iso[i];
     int k = last;
@@ -36,10 +38,13 @@ extern "C" int lbl_line_pairs(const int* mol, const int* iso, const double* nu0,
       last = k;
     }
     pair_index[i] = k;
-    const double sb = fabs(shift[i]) * p_max;
+    const double as = fabs(shift[i]);
+    if (isfinite(as) && as > smax) smax = as;
+    const double sb = as * p_max;
     const double v = nu0[i];
     if ((v >= lo_edge - sb) & (v <= hi_edge + sb)) ++pair_band[k];
   }
   *n_pairs = np_;
+  *max_abs_shift = smax;
   return LBL_OK;
 }

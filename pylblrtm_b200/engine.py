@@ -111,18 +111,22 @@ def grid_from_array(nu: np.ndarray, tile_width: float) -> Grid:
 
 
 def select_groups(sd: SpectralData, profile_gases: Sequence[str], nu_first: float, nu_last: float,
-                  cutoff: float, p_max: float, warn_level: int) -> Tuple[List[Group], np.ndarray]:
+                  cutoff: float, p_max: float, warn_level: int,
+                  stats: Optional[dict] = None) -> Tuple[List[Group], np.ndarray]:
     """Host replica of the group selection of forward.py:189-245.
 
     Returns the contributing groups in sorted (mol_id, iso_id) order and the
     group index of every line (-1 for lines of skipped groups). Emits the same
-    RuntimeWarnings and raises the same KeyError as the reference.
+    RuntimeWarnings and raises the same KeyError as the reference. ``stats``
+    (a dict) receives "max_abs_shift", the largest finite |shift| (0 if none).
     """
     lines = sd.lines
     mol = np.asarray(lines["mol_id"])
     iso = np.asarray(lines["iso_id"])
     n = np.asarray(lines["nu0"]).size
     gid = np.full(n, -1, dtype=np.int32)
+    if stats is not None:
+        stats["max_abs_shift"] = 0.0
     if n == 0:
         return [], gid
     # one native pass: distinct (mol, iso) pairs, band-mask counts (forward.py:190-191)
@@ -141,15 +145,19 @@ def select_groups(sd: SpectralData, profile_gases: Sequence[str], nu_first: floa
         pi_ = np.empty(max_pairs, np.int32)
         pb = np.empty(max_pairs, np.int64)
         n_pairs = ctypes.c_int(0)
+        smax = ctypes.c_double(-1.0)
         rc = host.lbl_line_pairs(mol32.ctypes.data, iso32.ctypes.data, nu0.ctypes.data, shift.ctypes.data, n,
                                  nu_first - cutoff, nu_last + cutoff, float(p_max), max_pairs, pm.ctypes.data,
-                                 pi_.ctypes.data, pb.ctypes.data, ctypes.byref(n_pairs), pair_index.ctypes.data)
+                                 pi_.ctypes.data, pb.ctypes.data, ctypes.byref(n_pairs), pair_index.ctypes.data,
+                                 ctypes.byref(smax))
         if rc == 0:
             break
         if max_pairs >= n:
             raise RuntimeError("lbl_line_pairs failed")
         max_pairs = min(n, 16 * max_pairs)
     k = n_pairs.value
+    if stats is not None:
+        stats["max_abs_shift"] = max(smax.value, 0.0)
     order = np.lexsort((pi_[:k], pm[:k]))                               # sorted (mol_id, iso_id)
     pairs = [(int(pm[j]), int(pi_[j])) for j in order]
     band_counts = pb[:k][order]
@@ -259,8 +267,8 @@ def to_host(t) -> np.ndarray:
     return h.numpy()
 
 
-def _upload(torch, a, dtype, device):
-    return torch.from_numpy(np.ascontiguousarray(a, dtype=dtype)).to(device, non_blocking=False)
+def _upload(torch, a, dtype, device, non_blocking: bool = False):
+    return torch.from_numpy(np.ascontiguousarray(a, dtype=dtype)).to(device, non_blocking=non_blocking)
 
 
 def sort_launches(n_lines: int) -> int:
@@ -292,10 +300,16 @@ class Job:
         self.n_prof, self.n_lay = layers.n_prof, layers.n_lay
         self.p_max = layers.p_max_atm() if self.n_lay > 0 else 1.0
         self.nu_first, self.nu_last = grid.nu_at(0), grid.nu_at(grid.n_nu - 1)
-        self.groups, gid = select_groups(sd, layers.gases, self.nu_first, self.nu_last, self.cutoff,
-                                         self.p_max, warn_level + 1)
-        self.n_lines = int(gid.size)
         self.h2d_bytes = 0
+        # the line arrays go to the device while the host selects the groups (copies from
+        # page-locked arrays are asynchronous; the first device stage orders after them)
+        L = sd.lines
+        self.lines_in = tuple(self._up(L[k], np.float64, non_blocking=True)
+                              for k in ("nu0", "Sref", "g_air", "g_self", "Elow", "n_air", "shift"))
+        st = {}
+        self.groups, gid = select_groups(sd, layers.gases, self.nu_first, self.nu_last, self.cutoff,
+                                         self.p_max, warn_level + 1, stats=st)
+        self.n_lines = int(gid.size)
         self.empty = not self.groups or self.n_lay == 0
         if self.empty:
             return
@@ -321,16 +335,11 @@ class Job:
                     up(offs, np.int32), up([g.tips_t.size for g in self.groups], np.int32),
                     up(np.concatenate([g.tips_t for g in self.groups]), np.float64),
                     up(np.concatenate([g.tips_q for g in self.groups]), np.float64))
-        L = sd.lines
-        self.lines_in = tuple(up(L[k], np.float64) for k in ("nu0", "Sref", "g_air", "g_self", "Elow",
-                                                             "n_air", "shift"))
         self.gid = up(gid, np.int32)
-        fin = np.abs(np.asarray(L["shift"], np.float64))
-        fin = fin[np.isfinite(fin)]
-        self.pad = (float(fin.max()) * self.p_max if fin.size else 0.0) * (1 + 1e-9) + 1e-9
+        self.pad = float(st["max_abs_shift"]) * self.p_max * (1 + 1e-9) + 1e-9
 
-    def _up(self, a, dtype):
-        t = _upload(self.torch, a, dtype, self.dev)
+    def _up(self, a, dtype, non_blocking: bool = False):
+        t = _upload(self.torch, a, dtype, self.dev, non_blocking)
         self.h2d_bytes += t.numel() * t.element_size()
         return t
 
