@@ -35,6 +35,8 @@ constexpr int ML_WARP_PTS = 32 * ML_P;         // points per warp sub-chunk
 constexpr int ML_THREADS = 256;                // max threads per CTA = lines staged per round
 constexpr int ML_CHUNK = ML_THREADS * ML_P;    // max points per CTA
 constexpr int ML_K = 16;                       // Chebyshev nodes per level
+constexpr int ML_KF = 8;                       // nodes for level-1 lines far from the chunk
+constexpr float ML_FAR1 = 5.f;                 // "far": more than (1 + ML_FAR1) half-widths from the centre
 constexpr float ML_MIN_H1 = 32.f;              // smallest chunk half-width (points) using level 1
 constexpr float ML_MIN_H2 = 16.f;              // smallest sub-chunk half-width using level 2
 constexpr int ML_NB = 2048;                    // near items buffered per batch
@@ -69,12 +71,13 @@ __device__ __forceinline__ void kahan_add(float& sum, float& comp, float v) {
   sum = t;
 }
 
-// p(t) = c0/2 + sum_{k>=1} c_k T_k(t) by Clenshaw's recurrence.
+// p(t) = c0/2 + sum_{k>=1} c_k T_k(t) by Clenshaw's recurrence (K coefficients).
+template <int K = ML_K>
 __device__ __forceinline__ float clenshaw16(const float* c, float t) {
   float b1 = 0.f, b2 = 0.f;
   const float t2 = 2.f * t;
 #pragma unroll
-  for (int k = ML_K - 1; k >= 1; --k) {
+  for (int k = K - 1; k >= 1; --k) {
     const float b0 = fmaf(t2, b1, c[k] - b2);
     b2 = b1;
     b1 = b0;
@@ -94,14 +97,16 @@ tau_ml_kernel(const LineF32* __restrict__ prep, int n_lines, const int2* __restr
   __shared__ unsigned char s_l2[ML_THREADS / 32][ML_THREADS];   // per-warp level-2 slots
   __shared__ unsigned char s_l3[ML_THREADS / 32][ML_THREADS];   // per-warp level-3 slots
   __shared__ unsigned char s_nl[ML_THREADS / 32][ML_THREADS];   // per-warp slots with near points in it
-  __shared__ int s_cnt[3][ML_THREADS / 32];
+  __shared__ int s_cnt[4][ML_THREADS / 32];
   __shared__ int s_seg_start[ML_THREADS + 1];       // near-item prefix per inner slot
   __shared__ short s_seg_lo[ML_THREADS];            // first near point per inner slot
   __shared__ unsigned char s_seg_mask[ML_THREADS];  // warps treating the inner line directly (level 3)
   __shared__ float s_core[ML_CHUNK];               // near-zone corrections (each point owned by one thread)
   __shared__ float s_nbuf[ML_NB];                   // near-item values of one batch
   __shared__ double s_red[ML_THREADS];
+  __shared__ double s_redf[ML_THREADS];
   __shared__ float s_c1[ML_K];
+  __shared__ float s_c1f[ML_KF];
   __shared__ float s_c2[ML_THREADS / 32][ML_K];
 
   const int row = blockIdx.y;
@@ -128,6 +133,7 @@ tau_ml_kernel(const LineF32* __restrict__ prep, int n_lines, const int2* __restr
   const bool use_l2 = H2 >= ML_MIN_H2;
   // Chebyshev node offsets owned by this thread: level 1 node (tid & 15), level 2 node (lane & 15)
   const float xn1 = H1 * (float)cospi((2.0 * (tid & 15) + 1.0) / (2.0 * ML_K));
+  const float xn1f = H1 * (float)cospi((2.0 * (tid & 7) + 1.0) / (2.0 * ML_KF));
   const float xn2 = H2 * (float)cospi((2.0 * (lane & 15) + 1.0) / (2.0 * ML_K));
   const float pf = (float)(w0 + lane * P);                   // this lane's first point
 
@@ -138,7 +144,7 @@ tau_ml_kernel(const LineF32* __restrict__ prep, int n_lines, const int2* __restr
   float acc[P];
 #pragma unroll
   for (int m = 0; m < P; ++m) acc[m] = 0.f;
-  float sum1 = 0.f, comp1 = 0.f, sum2 = 0.f, comp2 = 0.f;
+  float sum1 = 0.f, comp1 = 0.f, sumf = 0.f, compf = 0.f, sum2 = 0.f, comp2 = 0.f;
   unsigned long long n_pass = 0, n_nodes = 0, n_l3 = 0, n_near_items = 0;
 
   // register prefetch of the next round's line records
@@ -152,7 +158,9 @@ tau_ml_kernel(const LineF32* __restrict__ prep, int n_lines, const int2* __restr
     if (base + blockDim.x + tid < rng.y) nxt = lp[base + blockDim.x + tid];
     const bool pass = have && (L.nuc >= wlo) && (L.nuc <= whi);
     const float jf = (float)(L.j0 - c0i);           // |j0 - c0| < 1.5e9 (grid index span check)
-    const bool lev1 = pass && use_l1 && (fabsf(jf - C1) - H1 > H1 + 1.f);
+    const float d1 = fabsf(jf - C1) - H1;
+    const bool lev1 = pass && use_l1 && (d1 > H1 + 1.f);
+    const bool lev1f = lev1 && (d1 > ML_FAR1 * H1);     // far: 8 nodes suffice
     const bool inner = pass && !lev1;
     // near range (points with possibly |z|^2 < MID_Z2) of an inner line, clipped to the chunk
     const float y2 = L.y * L.y;
@@ -184,17 +192,20 @@ tau_ml_kernel(const LineF32* __restrict__ prep, int n_lines, const int2* __restr
       const int t = __shfl_up_sync(0xffffffffu, near_scan, o);
       if (lane >= o) near_scan += t;
     }
-    const unsigned b1 = __ballot_sync(0xffffffffu, lev1), b2 = __ballot_sync(0xffffffffu, inner);
-    if (lane == 0) { s_cnt[0][warp] = __popc(b1); s_cnt[1][warp] = __popc(b2); }
+    const unsigned b1 = __ballot_sync(0xffffffffu, lev1 && !lev1f), bf = __ballot_sync(0xffffffffu, lev1f);
+    const unsigned b2 = __ballot_sync(0xffffffffu, inner);
+    if (lane == 0) { s_cnt[0][warp] = __popc(b1); s_cnt[1][warp] = __popc(b2); s_cnt[3][warp] = __popc(bf); }
     if (lane == 31) s_cnt[2][warp] = near_scan;
     __syncthreads();
-    int off1 = 0, off2 = 0, off3 = 0, n1 = 0, n2 = 0, n_near = 0;
+    int off1 = 0, offf = 0, off2 = 0, off3 = 0, n1 = 0, nf = 0, n2 = 0, n_near = 0;
     for (int w = 0; w < n_warps; ++w) {
-      const int a1 = s_cnt[0][w], a2 = s_cnt[1][w], a3 = s_cnt[2][w];
+      const int a1 = s_cnt[0][w], a2 = s_cnt[1][w], a3 = s_cnt[2][w], af = s_cnt[3][w];
       off1 += (w < warp) ? a1 : 0;
+      offf += (w < warp) ? af : 0;
       off2 += (w < warp) ? a2 : 0;
       off3 += (w < warp) ? a3 : 0;
       n1 += a1;
+      nf += af;
       n2 += a2;
       n_near += a3;
     }
@@ -205,7 +216,9 @@ tau_ml_kernel(const LineF32* __restrict__ prep, int n_lines, const int2* __restr
       if (!lev1) clamp_val = L.amp_far * mid_clamped_term(0.f, y2);   // r = 1/MID_Z2 when y2 < MID_Z2
       r.h = make_float4(L.y, y2, L.amp, clamp_val);
       const unsigned lt = (1u << lane) - 1u;
-      if (lev1) {
+      if (lev1f) {
+        s1[n1 + offf + __popc(bf & lt)] = r;              // far level-1 lines after the others
+      } else if (lev1) {
         s1[off1 + __popc(b1 & lt)] = r;
       } else {
         const int slot = off2 + __popc(b2 & lt);
@@ -217,7 +230,7 @@ tau_ml_kernel(const LineF32* __restrict__ prep, int n_lines, const int2* __restr
     }
     if (tid == 0) s_seg_start[n2] = n_near;
     __syncthreads();
-    n_pass += (unsigned long long)(n1 + n2);
+    n_pass += (unsigned long long)(n1 + nf + n2);
 
     // ---- level 1: thread (tid & 15) evaluates its node for lines tid>>4, +16, ...
     {
@@ -229,7 +242,15 @@ tau_ml_kernel(const LineF32* __restrict__ prep, int n_lines, const int2* __restr
         a1 += line_value(x, R);
       }
       kahan_add(sum1, comp1, a1);
-      if (tid == 0) n_nodes += (unsigned long long)n1 * ML_K;
+      // far lines: thread (tid & 7) evaluates its node for far lines tid>>3, +32, ...
+      float af = 0.f;
+      for (int l = tid >> 3; l < nf; l += (int)(blockDim.x >> 3)) {
+        const MlLine R = s1[n1 + l];
+        const float x = fmaf(xn1f + R.g.x, R.g.y, -R.g.z);
+        af += line_value(x, R);
+      }
+      kahan_add(sumf, compf, af);
+      if (tid == 0) n_nodes += (unsigned long long)n1 * ML_K + (unsigned long long)nf * ML_KF;
     }
 
     // ---- per-warp split of the inner lines into level 2 and level 3
@@ -359,17 +380,28 @@ tau_ml_kernel(const LineF32* __restrict__ prep, int n_lines, const int2* __restr
 
   // ---- level-1 node values: reduce the 16-thread groups, then Chebyshev coefficients
   s_red[tid] = (double)sum1 - (double)comp1;
+  s_redf[tid] = (double)sumf - (double)compf;
   __syncthreads();
   if (tid < ML_K) {
     double f = 0.0;
     for (int i = tid; i < (int)blockDim.x; i += ML_K) f += s_red[i];
-    s_red[tid] = f;      // only read back after the barrier below, by threads < ML_K
+    s_red[tid] = f;      // only read back after the barrier below
+  } else if (tid < ML_K + ML_KF) {
+    const int j = tid - ML_K;
+    double f = 0.0;
+    for (int i = j; i < (int)blockDim.x; i += ML_KF) f += s_redf[i];
+    s_redf[j] = f;
   }
   __syncthreads();
   if (tid < ML_K) {
     double c = 0.0;
     for (int j = 0; j < ML_K; ++j) c += s_red[j] * cospi((double)tid * (2.0 * j + 1.0) / (2.0 * ML_K));
     s_c1[tid] = use_l1 ? (float)(c * (2.0 / ML_K)) : 0.f;
+  } else if (tid < ML_K + ML_KF) {
+    const int k = tid - ML_K;
+    double c = 0.0;
+    for (int j = 0; j < ML_KF; ++j) c += s_redf[j] * cospi((double)k * (2.0 * j + 1.0) / (2.0 * ML_KF));
+    s_c1f[k] = use_l1 ? (float)(c * (2.0 / ML_KF)) : 0.f;
   }
   // ---- level-2 node values of this warp: lanes j and j+16 hold halves of node j
   {
@@ -396,7 +428,10 @@ tau_ml_kernel(const LineF32* __restrict__ prep, int n_lines, const int2* __restr
     const int pl = w0 + lane * P + m;
     if (pl < n_c) {
       float v = s_core[pl];
-      if (use_l1) v += clenshaw16(c1, ((float)pl - C1) * inv_h1);
+      if (use_l1) {
+        const float t1 = ((float)pl - C1) * inv_h1;
+        v += clenshaw16(c1, t1) + clenshaw16<ML_KF>(s_c1f, t1);
+      }
       if (use_l2) v += clenshaw16(c2, ((float)pl - C2w) * inv_h2);
       const long long p = c0 + pl;
       const double nu = grid_nu(nu_min, step, p);
