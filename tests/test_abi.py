@@ -88,3 +88,36 @@ def test_engine_without_cuda_raises():
     from pylblrtm_b200 import synthetic
     with pytest.raises(_lib.EngineUnavailable, match="no CUDA device"):
         lbl.compute_transmittance(synthetic.co2_band(50), lbl.us_standard_atmosphere(["CO2"]), 700, 701)
+
+
+IO_HEADER = os.path.join(ROOT, "include", "lblio.h")
+
+
+def test_host_library_exports_its_header():
+    text = re.sub(r"/\*.*?\*/", "", open(IO_HEADER).read(), flags=re.S)
+    names = sorted(set(re.findall(r"\b(lbl_[a-z0-9_]+)\s*\(", text)))
+    assert names == sorted(_lib.HOST_SIGNATURES)
+    lib = ctypes.CDLL(_lib.IO_LIB_PATH)
+    assert all(hasattr(lib, n) for n in names)
+
+
+def test_line_pairs_scan_rejects_bad_arguments():
+    import numpy as np
+    host = _lib.load_host()
+    pm, pi_, pb = np.zeros(1, np.int32), np.zeros(1, np.int32), np.zeros(1, np.int64)
+    n = ctypes.c_int(0)
+    smax = ctypes.c_double(0.0)
+    mol = np.array([1, 2], np.int32)
+    iso = np.array([1, 1], np.int32)
+    nu = np.array([700.0, 701.0])
+    sh = np.array([0.0, -0.003])
+    idx = np.zeros(2, np.int32)
+    # two distinct pairs do not fit max_pairs = 1
+    assert host.lbl_line_pairs(mol.ctypes.data, iso.ctypes.data, nu.ctypes.data, sh.ctypes.data, 2, 690.0, 710.0,
+                               1.0, 1, pm.ctypes.data, pi_.ctypes.data, pb.ctypes.data, ctypes.byref(n),
+                               idx.ctypes.data, ctypes.byref(smax)) != 0
+    pm, pi_, pb = np.zeros(4, np.int32), np.zeros(4, np.int32), np.zeros(4, np.int64)
+    assert host.lbl_line_pairs(mol.ctypes.data, iso.ctypes.data, nu.ctypes.data, sh.ctypes.data, 2, 690.0, 710.0,
+                               1.0, 4, pm.ctypes.data, pi_.ctypes.data, pb.ctypes.data, ctypes.byref(n),
+                               idx.ctypes.data, ctypes.byref(smax)) == 0
+    assert n.value == 2 and list(idx) == [0, 1] and list(pb[:2]) == [1, 1] and smax.value == 0.003
