@@ -518,6 +518,7 @@ class Job:
             e1.record()
             timer.setdefault("tau_events", []).append((e0, e1))
         self.launches += 2
+        finish(od)                          # queue the layer sums before the error word is read
         self._raise_on_error(err, n_grp)
         if evals is not None:
             ev = evals.cpu().tolist()
@@ -527,7 +528,7 @@ class Job:
                 res.work = sum(res.work_split)
             else:
                 res.work = int(ev[0])
-        return finish(od)
+        return res
 
 
 def _jacobian_impl(job: Job, gas: str, g_tau=None, deterministic: bool = False):
