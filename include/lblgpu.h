@@ -167,12 +167,15 @@ int lbl_tau_tiles_f32(const LineF32* prep, int n_lines, const int* ranges, const
  * loop evaluations, [2] near-zone points. flags: LBL_DETERMINISTIC adds the
  * near-zone corrections in a fixed order (bit-reproducible across launches and
  * batchings); without it overlapping near zones are summed by shared-memory
- * atomics (reproducible to ~1e-9 relative). n_nu <= 1.5e9. Replaces
- * pylblrtm/forward.py:295-315. */
+ * atomics (reproducible to ~1e-9 relative). n_nu <= 1.5e9. Only the reference
+ * tiles [tile_first, tile_first + tile_count) of the grid are computed (all of
+ * them: 0 and ceil(n_nu / tile_samples)); od is then [n_rows, n_local] with the
+ * tiles' n_local points, grid values staying nu_min + i*step of the full grid (a
+ * wavenumber shard gives bit-identical results). Replaces pylblrtm/forward.py:295-315. */
 int lbl_tau_tiles_ml_f32(const LineF32* prep, int n_lines, const int* ranges, const double* t_layer, int n_rows,
                          double nu_min, double step, long long n_nu, int tile_samples, double cutoff, int n_grp,
-                         float* od, int* err, unsigned long long* evals, unsigned long long* work, int flags,
-                         void* stream);
+                         float* od, int* err, unsigned long long* evals, unsigned long long* work, int tile_first,
+                         int tile_count, int flags, void* stream);
 
 /* Layer Jacobians by the multi-level float32 summation (no reference
  * counterpart; the retrieval adjoint): writes od (as lbl_tau_tiles_ml_f32),

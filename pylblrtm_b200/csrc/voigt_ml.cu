@@ -90,7 +90,8 @@ __global__ void __launch_bounds__(ML_THREADS, 4)
 tau_ml_kernel(const LineF32* __restrict__ prep, int n_lines, const int2* __restrict__ ranges,
               const double* __restrict__ t_layer, double nu_min, double step, long long n_nu,
               int tile_samples, int chunks_per_tile, double cutoff, int n_grp, float* __restrict__ od,
-              int* err, unsigned long long* evals, unsigned long long* work) {
+              int* err, unsigned long long* evals, unsigned long long* work, int tile_first,
+              long long out_first, long long out_stride) {
   constexpr int P = ML_P;
   __shared__ MlLine s1[ML_THREADS];                 // level-1 lines of the round
   __shared__ MlLine s2[ML_THREADS];                 // inner lines of the round
@@ -110,7 +111,7 @@ tau_ml_kernel(const LineF32* __restrict__ prep, int n_lines, const int2* __restr
   __shared__ float s_c2[ML_THREADS / 32][ML_K];
 
   const int row = blockIdx.y;
-  const int tile = blockIdx.x / chunks_per_tile, chunk = blockIdx.x % chunks_per_tile;
+  const int tile = tile_first + (int)(blockIdx.x / chunks_per_tile), chunk = blockIdx.x % chunks_per_tile;
   const long long t0 = (long long)tile * tile_samples;
   const long long t1 = min(t0 + (long long)tile_samples, n_nu);
   const long long c0 = t0 + (long long)chunk * (blockDim.x * P);
@@ -417,7 +418,7 @@ tau_ml_kernel(const LineF32* __restrict__ prep, int n_lines, const int2* __restr
   __syncthreads();
 
   const double T = t_layer[row];
-  float* out = od + (long long)row * n_nu;
+  float* out = od + (long long)row * out_stride;   // points [out_first, out_first + out_stride) of the grid
   float c1[ML_K], c2[ML_K];
 #pragma unroll
   for (int k = 0; k < ML_K; ++k) { c1[k] = s_c1[k]; c2[k] = s_c2[warp][k]; }
@@ -437,7 +438,7 @@ tau_ml_kernel(const LineF32* __restrict__ prep, int n_lines, const int2* __restr
       const double nu = grid_nu(nu_min, step, p);
       const float o = (float)(((double)acc[m] + (double)v) * radiation_term_grid(nu, T));
       bad |= !isfinite(o);
-      out[p] = o;
+      out[p - out_first] = o;
     }
   }
   if (bad) flag_error(err, row * (n_grp + 1) + n_grp);
@@ -456,24 +457,33 @@ using namespace lbl;
 extern "C" int lbl_tau_tiles_ml_f32(const LineF32* prep, int n_lines, const int* ranges, const double* t_layer,
                                     int n_rows, double nu_min, double step, long long n_nu, int tile_samples,
                                     double cutoff, int n_grp, float* od, int* err, unsigned long long* evals,
-                                    unsigned long long* work, int flags, void* stream) {
+                                    unsigned long long* work, int tile_first, int tile_count, int flags,
+                                    void* stream) {
   if (!prep || !ranges || !t_layer || !od || n_lines < 1 || n_rows < 1 || n_rows > 65535 || n_nu < 1 ||
       n_nu > 1500000000LL || tile_samples < 1 || !(step > 0) || !(cutoff >= 0) || n_grp < 1)
     return lbl_set_error(LBL_EINVAL, "lbl_tau_tiles_ml_f32: bad arguments");
+  const long long n_all = (n_nu + tile_samples - 1) / tile_samples;
+  if (tile_first < 0 || tile_count < 1 || (long long)tile_first + tile_count > n_all)
+    return lbl_set_error(LBL_EINVAL, "lbl_tau_tiles_ml_f32: tile range outside the grid");
+  const long long out_first = (long long)tile_first * tile_samples;
+  const long long out_end = (long long)(tile_first + tile_count) * tile_samples < n_nu
+                                ? (long long)(tile_first + tile_count) * tile_samples : n_nu;
   const int per_tile = tile_samples < ML_CHUNK ? tile_samples : ML_CHUNK;
   const int threads = 32 * ((per_tile + ML_WARP_PTS - 1) / ML_WARP_PTS);
   const int cp = threads * ML_P;
-  const long long n_tiles = (n_nu + tile_samples - 1) / tile_samples;
+  const long long n_tiles = tile_count;
   const long long chunks = (tile_samples + cp - 1) / cp;
   if (n_tiles * chunks > 0x7fffffffLL) return lbl_set_error(LBL_EINVAL, "lbl_tau_tiles_ml_f32: grid too large");
   dim3 grid((unsigned)(n_tiles * chunks), (unsigned)n_rows);
   if (flags & LBL_DETERMINISTIC)
     tau_ml_kernel<true><<<grid, threads, 0, (cudaStream_t)stream>>>(prep, n_lines, (const int2*)ranges, t_layer,
                                                                    nu_min, step, n_nu, tile_samples, (int)chunks,
-                                                                   cutoff, n_grp, od, err, evals, work);
+                                                                   cutoff, n_grp, od, err, evals, work,
+                                                                   tile_first, out_first, out_end - out_first);
   else
     tau_ml_kernel<false><<<grid, threads, 0, (cudaStream_t)stream>>>(prep, n_lines, (const int2*)ranges, t_layer,
                                                                     nu_min, step, n_nu, tile_samples, (int)chunks,
-                                                                    cutoff, n_grp, od, err, evals, work);
+                                                                    cutoff, n_grp, od, err, evals, work,
+                                                                    tile_first, out_first, out_end - out_first);
   return lbl_check_launch("lbl_tau_tiles_ml_f32");
 }

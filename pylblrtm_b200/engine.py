@@ -427,11 +427,14 @@ class Job:
     def run(self, precision: str = "fp32", mu: Optional[Sequence[float]] = None, want_od: bool = True,
             want_tau: bool = False, want_trans: bool = False, count_evals: bool = False,
             timer: Optional[dict] = None, channels: Optional[Tuple[int, int]] = None,
-            deterministic: bool = False) -> EngineResult:
+            deterministic: bool = False, tiles: Optional[Tuple[int, int]] = None) -> EngineResult:
         """All device stages; ``timer`` (dict) receives CUDA-event times of the summation kernel.
 
         ``channels = (width_points, n_channels)`` adds channel-mean transmittances
         over consecutive half-open blocks of ``width_points`` grid points.
+        ``tiles = (first, count)`` (multi-level float32 engine only) computes just those
+        reference tiles of the grid: od, tau and trans then cover their points only,
+        with the grid values of the full grid (a wavenumber shard).
         """
         if precision not in PRECISIONS:
             raise ValueError(f"precision must be one of {PRECISIONS}, got {precision!r}")
@@ -442,6 +445,14 @@ class Job:
         grid = self.grid
         n_prof, n_lay, n_nu = self.n_prof, self.n_lay, grid.n_nu
         n_rows = n_prof * n_lay
+        n_tiles = -(-n_nu // grid.tile_samples)
+        t_first, t_count = (0, n_tiles) if tiles is None else (int(tiles[0]), int(tiles[1]))
+        if tiles is not None:
+            if precision != "fp32" or channels is not None:
+                raise ValueError("tiles needs precision 'fp32' and no channels")
+            if t_first < 0 or t_count < 1 or t_first + t_count > n_tiles:
+                raise ValueError(f"tiles ({t_first}, {t_count}) outside the grid's {n_tiles} tiles")
+        n_nu = min(n_nu, (t_first + t_count) * grid.tile_samples) - t_first * grid.tile_samples
         res = EngineResult(groups=self.groups)
         single = precision != "fp64"
         od_dtype = torch.float32 if single else torch.float64
@@ -507,10 +518,11 @@ class Job:
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             e0.record()
         common = (prep.data_ptr(), n_kept, ranges.data_ptr(), t_lay.data_ptr(), n_rows, grid.nu_min, grid.step,
-                  n_nu, grid.tile_samples, self.cutoff, n_grp, od.data_ptr(), err.data_ptr(), _lib.ptr(evals))
+                  grid.n_nu, grid.tile_samples, self.cutoff, n_grp, od.data_ptr(), err.data_ptr(),
+                  _lib.ptr(evals))
         if precision == "fp32":
             _lib.call("lbl_tau_tiles_ml_f32", *common,
-                      0 if evals is None else evals.data_ptr() + 8,
+                      0 if evals is None else evals.data_ptr() + 8, t_first, t_count,
                       _lib.LBL_DETERMINISTIC if deterministic else 0, stream)
         else:
             _lib.call("lbl_tau_tiles_f32" if single else "lbl_tau_tiles_f64", *common, stream)

@@ -4,8 +4,11 @@ The forward model shards without any data-path exchange: profiles of a batch are
 independent, so each rank computes a contiguous slice of them
 (:func:`profile_slice`) and the results are gathered once at the end
 (:func:`transmittance_batch_sharded`, an all-gather over NCCL / NVLink, or over gloo
-on CPU). A single spectrum is not split: every rank runs its own (the bench's
-replicas, weak scaling).
+on CPU). One spectrum splits by wavenumber (:func:`compute_transmittance_sharded`):
+each rank computes a contiguous range of the grid's reference tiles with the grid
+values of the full grid (every line list and layer on every rank; the tile-window
+rule makes the tiles independent), and the pieces are all-gathered; with the
+deterministic sums the result equals the single-GPU spectrum bit for bit.
 
 The surrogate's training has one real exchange step: data-parallel ranks sum their
 weight and bias gradients (:func:`allreduce_gradients`) between the backward pass and
@@ -85,6 +88,67 @@ def transmittance_batch_sharded(spectral_data, pressure_hpa, temperature_k, vmr,
     if not gather:
         return axis, local
     return axis, gather_rows(local, n, group)
+
+
+def gather_pieces(local, counts: Sequence[int], group=None):
+    """All-gather 1-D pieces of known lengths ``counts`` (rank order) into one tensor."""
+    import torch
+    dist = _dist()
+    world, _ = world_and_rank(group)
+    if world == 1:
+        return local
+    m = max(max(counts), 1)
+    pad = torch.zeros(m, dtype=local.dtype, device=local.device)
+    pad[: local.numel()] = local
+    parts = [torch.empty_like(pad) for _ in range(world)]
+    dist.all_gather(parts, pad, group=group)
+    return torch.cat([p[:c] for p, c in zip(parts, counts)])
+
+
+def compute_transmittance_sharded(spectral_data, profile, nu_min_cm1: float, nu_max_cm1: float, *,
+                                  step_cm1: float = 0.001, line_cutoff_cm1: float = 25.0,
+                                  tile_width_cm1: float = 2.0, mu_view: float = 1.0, deterministic: bool = True,
+                                  group=None, compute: Optional[Callable] = None):
+    """``compute_transmittance`` with the reference tiles of the grid split across the
+    ranks of ``group`` (multi-level float32 engine). Every rank returns the full
+    ``(nu, T)``. ``compute(first, count)`` replaces the device computation of a tile
+    range (tests); it returns that range's transmittance as a 1-D tensor.
+    """
+    import torch
+    from . import engine
+    from .atmosphere import AtmosphericProfile
+    from .spectral_data import SpectralData
+    if compute is None:
+        if not isinstance(spectral_data, SpectralData):
+            raise TypeError("spectral_data must be a SpectralData instance")
+        if not isinstance(profile, AtmosphericProfile):
+            raise TypeError("profile must be an AtmosphericProfile instance")
+    if nu_min_cm1 >= nu_max_cm1:
+        raise ValueError("nu_min_cm1 must be strictly less than nu_max_cm1")
+    if step_cm1 <= 0:
+        raise ValueError("step_cm1 must be positive")
+    if not (0.0 < mu_view <= 1.0):
+        raise ValueError("mu_view must be in (0, 1]")
+    grid = engine.make_grid(nu_min_cm1, nu_max_cm1, step_cm1, tile_width_cm1)
+    ts = grid.tile_samples
+    n_tiles = -(-grid.n_nu // ts)
+    world, rank = world_and_rank(group)
+    spans = [profile_slice(n_tiles, world, r) for r in range(world)]
+    counts = [max(0, min(grid.n_nu, sl.stop * ts) - sl.start * ts) if sl.stop > sl.start else 0 for sl in spans]
+    sl = spans[rank]
+    if compute is None:
+        def compute(first, count):
+            job = engine.Job(spectral_data, engine.layer_input_from_profile(profile), grid,
+                             float(line_cutoff_cm1), warn_level=3)
+            res = job.run("fp32", mu=[float(mu_view)], want_od=False, want_trans=True,
+                          deterministic=deterministic, tiles=(first, count))
+            return res.trans[0]
+    dev = torch.device("cuda", torch.cuda.current_device()) if torch.cuda.is_available() else torch.device("cpu")
+    local = compute(sl.start, sl.stop - sl.start) if sl.stop > sl.start else \
+        torch.zeros(0, dtype=torch.float64, device=dev)
+    full = gather_pieces(local, counts, group)
+    out = full.cpu().numpy() if full.is_cuda else full.numpy()
+    return grid.nu, out
 
 
 def allreduce_gradients(grads: Sequence, group=None) -> None:

@@ -275,3 +275,25 @@ def test_fp32_bitwise_reproducible_with_overlapping_near_zones(cuda):
     assert torch.max(torch.abs(d - a)).item() <= 1e-6 * torch.max(torch.abs(a)).item()
     with pytest.raises(ValueError, match="deterministic"):
         single.run("fp32-direct", deterministic=True)
+
+
+def test_wavenumber_shards_equal_the_full_spectrum(cuda):
+    """Reference tiles computed in three ranges (shards) give the full spectrum bit for bit."""
+    from pylblrtm_b200 import shard
+    sd = synthetic.restrict(synthetic.three_gas_lines(30000, 1480.0, 1540.0, seed=9), 1480.0, 1540.0)
+    prof = synthetic.profile_from_levels(synthetic.logp_levels(9))
+    sd = synthetic.scale_strengths(sd, 1e-4)
+    grid = engine.make_grid(1500.0, 1507.3, 0.001, 2.0)          # 4 tiles, the last one partial
+    job = engine.Job(sd, engine.layer_input_from_profile(prof), grid, 25.0)
+    full = job.run("fp32", mu=[0.8], want_od=True, want_trans=True, deterministic=True)
+    pieces = [job.run("fp32", mu=[0.8], want_od=True, want_trans=True, deterministic=True, tiles=t)
+              for t in ((0, 1), (1, 2), (3, 1))]
+    assert torch.equal(torch.cat([p.trans for p in pieces], dim=1), full.trans)
+    assert torch.equal(torch.cat([p.od for p in pieces], dim=2), full.od)
+    nu, t = shard.compute_transmittance_sharded(sd, prof, 1500.0, 1507.3, mu_view=0.8)
+    _, t_ref = lbl.compute_transmittance(sd, prof, 1500.0, 1507.3, mu_view=0.8, deterministic=True)
+    assert np.array_equal(t, t_ref) and t.min() < 0.99
+    with pytest.raises(ValueError, match="outside the grid"):
+        job.run("fp32", tiles=(3, 2))
+    with pytest.raises(ValueError, match="tiles needs"):
+        job.run("fp64", tiles=(0, 1))

@@ -54,7 +54,14 @@ def _worker(rank, world, port, out):
         shard.allreduce_gradients(grads)
         tot = sum(r + 1 for r in range(world))
         ok_reduce = all(torch.equal(g, tot * b) for g, b in zip(grads, base))
-        out[rank] = int(ok_gather) + 2 * int(ok_local) + 4 * int(ok_reduce)
+        # wavenumber shards: the fake computation returns each point's global index
+        grid_n = 2001                                   # 0.0005 step over 1 cm^-1, tiles of 400 points
+        def fake(first, count):
+            return torch.arange(first * 400, min(grid_n, (first + count) * 400), dtype=torch.float64)
+        nu, t = shard.compute_transmittance_sharded(None, None, 700.0, 701.0, step_cm1=0.0005, tile_width_cm1=0.2,
+                                                    compute=fake)
+        ok_wave = t.shape == (grid_n,) and np.array_equal(t, np.arange(grid_n, dtype=np.float64)) and nu.size == grid_n
+        out[rank] = int(ok_gather) + 2 * int(ok_local) + 4 * int(ok_reduce) + 8 * int(ok_wave)
     finally:
         dist.destroy_process_group()
 
@@ -69,7 +76,7 @@ def test_two_gloo_ranks_gather_and_reduce():
     world = 2
     out = mp.get_context("spawn").Manager().dict()
     mp.start_processes(_worker, args=(world, _free_port(), out), nprocs=world, join=True, start_method="spawn")
-    assert dict(out) == {0: 7, 1: 7}
+    assert dict(out) == {0: 15, 1: 15}
 
 
 def test_single_process_is_identity():
