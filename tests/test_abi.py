@@ -121,3 +121,31 @@ def test_line_pairs_scan_rejects_bad_arguments():
                                1.0, 4, pm.ctypes.data, pi_.ctypes.data, pb.ctypes.data, ctypes.byref(n),
                                idx.ctypes.data, ctypes.byref(smax)) == 0
     assert n.value == 2 and list(idx) == [0, 1] and list(pb[:2]) == [1, 1] and smax.value == 0.003
+
+
+def _declared_arities(header):
+    """Parameter count of every lbl_* function declared in a header."""
+    text = re.sub(r"/\*.*?\*/", "", open(header).read(), flags=re.S)
+    out = {}
+    for m in re.finditer(r"\b(lbl_[a-z0-9_]+)\s*\(([^;{]*?)\)\s*;", text, flags=re.S):
+        params = m.group(2).strip()
+        out[m.group(1)] = 0 if params in ("", "void") else params.count(",") + 1
+    return out
+
+
+def test_binding_arities_match_headers():
+    """Every ctypes binding passes exactly the parameters its C declaration has."""
+    for header, sigs in ((HEADER, _lib.SIGNATURES), (IO_HEADER, _lib.HOST_SIGNATURES)):
+        arity = _declared_arities(header)
+        assert sorted(arity) == sorted(sigs)
+        bad = {n: (arity[n], len(sigs[n][1])) for n in sigs if arity[n] != len(sigs[n][1])}
+        assert not bad, bad
+
+
+def test_built_library_is_current():
+    """The in-tree libraries are newer than every source they are built from."""
+    from pylblrtm_b200.csrc import build as b
+    deps = b.SOURCES + b.HEADERS
+    assert not b._stale(b.LIB, deps), "liblblgpu.so is older than its sources: rebuild"
+    io_deps = ["hitran_par.cpp", "host_scan.cpp", os.path.join("..", "..", "include", "lblio.h")]
+    assert not b._stale(b.IO_LIB, io_deps), "liblblio.so is older than its sources: rebuild"
