@@ -434,18 +434,19 @@ def main():
     acc = None if (a.no_accuracy or world > 1 or (a.nu_min, a.nu_max) != (600.0, 2500.0)) else accuracy(torch, job)
     tau_avg = sum(tau_ms) / len(tau_ms)
     # HBM-bound stages: algorithmic bytes / CUDA-event time
-    hbm_peak = None
     try:
         with open(os.path.join(os.path.dirname(os.path.abspath(__file__)), "MEASURED_PEAKS.json")) as f:
             hbm_peak = float(json.load(f)["hbm_gbs"])
+        hbm_source = "MEASURED_PEAKS.json hbm_gbs (copy, burst), of measured"
     except (OSError, KeyError, ValueError):
         hbm_peak = 6650.0
+        hbm_source = "fallback 6650 GB/s (no MEASURED_PEAKS.json), of fallback"
     n_rows_, n_kept_, n_grp_, rec_ = timer["prep_shape"]
     prep_ms = sum(b.elapsed_time(c) for b, c in timer["prep_events"]) / len(timer["prep_events"])
     sum_ms = sum(b.elapsed_time(c) for b, c in timer["sum_events"]) / len(timer["sum_events"])
     prep_bytes = n_rows_ * n_kept_ * rec_ + n_kept_ * 64 + n_rows_ * n_grp_ * 48
     sum_bytes = n_rows_ * grid.n_nu * (4 if a.precision != "fp64" else 8) + grid.n_nu * 8
-    hbm = {"peak_gbs": hbm_peak, "peak_source": "MEASURED_PEAKS.json hbm_gbs (copy, burst)",
+    hbm = {"peak_gbs": hbm_peak, "peak_source": hbm_source,
            "line_prep": {"ms": prep_ms, "bytes": prep_bytes, "gbs": prep_bytes / prep_ms / 1e6,
                          "frac": prep_bytes / prep_ms / 1e6 / hbm_peak,
                          "bytes_rule": "32-B record written per (layer, line) + 64-B line record read once "
