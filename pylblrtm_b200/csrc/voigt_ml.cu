@@ -9,7 +9,9 @@
 //           (<= 2048 points of one reference tile): their summed profile is
 //           analytic on a Bernstein ellipse with rho >= 2 + sqrt(3) around the
 //           chunk, so it is evaluated at K1 = 16 Chebyshev nodes and interpolated
-//           (interpolation error ~rho^-16 ~ 1e-9 of the level-1 sum);
+//           (interpolation error ~rho^-16 ~ 1e-9 of the level-1 sum; lines more than
+//           six half-widths out use 8 nodes). A separate kernel (tau_far_kernel)
+//           computes this level and writes its interpolant into od;
 //  level 2  the other lines farther than one sub-chunk half-width from a warp's
 //           256-point sub-chunk: 16 Chebyshev nodes per sub-chunk, same geometry;
 //  level 3  the remaining lines: direct evaluation at every point. The warp's
@@ -17,11 +19,13 @@
 //           |z|^2 clamped to >= MID_Z2 = 64, so every point inside a line's near
 //           zone receives the same constant. A CTA-wide near pass then gives each
 //           near point (accurate value - that constant): float continued fraction
-//           for 36 <= |z|^2 < 64, Weideman's float64 approximation below. Its values
-//           are added per point in a fixed order, so results are bit-reproducible.
+//           for 36 <= |z|^2 < 64, Weideman's float64 approximation below.
 //
 // Inside a reference tile the set of lines is fixed, so every level-1/2 sum is
 // smooth over its interval; the window test keeps the reference's truncation.
+// tau_ml_kernel reads only the lines that can be inner for its chunk (a range per
+// tile from lbl_ml_inner_ranges), applies the same level-1 test and skips the
+// level-1 lines among them.
 #include <math.h>
 
 #include "faddeeva.cuh"
@@ -85,29 +89,219 @@ __device__ __forceinline__ float clenshaw16(const float* c, float t) {
   return fmaf(t, b1, 0.5f * c[0] - b2);
 }
 
+// ---------------------------------------------------------------------------
+// Level 1 as its own kernel. Nine in ten lines of a chunk's window are level-1
+// lines; each contributes only through the chunk's Chebyshev nodes, so one thread
+// takes one line and evaluates it at all nodes from registers (no shared-memory
+// staging, no barriers). The kernel writes the level-1 interpolant of every chunk
+// point into od, where tau_ml_kernel adds the inner lines and applies R(nu, T).
+constexpr int MF_THREADS = 256;                // lines per round
+constexpr int MF_FLUSH = 8;                    // rounds summed in float before the double sums
+
+__device__ __forceinline__ LineF32 load_line(const LineF32* p) {
+  union {
+    float4 v[2];
+    LineF32 l;
+  } u;
+  const float4* q = reinterpret_cast<const float4*>(p);   // records are 32 B in a cudaMalloc'd array
+  u.v[0] = __ldg(q);
+  u.v[1] = __ldg(q + 1);
+  return u.l;
+}
+
+// amp * Re w by the far-wing form (amp_far = amp y / sqrt(pi)), added to f (|z|^2 >= FAR_Z2, y >= 0).
+__device__ __forceinline__ void far_wing_add(float& f, float x, float y2, float ny2, float amp_far) {
+  const float r = rcp_approx(fmaf(x, x, y2));
+  f = fmaf(amp_far * r, fmaf(fmaf(ny2, r, 1.5f), r, 1.0f), f);
+}
+
+// amp * Re w at one node for a level-1 line that is not in the far-wing regime at
+// every node (broad lines, coarse geometry): the engine's full float32 algorithm.
+static __device__ __noinline__ float far_node_general(float x, float y, float y2, float amp, float amp_far) {
+  const float z2 = fmaf(x, x, y2);
+  if (z2 >= FAR_Z2 && y >= 0.f) {
+    const float r = rcp_approx(z2);
+    return amp_far * r * fmaf(fmaf(-2.0f * y2, r, 1.5f), r, 1.0f);
+  }
+  if (z2 >= CORE_Z2 && y >= 0.f) return amp * re_w_f32_mid(x, y, y2, z2);
+  return (float)((double)amp * weideman_re((double)x, (double)y));
+}
+
+// Node sums of one level-1 line: nodes k and K-1-k sit at +xs[k] and -xs[k] from the chunk centre.
+template <int K>
+__device__ __forceinline__ void far_line_nodes(float (&f)[K], const float (&xs)[K / 2], const LineF32& L, float xc,
+                                               float y2, bool fast) {
+  if (fast) {
+    const float ny2 = -2.0f * y2, na = -L.a;
+#pragma unroll
+    for (int k = 0; k < K / 2; ++k) {
+      far_wing_add(f[k], fmaf(xs[k], L.a, xc), y2, ny2, L.amp_far);
+      far_wing_add(f[K - 1 - k], fmaf(xs[k], na, xc), y2, ny2, L.amp_far);
+    }
+  } else {
+#pragma unroll
+    for (int k = 0; k < K / 2; ++k) {
+      f[k] += far_node_general(fmaf(xs[k], L.a, xc), L.y, y2, L.amp, L.amp_far);
+      f[K - 1 - k] += far_node_general(fmaf(xs[k], -L.a, xc), L.y, y2, L.amp, L.amp_far);
+    }
+  }
+}
+
+__global__ void __launch_bounds__(MF_THREADS, 2)
+tau_far_kernel(const LineF32* __restrict__ prep, int n_lines, const int2* __restrict__ ranges, double nu_min,
+               double step, long long n_nu, int tile_samples, int chunks_per_tile, int chunk_pts, double cutoff,
+               float* __restrict__ od, unsigned long long* evals, unsigned long long* work, int tile_first,
+               long long out_first, long long out_stride) {
+  __shared__ double s_part[MF_THREADS / 32][ML_K + ML_KF];
+  __shared__ float s_coef[ML_K + ML_KF];
+  __shared__ unsigned s_cnt[2];
+
+  const int row = blockIdx.y;
+  const int tile = tile_first + (int)(blockIdx.x / chunks_per_tile), chunk = blockIdx.x % chunks_per_tile;
+  const long long t0 = (long long)tile * tile_samples;
+  const long long t1 = min(t0 + (long long)tile_samples, n_nu);
+  const long long c0 = t0 + (long long)chunk * chunk_pts;
+  if (c0 >= t1) return;
+  const int n_c = (int)(min(c0 + (long long)chunk_pts, t1) - c0);
+  const float H1 = 0.5f * (float)(n_c - 1), C1 = H1;      // same chunk geometry as tau_ml_kernel
+  if (!(H1 >= ML_MIN_H1)) return;                         // no level 1: tau_ml_kernel takes every line
+  const int c0i = (int)c0;
+  const double wlo = __dsub_rn(grid_nu(nu_min, step, t0), cutoff);
+  const double whi = __dadd_rn(grid_nu(nu_min, step, t1 - 1), cutoff);
+  const int2 rng = ranges[tile];
+  const LineF32* lp = prep + (long long)row * n_lines;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  if (tid < 2) s_cnt[tid] = 0u;
+
+  float xa[ML_K / 2], xb[ML_KF / 2];                      // node offsets, as tau_ml_kernel places them
+#pragma unroll
+  for (int k = 0; k < ML_K / 2; ++k) xa[k] = H1 * (float)cospi((2.0 * k + 1.0) / (2.0 * ML_K));
+#pragma unroll
+  for (int k = 0; k < ML_KF / 2; ++k) xb[k] = H1 * (float)cospi((2.0 * k + 1.0) / (2.0 * ML_KF));
+
+  float f1[ML_K], ff[ML_KF];
+  double d1[ML_K], df[ML_KF];
+#pragma unroll
+  for (int k = 0; k < ML_K; ++k) { f1[k] = 0.f; d1[k] = 0.0; }
+#pragma unroll
+  for (int k = 0; k < ML_KF; ++k) { ff[k] = 0.f; df[k] = 0.0; }
+  unsigned n1 = 0, nf = 0;
+
+  LineF32 nxt;
+  if (rng.x + tid < rng.y) nxt = load_line(lp + rng.x + tid);
+  int rounds = 0;
+  for (int base = rng.x; base < rng.y; base += MF_THREADS) {
+    const LineF32 L = nxt;
+    const bool have = base + tid < rng.y;
+    if (base + MF_THREADS + tid < rng.y) nxt = load_line(lp + base + MF_THREADS + tid);
+    // the level-1 test of tau_ml_kernel, expression for expression
+    const bool pass = have && (L.nuc >= wlo) && (L.nuc <= whi);
+    const float jf = (float)(L.j0 - c0i);
+    const float dd = fabsf(jf - C1) - H1;
+    if (pass && dd > H1 + 1.f) {
+      const float xc = fmaf(C1 - jf, L.a, -L.b);         // line centre -> chunk centre, in x units
+      const float y2 = L.y * L.y;
+      // every node lies on one side of the line; the nearest is xa[0] in from the centre
+      const float xm = fmaf(-xa[0], L.a, fabsf(xc));
+      const bool fast = fmaf(xm, xm, y2) >= FAR_Z2 && L.y >= 0.f;
+      if (dd > ML_FAR1 * H1) {
+        far_line_nodes<ML_KF>(ff, xb, L, xc, y2, fast);
+        ++nf;
+      } else {
+        far_line_nodes<ML_K>(f1, xa, L, xc, y2, fast);
+        ++n1;
+      }
+    }
+    if (++rounds == MF_FLUSH) {
+      rounds = 0;
+#pragma unroll
+      for (int k = 0; k < ML_K; ++k) { d1[k] += (double)f1[k]; f1[k] = 0.f; }
+#pragma unroll
+      for (int k = 0; k < ML_KF; ++k) { df[k] += (double)ff[k]; ff[k] = 0.f; }
+    }
+  }
+#pragma unroll
+  for (int k = 0; k < ML_K; ++k) d1[k] += (double)f1[k];
+#pragma unroll
+  for (int k = 0; k < ML_KF; ++k) df[k] += (double)ff[k];
+
+  // node sums over the CTA in double: warps, then across warps
+#pragma unroll
+  for (int k = 0; k < ML_K; ++k) {
+    double v = d1[k];
+#pragma unroll
+    for (int o = 16; o >= 1; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    if (lane == 0) s_part[warp][k] = v;
+  }
+#pragma unroll
+  for (int k = 0; k < ML_KF; ++k) {
+    double v = df[k];
+#pragma unroll
+    for (int o = 16; o >= 1; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    if (lane == 0) s_part[warp][ML_K + k] = v;
+  }
+  n1 = __reduce_add_sync(0xffffffffu, n1);
+  nf = __reduce_add_sync(0xffffffffu, nf);
+  __syncthreads();                                         // s_cnt zeroed, s_part written
+  if (lane == 0) {
+    atomicAdd(&s_cnt[0], n1);
+    atomicAdd(&s_cnt[1], nf);
+  }
+  if (tid < ML_K + ML_KF) {                                // column tid: only this thread touches it
+    double s = 0.0;
+    for (int w = 0; w < MF_THREADS / 32; ++w) s += s_part[w][tid];
+    s_part[0][tid] = s;
+  }
+  __syncthreads();
+  // Chebyshev coefficients (DCT of the node values)
+  if (tid < ML_K) {
+    double c = 0.0;
+    for (int j = 0; j < ML_K; ++j) c += s_part[0][j] * cospi((double)tid * (2.0 * j + 1.0) / (2.0 * ML_K));
+    s_coef[tid] = (float)(c * (2.0 / ML_K));
+  } else if (tid < ML_K + ML_KF) {
+    const int k = tid - ML_K;
+    double c = 0.0;
+    for (int j = 0; j < ML_KF; ++j)
+      c += s_part[0][ML_K + j] * cospi((double)k * (2.0 * j + 1.0) / (2.0 * ML_KF));
+    s_coef[tid] = (float)(c * (2.0 / ML_KF));
+  }
+  __syncthreads();
+  float c1[ML_K], cf[ML_KF];
+#pragma unroll
+  for (int k = 0; k < ML_K; ++k) c1[k] = s_coef[k];
+#pragma unroll
+  for (int k = 0; k < ML_KF; ++k) cf[k] = s_coef[ML_K + k];
+  const float inv_h1 = 1.0f / H1;
+  float* out = od + (long long)row * out_stride + (c0 - out_first);
+  for (int p = tid; p < n_c; p += MF_THREADS) {
+    const float t = ((float)p - C1) * inv_h1;
+    out[p] = clenshaw16(c1, t) + clenshaw16<ML_KF>(cf, t);
+  }
+  if (tid == 0) {
+    const unsigned long long a = s_cnt[0], b = s_cnt[1];
+    if (evals && a + b) atomicAdd(evals, (a + b) * (unsigned long long)n_c);
+    if (work && a + b) atomicAdd(&work[0], a * ML_K + b * ML_KF);
+  }
+}
+
 template <bool DET>
 __global__ void __launch_bounds__(ML_THREADS, 4)
 tau_ml_kernel(const LineF32* __restrict__ prep, int n_lines, const int2* __restrict__ ranges,
-              const double* __restrict__ t_layer, double nu_min, double step, long long n_nu,
-              int tile_samples, int chunks_per_tile, double cutoff, int n_grp, float* __restrict__ od,
-              int* err, unsigned long long* evals, unsigned long long* work, int tile_first,
-              long long out_first, long long out_stride) {
+              const int2* __restrict__ inner_ranges, const double* __restrict__ t_layer, double nu_min,
+              double step, long long n_nu, int tile_samples, int chunks_per_tile, double cutoff, int n_grp,
+              float* __restrict__ od, int* err, unsigned long long* evals, unsigned long long* work,
+              int tile_first, long long out_first, long long out_stride) {
   constexpr int P = ML_P;
-  __shared__ MlLine s1[ML_THREADS];                 // level-1 lines of the round
   __shared__ MlLine s2[ML_THREADS];                 // inner lines of the round
   __shared__ unsigned char s_l2[ML_THREADS / 32][ML_THREADS];   // per-warp level-2 slots
   __shared__ unsigned char s_l3[ML_THREADS / 32][ML_THREADS];   // per-warp level-3 slots
   __shared__ unsigned char s_nl[ML_THREADS / 32][ML_THREADS];   // per-warp slots with near points in it
-  __shared__ int s_cnt[4][ML_THREADS / 32];
+  __shared__ int s_cnt[2][ML_THREADS / 32];
   __shared__ int s_seg_start[ML_THREADS + 1];       // near-item prefix per inner slot
   __shared__ short s_seg_lo[ML_THREADS];            // first near point per inner slot
   __shared__ unsigned char s_seg_mask[ML_THREADS];  // warps treating the inner line directly (level 3)
   __shared__ float s_core[ML_CHUNK];               // near-zone corrections (each point owned by one thread)
   __shared__ float s_nbuf[ML_NB];                   // near-item values of one batch
-  __shared__ double s_red[ML_THREADS];
-  __shared__ double s_redf[ML_THREADS];
-  __shared__ float s_c1[ML_K];
-  __shared__ float s_c1f[ML_KF];
   __shared__ float s_c2[ML_THREADS / 32][ML_K];
 
   const int row = blockIdx.y;
@@ -120,21 +314,25 @@ tau_ml_kernel(const LineF32* __restrict__ prep, int n_lines, const int2* __restr
   const int c0i = (int)c0;
   const double wlo = __dsub_rn(grid_nu(nu_min, step, t0), cutoff);
   const double whi = __dadd_rn(grid_nu(nu_min, step, t1 - 1), cutoff);
-  const int2 rng = ranges[tile];
   const LineF32* lp = prep + (long long)row * n_lines;
 
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, n_warps = blockDim.x >> 5;
   // chunk geometry (points relative to c0)
   const float H1 = 0.5f * (float)(n_c - 1), C1 = H1;
   const bool use_l1 = H1 >= ML_MIN_H1;
+  // With level 1 (done by tau_far_kernel) only lines inside the tile's inner range
+  // can be inner lines of this chunk; without it every line of the window is.
+  int2 rng = ranges[tile];
+  if (use_l1 && inner_ranges) {
+    const int2 q = inner_ranges[tile];
+    rng = make_int2(max(rng.x, q.x), min(rng.y, q.y));
+  }
   // this warp's sub-chunk
   const int w0 = warp * ML_WARP_PTS;
   const int n_w = max(0, min(ML_WARP_PTS, n_c - w0));
   const float H2 = 0.5f * (float)(n_w - 1), C2w = (float)w0 + H2;
   const bool use_l2 = H2 >= ML_MIN_H2;
-  // Chebyshev node offsets owned by this thread: level 1 node (tid & 15), level 2 node (lane & 15)
-  const float xn1 = H1 * (float)cospi((2.0 * (tid & 15) + 1.0) / (2.0 * ML_K));
-  const float xn1f = H1 * (float)cospi((2.0 * (tid & 7) + 1.0) / (2.0 * ML_KF));
+  // level-2 Chebyshev node owned by this lane: (lane & 15)
   const float xn2 = H2 * (float)cospi((2.0 * (lane & 15) + 1.0) / (2.0 * ML_K));
   const float pf = (float)(w0 + lane * P);                   // this lane's first point
 
@@ -145,7 +343,7 @@ tau_ml_kernel(const LineF32* __restrict__ prep, int n_lines, const int2* __restr
   float acc[P];
 #pragma unroll
   for (int m = 0; m < P; ++m) acc[m] = 0.f;
-  float sum1 = 0.f, comp1 = 0.f, sumf = 0.f, compf = 0.f, sum2 = 0.f, comp2 = 0.f;
+  float sum2 = 0.f, comp2 = 0.f;
   unsigned long long n_pass = 0, n_nodes = 0, n_l3 = 0, n_near_items = 0;
 
   // register prefetch of the next round's line records
@@ -160,8 +358,7 @@ tau_ml_kernel(const LineF32* __restrict__ prep, int n_lines, const int2* __restr
     const bool pass = have && (L.nuc >= wlo) && (L.nuc <= whi);
     const float jf = (float)(L.j0 - c0i);           // |j0 - c0| < 1.5e9 (grid index span check)
     const float d1 = fabsf(jf - C1) - H1;
-    const bool lev1 = pass && use_l1 && (d1 > H1 + 1.f);
-    const bool lev1f = lev1 && (d1 > ML_FAR1 * H1);     // far: 8 nodes suffice
+    const bool lev1 = pass && use_l1 && (d1 > H1 + 1.f);   // tau_far_kernel's line
     const bool inner = pass && !lev1;
     // near range (points with possibly |z|^2 < MID_Z2) of an inner line, clipped to the chunk
     const float y2 = L.y * L.y;
@@ -193,66 +390,32 @@ tau_ml_kernel(const LineF32* __restrict__ prep, int n_lines, const int2* __restr
       const int t = __shfl_up_sync(0xffffffffu, near_scan, o);
       if (lane >= o) near_scan += t;
     }
-    const unsigned b1 = __ballot_sync(0xffffffffu, lev1 && !lev1f), bf = __ballot_sync(0xffffffffu, lev1f);
     const unsigned b2 = __ballot_sync(0xffffffffu, inner);
-    if (lane == 0) { s_cnt[0][warp] = __popc(b1); s_cnt[1][warp] = __popc(b2); s_cnt[3][warp] = __popc(bf); }
-    if (lane == 31) s_cnt[2][warp] = near_scan;
+    if (lane == 0) s_cnt[0][warp] = __popc(b2);
+    if (lane == 31) s_cnt[1][warp] = near_scan;
     __syncthreads();
-    int off1 = 0, offf = 0, off2 = 0, off3 = 0, n1 = 0, nf = 0, n2 = 0, n_near = 0;
+    int off2 = 0, off3 = 0, n2 = 0, n_near = 0;
     for (int w = 0; w < n_warps; ++w) {
-      const int a1 = s_cnt[0][w], a2 = s_cnt[1][w], a3 = s_cnt[2][w], af = s_cnt[3][w];
-      off1 += (w < warp) ? a1 : 0;
-      offf += (w < warp) ? af : 0;
+      const int a2 = s_cnt[0][w], a3 = s_cnt[1][w];
       off2 += (w < warp) ? a2 : 0;
       off3 += (w < warp) ? a3 : 0;
-      n1 += a1;
-      nf += af;
       n2 += a2;
       n_near += a3;
     }
-    if (pass) {
+    if (inner) {
       MlLine r;
-      r.g = make_float4(lev1 ? C1 - jf : jf, L.a, L.b, L.amp_far);
-      float clamp_val = 0.f;                          // used by level 3 only
-      if (!lev1) clamp_val = L.amp_far * mid_clamped_term(0.f, y2);   // r = 1/MID_Z2 when y2 < MID_Z2
+      r.g = make_float4(jf, L.a, L.b, L.amp_far);
+      const float clamp_val = L.amp_far * mid_clamped_term(0.f, y2);   // r = 1/MID_Z2 when y2 < MID_Z2
       r.h = make_float4(L.y, y2, L.amp, clamp_val);
-      const unsigned lt = (1u << lane) - 1u;
-      if (lev1f) {
-        s1[n1 + offf + __popc(bf & lt)] = r;              // far level-1 lines after the others
-      } else if (lev1) {
-        s1[off1 + __popc(b1 & lt)] = r;
-      } else {
-        const int slot = off2 + __popc(b2 & lt);
-        s2[slot] = r;
-        s_seg_start[slot] = off3 + near_scan - near_n;       // exclusive prefix in slot order
-        s_seg_lo[slot] = (short)near_lo;
-        s_seg_mask[slot] = (unsigned char)l3mask;
-      }
+      const int slot = off2 + __popc(b2 & ((1u << lane) - 1u));
+      s2[slot] = r;
+      s_seg_start[slot] = off3 + near_scan - near_n;         // exclusive prefix in slot order
+      s_seg_lo[slot] = (short)near_lo;
+      s_seg_mask[slot] = (unsigned char)l3mask;
     }
     if (tid == 0) s_seg_start[n2] = n_near;
     __syncthreads();
-    n_pass += (unsigned long long)(n1 + nf + n2);
-
-    // ---- level 1: thread (tid & 15) evaluates its node for lines tid>>4, +16, ...
-    {
-      float a1 = 0.f;
-      const int stride = blockDim.x >> 4;
-      for (int l = tid >> 4; l < n1; l += stride) {
-        const MlLine R = s1[l];
-        const float x = fmaf(xn1 + R.g.x, R.g.y, -R.g.z);     // (node - centre) * s
-        a1 += line_value(x, R);
-      }
-      kahan_add(sum1, comp1, a1);
-      // far lines: thread (tid & 7) evaluates its node for far lines tid>>3, +32, ...
-      float af = 0.f;
-      for (int l = tid >> 3; l < nf; l += (int)(blockDim.x >> 3)) {
-        const MlLine R = s1[n1 + l];
-        const float x = fmaf(xn1f + R.g.x, R.g.y, -R.g.z);
-        af += line_value(x, R);
-      }
-      kahan_add(sumf, compf, af);
-      if (tid == 0) n_nodes += (unsigned long long)n1 * ML_K + (unsigned long long)nf * ML_KF;
-    }
+    n_pass += (unsigned long long)n2;
 
     // ---- per-warp split of the inner lines into level 2 and level 3
     int n2w = 0, n3w = 0, nnw = 0;
@@ -379,31 +542,6 @@ tau_ml_kernel(const LineF32* __restrict__ prep, int n_lines, const int2* __restr
   }
   __syncthreads();
 
-  // ---- level-1 node values: reduce the 16-thread groups, then Chebyshev coefficients
-  s_red[tid] = (double)sum1 - (double)comp1;
-  s_redf[tid] = (double)sumf - (double)compf;
-  __syncthreads();
-  if (tid < ML_K) {
-    double f = 0.0;
-    for (int i = tid; i < (int)blockDim.x; i += ML_K) f += s_red[i];
-    s_red[tid] = f;      // only read back after the barrier below
-  } else if (tid < ML_K + ML_KF) {
-    const int j = tid - ML_K;
-    double f = 0.0;
-    for (int i = j; i < (int)blockDim.x; i += ML_KF) f += s_redf[i];
-    s_redf[j] = f;
-  }
-  __syncthreads();
-  if (tid < ML_K) {
-    double c = 0.0;
-    for (int j = 0; j < ML_K; ++j) c += s_red[j] * cospi((double)tid * (2.0 * j + 1.0) / (2.0 * ML_K));
-    s_c1[tid] = use_l1 ? (float)(c * (2.0 / ML_K)) : 0.f;
-  } else if (tid < ML_K + ML_KF) {
-    const int k = tid - ML_K;
-    double c = 0.0;
-    for (int j = 0; j < ML_KF; ++j) c += s_redf[j] * cospi((double)k * (2.0 * j + 1.0) / (2.0 * ML_KF));
-    s_c1f[k] = use_l1 ? (float)(c * (2.0 / ML_KF)) : 0.f;
-  }
   // ---- level-2 node values of this warp: lanes j and j+16 hold halves of node j
   {
     float f2 = sum2 - comp2;
@@ -419,22 +557,19 @@ tau_ml_kernel(const LineF32* __restrict__ prep, int n_lines, const int2* __restr
 
   const double T = t_layer[row];
   float* out = od + (long long)row * out_stride;   // points [out_first, out_first + out_stride) of the grid
-  float c1[ML_K], c2[ML_K];
+  float c2[ML_K];
 #pragma unroll
-  for (int k = 0; k < ML_K; ++k) { c1[k] = s_c1[k]; c2[k] = s_c2[warp][k]; }
-  const float inv_h1 = use_l1 ? 1.0f / H1 : 0.f, inv_h2 = use_l2 ? 1.0f / H2 : 0.f;
+  for (int k = 0; k < ML_K; ++k) c2[k] = s_c2[warp][k];
+  const float inv_h2 = use_l2 ? 1.0f / H2 : 0.f;
   bool bad = false;
 #pragma unroll
   for (int m = 0; m < P; ++m) {
     const int pl = w0 + lane * P + m;
     if (pl < n_c) {
-      float v = s_core[pl];
-      if (use_l1) {
-        const float t1 = ((float)pl - C1) * inv_h1;
-        v += clenshaw16(c1, t1) + clenshaw16<ML_KF>(s_c1f, t1);
-      }
-      if (use_l2) v += clenshaw16(c2, ((float)pl - C2w) * inv_h2);
       const long long p = c0 + pl;
+      float v = s_core[pl];
+      if (use_l1) v += out[p - out_first];             // level-1 interpolant from tau_far_kernel
+      if (use_l2) v += clenshaw16(c2, ((float)pl - C2w) * inv_h2);
       const double nu = grid_nu(nu_min, step, p);
       const float o = (float)(((double)acc[m] + (double)v) * radiation_term_grid(nu, T));
       bad |= !isfinite(o);
@@ -454,11 +589,26 @@ tau_ml_kernel(const LineF32* __restrict__ prep, int n_lines, const int2* __restr
 
 using namespace lbl;
 
-extern "C" int lbl_tau_tiles_ml_f32(const LineF32* prep, int n_lines, const int* ranges, const double* t_layer,
-                                    int n_rows, double nu_min, double step, long long n_nu, int tile_samples,
-                                    double cutoff, int n_grp, float* od, int* err, unsigned long long* evals,
-                                    unsigned long long* work, int tile_first, int tile_count, int flags,
-                                    void* stream) {
+extern "C" int lbl_ml_inner_ranges(const LineIn* lines, const int* n_kept, double nu_min, double step, long long n_nu,
+                                   int tile_samples, double pad, int n_tiles, int* inner, void* stream) {
+  if (tile_samples < 1 || !(step > 0))
+    return lbl_set_error(LBL_EINVAL, "lbl_ml_inner_ranges: bad arguments");
+  // A line is inner for a chunk of n_c points (half-width H = (n_c - 1) / 2) when its
+  // grid index j0 = rint((nuc - nu_min) / step) lies within H + 1 points of the chunk,
+  // so nuc lies within (H + 1.5) steps of it; chunks lie inside their tile and have at
+  // most min(tile_samples, chunk size) points. Two further steps absorb rounding.
+  const int per_tile = tile_samples < ML_CHUNK ? tile_samples : ML_CHUNK;
+  const int cp = 32 * ((per_tile + ML_WARP_PTS - 1) / ML_WARP_PTS) * ML_P;
+  const int n_c_max = tile_samples < cp ? tile_samples : cp;
+  const double reach = (0.5 * (n_c_max - 1) + 3.5) * step;
+  return lbl_tile_ranges(lines, n_kept, nu_min, step, n_nu, tile_samples, reach, pad, n_tiles, inner, stream);
+}
+
+extern "C" int lbl_tau_tiles_ml_f32(const LineF32* prep, int n_lines, const int* ranges, const int* inner,
+                                    const double* t_layer, int n_rows, double nu_min, double step, long long n_nu,
+                                    int tile_samples, double cutoff, int n_grp, float* od, int* err,
+                                    unsigned long long* evals, unsigned long long* work, int tile_first,
+                                    int tile_count, int flags, void* stream) {
   if (!prep || !ranges || !t_layer || !od || n_lines < 1 || n_rows < 1 || n_rows > 65535 || n_nu < 1 ||
       n_nu > 1500000000LL || tile_samples < 1 || !(step > 0) || !(cutoff >= 0) || n_grp < 1)
     return lbl_set_error(LBL_EINVAL, "lbl_tau_tiles_ml_f32: bad arguments");
@@ -475,15 +625,17 @@ extern "C" int lbl_tau_tiles_ml_f32(const LineF32* prep, int n_lines, const int*
   const long long chunks = (tile_samples + cp - 1) / cp;
   if (n_tiles * chunks > 0x7fffffffLL) return lbl_set_error(LBL_EINVAL, "lbl_tau_tiles_ml_f32: grid too large");
   dim3 grid((unsigned)(n_tiles * chunks), (unsigned)n_rows);
+  cudaStream_t st = (cudaStream_t)stream;
+  tau_far_kernel<<<grid, MF_THREADS, 0, st>>>(prep, n_lines, (const int2*)ranges, nu_min, step, n_nu, tile_samples,
+                                               (int)chunks, cp, cutoff, od, evals, work, tile_first, out_first,
+                                               out_end - out_first);
   if (flags & LBL_DETERMINISTIC)
-    tau_ml_kernel<true><<<grid, threads, 0, (cudaStream_t)stream>>>(prep, n_lines, (const int2*)ranges, t_layer,
-                                                                   nu_min, step, n_nu, tile_samples, (int)chunks,
-                                                                   cutoff, n_grp, od, err, evals, work,
-                                                                   tile_first, out_first, out_end - out_first);
+    tau_ml_kernel<true><<<grid, threads, 0, st>>>(prep, n_lines, (const int2*)ranges, (const int2*)inner, t_layer,
+                                                  nu_min, step, n_nu, tile_samples, (int)chunks, cutoff, n_grp, od,
+                                                  err, evals, work, tile_first, out_first, out_end - out_first);
   else
-    tau_ml_kernel<false><<<grid, threads, 0, (cudaStream_t)stream>>>(prep, n_lines, (const int2*)ranges, t_layer,
-                                                                    nu_min, step, n_nu, tile_samples, (int)chunks,
-                                                                    cutoff, n_grp, od, err, evals, work,
-                                                                    tile_first, out_first, out_end - out_first);
+    tau_ml_kernel<false><<<grid, threads, 0, st>>>(prep, n_lines, (const int2*)ranges, (const int2*)inner, t_layer,
+                                                   nu_min, step, n_nu, tile_samples, (int)chunks, cutoff, n_grp, od,
+                                                   err, evals, work, tile_first, out_first, out_end - out_first);
   return lbl_check_launch("lbl_tau_tiles_ml_f32");
 }

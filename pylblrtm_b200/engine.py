@@ -502,6 +502,10 @@ class Job:
         rec = _lib.SIZEOF_LINE_F32 if single else _lib.SIZEOF_LINE_F64
         prep = torch.empty((n_rows * n_kept * rec // 8,), dtype=torch.float64, device=dev)
         self.last_prep_bytes = n_rows * n_kept * rec          # prepared line records of the summation
+        if precision == "fp32":                               # lines that can be inner lines of a tile's chunks
+            inner = torch.empty_like(ranges)
+            _lib.call("lbl_ml_inner_ranges", lines.data_ptr(), kept.data_ptr(), grid.nu_min, grid.step,
+                      grid.n_nu, grid.tile_samples, self.pad, ranges.shape[0], inner.data_ptr(), stream)
         if timer is not None:
             p0, p1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             p0.record()
@@ -521,9 +525,10 @@ class Job:
                   grid.n_nu, grid.tile_samples, self.cutoff, n_grp, od.data_ptr(), err.data_ptr(),
                   _lib.ptr(evals))
         if precision == "fp32":
-            _lib.call("lbl_tau_tiles_ml_f32", *common,
+            _lib.call("lbl_tau_tiles_ml_f32", common[0], common[1], common[2], inner.data_ptr(), *common[3:],
                       0 if evals is None else evals.data_ptr() + 8, t_first, t_count,
                       _lib.LBL_DETERMINISTIC if deterministic else 0, stream)
+            self.launches += 2
         else:
             _lib.call("lbl_tau_tiles_f32" if single else "lbl_tau_tiles_f64", *common, stream)
         if timer is not None:

@@ -297,3 +297,35 @@ def test_wavenumber_shards_equal_the_full_spectrum(cuda):
         job.run("fp32", tiles=(3, 2))
     with pytest.raises(ValueError, match="tiles needs"):
         job.run("fp64", tiles=(0, 1))
+
+
+@pytest.mark.parametrize("tile,step", [(2.0, 0.001), (5.0, 0.001), (0.05, 0.001), (0.3, 0.0025)])
+def test_inner_ranges_select_every_inner_line(cuda, tile, step, monkeypatch):
+    """The multi-level sum with the per-tile inner-line ranges does exactly the work of
+    the same sum scanning every candidate line of the tile (inner = NULL): equal
+    reference-rule evaluation counts and equal level-2 / level-3 / near-zone counts, so
+    no inner line is lost, and optical depths equal to float rounding (the scans group
+    lines into different 256-line rounds). Pressure shifts are 40x the synthetic ones;
+    tiles of one chunk, three chunks, and tiles too small for level 1."""
+    sd = synthetic.restrict(synthetic.three_gas_lines(20000, 1490.0, 1520.0, seed=4), 1490.0, 1520.0)
+    lines = {k: v.copy() for k, v in sd.lines.items()}
+    lines["shift"] = lines["shift"] * 40.0
+    sd = SpectralData(lines, dict(sd.tips), dict(sd.molar_masses), sd.molecule)
+    lv = synthetic.perturbed_levels(synthetic.logp_levels(7), 2, seed=8)
+    gases = ["H2O", "CO2", "O3"]
+    li = engine.LayerInput(gases=gases, levels_p=lv["p"], levels_t=lv["t"],
+                           levels_vmr=np.stack([lv[g] for g in gases], axis=1))
+    job = engine.Job(sd, li, engine.make_grid(1500.0, 1510.3, step, tile), 5.0)
+    with_inner = job.run("fp32", deterministic=True, count_evals=True)
+    real_call = _lib.call
+
+    def no_inner(name, *args):
+        if name == "lbl_tau_tiles_ml_f32":
+            args = args[:3] + (0,) + args[4:]
+        return real_call(name, *args)
+
+    monkeypatch.setattr(_lib, "call", no_inner)
+    scan_all = job.run("fp32", deterministic=True, count_evals=True)
+    assert with_inner.evals == scan_all.evals and with_inner.work_split == scan_all.work_split
+    rel = ((with_inner.od - scan_all.od).abs() / scan_all.od.abs().clamp_min(1e-30)).max().item()
+    assert rel <= 2e-6, rel
