@@ -168,7 +168,7 @@ int lbl_ml_inner_ranges(const LineIn* lines, const int* n_kept, double nu_min, d
  * default float32 engine): per CTA chunk (<= 2048 points of one reference
  * tile), lines farther than a chunk half-width contribute through 16 Chebyshev
  * nodes over the chunk (8 beyond six half-widths; a line-per-thread kernel that
- * writes its interpolant into od first), the remaining lines farther than a
+ * runs first and hands the chunk's coefficients over through od), the remaining lines farther than a
  * 256-point sub-chunk half-width through 16 nodes over that sub-chunk, the rest
  * directly. inner (nullable; from lbl_ml_inner_ranges with the ranges' lines
  * and pad) limits the second kernel to the lines that can be inner; NULL scans

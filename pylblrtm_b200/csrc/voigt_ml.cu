@@ -93,8 +93,9 @@ __device__ __forceinline__ float clenshaw16(const float* c, float t) {
 // Level 1 as its own kernel. Nine in ten lines of a chunk's window are level-1
 // lines; each contributes only through the chunk's Chebyshev nodes, so one thread
 // takes one line and evaluates it at all nodes from registers (no shared-memory
-// staging, no barriers). The kernel writes the level-1 interpolant of every chunk
-// point into od, where tau_ml_kernel adds the inner lines and applies R(nu, T).
+// staging, no barriers). The kernel leaves the chunk's 16 + 8 Chebyshev coefficients
+// in the first 24 floats of the chunk's own od slice (level 1 needs >= 65 points);
+// tau_ml_kernel reads them before it writes the slice.
 constexpr int MF_THREADS = 256;                // lines per round
 constexpr int MF_FLUSH = 8;                    // rounds summed in float before the double sums
 
@@ -265,18 +266,7 @@ tau_far_kernel(const LineF32* __restrict__ prep, int n_lines, const int2* __rest
       c += s_part[0][ML_K + j] * cospi((double)k * (2.0 * j + 1.0) / (2.0 * ML_KF));
     s_coef[tid] = (float)(c * (2.0 / ML_KF));
   }
-  __syncthreads();
-  float c1[ML_K], cf[ML_KF];
-#pragma unroll
-  for (int k = 0; k < ML_K; ++k) c1[k] = s_coef[k];
-#pragma unroll
-  for (int k = 0; k < ML_KF; ++k) cf[k] = s_coef[ML_K + k];
-  const float inv_h1 = 1.0f / H1;
-  float* out = od + (long long)row * out_stride + (c0 - out_first);
-  for (int p = tid; p < n_c; p += MF_THREADS) {
-    const float t = ((float)p - C1) * inv_h1;
-    out[p] = clenshaw16(c1, t) + clenshaw16<ML_KF>(cf, t);
-  }
+  if (tid < ML_K + ML_KF) od[(long long)row * out_stride + (c0 - out_first) + tid] = s_coef[tid];
   if (tid == 0) {
     const unsigned long long a = s_cnt[0], b = s_cnt[1];
     if (evals && a + b) atomicAdd(evals, (a + b) * (unsigned long long)n_c);
@@ -302,6 +292,7 @@ tau_ml_kernel(const LineF32* __restrict__ prep, int n_lines, const int2* __restr
   __shared__ unsigned char s_seg_mask[ML_THREADS];  // warps treating the inner line directly (level 3)
   __shared__ float s_core[ML_CHUNK];               // near-zone corrections (each point owned by one thread)
   __shared__ float s_nbuf[ML_NB];                   // near-item values of one batch
+  __shared__ float s_c1[ML_K + ML_KF];              // level-1 coefficients from tau_far_kernel
   __shared__ float s_c2[ML_THREADS / 32][ML_K];
 
   const int row = blockIdx.y;
@@ -337,6 +328,8 @@ tau_ml_kernel(const LineF32* __restrict__ prep, int n_lines, const int2* __restr
   const float pf = (float)(w0 + lane * P);                   // this lane's first point
 
   for (int i = tid; i < ML_CHUNK; i += blockDim.x) s_core[i] = 0.f;
+  // read before the first barrier; this CTA writes the slice only after the last one
+  if (use_l1 && tid < ML_K + ML_KF) s_c1[tid] = od[(long long)row * out_stride + (c0 - out_first) + tid];
 
   // level-3 sums hold only the lines within ~2 sub-chunk widths (tens of terms), so
   // plain float accumulation suffices; the long node sums use Kahan compensation.
@@ -560,7 +553,7 @@ tau_ml_kernel(const LineF32* __restrict__ prep, int n_lines, const int2* __restr
   float c2[ML_K];
 #pragma unroll
   for (int k = 0; k < ML_K; ++k) c2[k] = s_c2[warp][k];
-  const float inv_h2 = use_l2 ? 1.0f / H2 : 0.f;
+  const float inv_h1 = use_l1 ? 1.0f / H1 : 0.f, inv_h2 = use_l2 ? 1.0f / H2 : 0.f;
   bool bad = false;
 #pragma unroll
   for (int m = 0; m < P; ++m) {
@@ -568,7 +561,10 @@ tau_ml_kernel(const LineF32* __restrict__ prep, int n_lines, const int2* __restr
     if (pl < n_c) {
       const long long p = c0 + pl;
       float v = s_core[pl];
-      if (use_l1) v += out[p - out_first];             // level-1 interpolant from tau_far_kernel
+      if (use_l1) {
+        const float t1 = ((float)pl - C1) * inv_h1;
+        v += clenshaw16(s_c1, t1) + clenshaw16<ML_KF>(s_c1 + ML_K, t1);
+      }
       if (use_l2) v += clenshaw16(c2, ((float)pl - C2w) * inv_h2);
       const double nu = grid_nu(nu_min, step, p);
       const float o = (float)(((double)acc[m] + (double)v) * radiation_term_grid(nu, T));
