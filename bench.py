@@ -40,7 +40,7 @@ FLOPS_PER_EVAL_FAR = 12      # two-term far-wing form: 5 FFMA + 1 FMUL + 1 RCP (
 FLOPS_NODE = 12              # Chebyshev-node evaluation (two-term form)
 FLOPS_L3 = 38                # level-3 loop evaluation (clamped five-term form)
 FLOPS_NEAR = 60              # near-zone point (float continued fraction / float64 rational, average)
-FLOPS_CHEB_PER_POINT = 128   # two 16-term Clenshaw sums per point and layer
+FLOPS_CHEB_PER_POINT = 144   # 16 + 8 Clenshaw terms for each of levels 1 and 2 (3 flops a term)
 CPU_SAMPLE = (1000.0, 1000.5)  # sub-window timed on the host (all 60 layers)
 
 

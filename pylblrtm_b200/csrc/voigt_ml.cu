@@ -13,7 +13,8 @@
 //           six half-widths out use 8 nodes). A separate kernel (tau_far_kernel)
 //           computes this level and writes its interpolant into od;
 //  level 2  the other lines farther than one sub-chunk half-width from a warp's
-//           256-point sub-chunk: 16 Chebyshev nodes per sub-chunk, same geometry;
+//           256-point sub-chunk: 16 Chebyshev nodes per sub-chunk, same geometry
+//           (8 beyond six sub-chunk half-widths);
 //  level 3  the remaining lines: direct evaluation at every point. The warp's
 //           loop is branch-free: it evaluates the five-term asymptotic form with
 //           |z|^2 clamped to >= MID_Z2 = 64, so every point inside a line's near
@@ -294,6 +295,7 @@ tau_ml_kernel(const LineF32* __restrict__ prep, int n_lines, const int2* __restr
   __shared__ float s_nbuf[ML_NB];                   // near-item values of one batch
   __shared__ float s_c1[ML_K + ML_KF];              // level-1 coefficients from tau_far_kernel
   __shared__ float s_c2[ML_THREADS / 32][ML_K];
+  __shared__ float s_c2f[ML_THREADS / 32][ML_KF];
 
   const int row = blockIdx.y;
   const int tile = tile_first + (int)(blockIdx.x / chunks_per_tile), chunk = blockIdx.x % chunks_per_tile;
@@ -323,8 +325,9 @@ tau_ml_kernel(const LineF32* __restrict__ prep, int n_lines, const int2* __restr
   const int n_w = max(0, min(ML_WARP_PTS, n_c - w0));
   const float H2 = 0.5f * (float)(n_w - 1), C2w = (float)w0 + H2;
   const bool use_l2 = H2 >= ML_MIN_H2;
-  // level-2 Chebyshev node owned by this lane: (lane & 15)
+  // level-2 Chebyshev nodes owned by this lane: (lane & 15), and (lane & 7) of the 8-node set
   const float xn2 = H2 * (float)cospi((2.0 * (lane & 15) + 1.0) / (2.0 * ML_K));
+  const float xn2f = H2 * (float)cospi((2.0 * (lane & 7) + 1.0) / (2.0 * ML_KF));
   const float pf = (float)(w0 + lane * P);                   // this lane's first point
 
   for (int i = tid; i < ML_CHUNK; i += blockDim.x) s_core[i] = 0.f;
@@ -336,7 +339,7 @@ tau_ml_kernel(const LineF32* __restrict__ prep, int n_lines, const int2* __restr
   float acc[P];
 #pragma unroll
   for (int m = 0; m < P; ++m) acc[m] = 0.f;
-  float sum2 = 0.f, comp2 = 0.f;
+  float sum2 = 0.f, comp2 = 0.f, sum2f = 0.f;
   unsigned long long n_pass = 0, n_nodes = 0, n_l3 = 0, n_near_items = 0;
 
   // register prefetch of the next round's line records
@@ -410,25 +413,31 @@ tau_ml_kernel(const LineF32* __restrict__ prep, int n_lines, const int2* __restr
     __syncthreads();
     n_pass += (unsigned long long)n2;
 
-    // ---- per-warp split of the inner lines into level 2 and level 3
-    int n2w = 0, n3w = 0, nnw = 0;
+    // ---- per-warp split of the inner lines into level 2 (16 nodes; 8 beyond six
+    // sub-chunk half-widths, listed from the back of s_l2) and level 3
+    int n2w = 0, n2fw = 0, n3w = 0, nnw = 0;
     for (int k = 0; k < n2; k += 32) {
       const int l = k + lane;
-      bool is2 = false, is3 = false, nz = false;
+      bool is2 = false, is2f = false, is3 = false, nz = false;
       if (l < n2) {
         const float d = fabsf(s2[l].g.x - C2w) - H2;
-        is2 = use_l2 && d > H2 + 1.f;
-        is3 = !is2 && n_w > 0;
+        const bool lev2 = use_l2 && d > H2 + 1.f;
+        is2f = lev2 && d > ML_FAR1 * H2;
+        is2 = lev2 && !is2f;
+        is3 = !lev2 && n_w > 0;
         if constexpr (DET) {   // near points of slot l inside this warp's sub-chunk (level 3 here)
           const int st = s_seg_start[l], len = s_seg_start[l + 1] - st, lo = s_seg_lo[l];
           nz = len > 0 && ((s_seg_mask[l] >> warp) & 1u) && lo < w0 + n_w && lo + len > w0;
         }
       }
       const unsigned q2 = __ballot_sync(0xffffffffu, is2), q3 = __ballot_sync(0xffffffffu, is3);
+      const unsigned q2f = __ballot_sync(0xffffffffu, is2f);
       const unsigned lt = (1u << lane) - 1u;
       if (is2) s_l2[warp][n2w + __popc(q2 & lt)] = (unsigned char)l;
+      if (is2f) s_l2[warp][ML_THREADS - 1 - (n2fw + __popc(q2f & lt))] = (unsigned char)l;
       if (is3) s_l3[warp][n3w + __popc(q3 & lt)] = (unsigned char)l;
       n2w += __popc(q2);
+      n2fw += __popc(q2f);
       n3w += __popc(q3);
       if constexpr (DET) {
         const unsigned qn = __ballot_sync(0xffffffffu, nz);
@@ -448,7 +457,13 @@ tau_ml_kernel(const LineF32* __restrict__ prep, int n_lines, const int2* __restr
         a2 += line_value(x, R);
       }
       kahan_add(sum2, comp2, a2);
-      if (lane == 0) n_nodes += (unsigned long long)n2w * ML_K;
+      // far level-2 lines: quarter-warps take one line each, lane (& 7) = node
+      for (int i = lane >> 3; i < n2fw; i += 4) {
+        const MlLine R = s2[s_l2[warp][ML_THREADS - 1 - i]];
+        const float x = fmaf(xn2f + (C2w - R.g.x), R.g.y, -R.g.z);
+        sum2f += line_value(x, R);
+      }
+      if (lane == 0) n_nodes += (unsigned long long)n2w * ML_K + (unsigned long long)n2fw * ML_KF;
     }
 
     // ---- level 3, far part: every point of the warp, |z|^2 clamped (branch-free)
@@ -545,6 +560,16 @@ tau_ml_kernel(const LineF32* __restrict__ prep, int n_lines, const int2* __restr
       c += (double)fj * cospi((double)(lane & 15) * (2.0 * j + 1.0) / (2.0 * ML_K));
     }
     if (lane < ML_K) s_c2[warp][lane] = use_l2 ? (float)(c * (2.0 / ML_K)) : 0.f;
+    // 8-node set: lanes j, j+8, j+16, j+24 hold quarters of node j
+    float g2 = sum2f;
+    g2 += __shfl_xor_sync(0xffffffffu, g2, 16);
+    g2 += __shfl_xor_sync(0xffffffffu, g2, 8);
+    double cf = 0.0;
+    for (int j = 0; j < ML_KF; ++j) {
+      const float gj = __shfl_sync(0xffffffffu, g2, j);
+      cf += (double)gj * cospi((double)(lane & 7) * (2.0 * j + 1.0) / (2.0 * ML_KF));
+    }
+    if (lane < ML_KF) s_c2f[warp][lane] = use_l2 ? (float)(cf * (2.0 / ML_KF)) : 0.f;
   }
   __syncthreads();
 
@@ -565,7 +590,10 @@ tau_ml_kernel(const LineF32* __restrict__ prep, int n_lines, const int2* __restr
         const float t1 = ((float)pl - C1) * inv_h1;
         v += clenshaw16(s_c1, t1) + clenshaw16<ML_KF>(s_c1 + ML_K, t1);
       }
-      if (use_l2) v += clenshaw16(c2, ((float)pl - C2w) * inv_h2);
+      if (use_l2) {
+        const float t2 = ((float)pl - C2w) * inv_h2;
+        v += clenshaw16(c2, t2) + clenshaw16<ML_KF>(s_c2f[warp], t2);
+      }
       const double nu = grid_nu(nu_min, step, p);
       const float o = (float)(((double)acc[m] + (double)v) * radiation_term_grid(nu, T));
       bad |= !isfinite(o);
