@@ -13,6 +13,15 @@ void lbl_host_faddeeva_f64(const double* x, const double* y, long long n, double
   }
 }
 
+// Re w by Weideman's approximation with the 36-term set (terms = 36) or the 28-term
+// set of the float32 multi-level engine's near zone (terms = 28).
+int lbl_host_weideman_re(const double* x, const double* y, long long n, int terms, double* re) {
+  if (terms != 36 && terms != 28) return -1;
+  for (long long i = 0; i < n; ++i)
+    re[i] = terms == 36 ? lbl::weideman_re(x[i], y[i]) : lbl::weideman_re_f32(x[i], y[i]);
+  return 0;
+}
+
 void lbl_host_faddeeva_f32(const float* x, const float* y, long long n, float* re, float* im, int mode) {
   for (long long i = 0; i < n; ++i) {
     if (mode == 1) {

@@ -7,14 +7,18 @@ Numer. Anal. 31(5):1497-1518: for Im z >= 0,
     Z = (L + iz) / (L - iz),  L = (N / sqrt(2))^(1/2),
 
 where a_n are the Fourier coefficients of (L^2 + t^2) exp(-t^2) under the map
-t = L tan(theta/2), obtained here by an FFT on 4N points. Run:
+t = L tan(theta/2), obtained here by an FFT on 4N points. Two sets: N = 36 (|w|
+relative error <= 2e-14 for |z| <= 6; the float64 engine and the Jacobians) and
+N = 28 (the float32 multi-level engine's near zone: Re w relative error <= 7e-7
+for y >= 1e-4 and <= 1e-8 for y >= 0.01 inside |z|^2 < 36, against
+scipy.special.wofz; float32 rounding of the sums is ~1e-7). Run:
 
     python pylblrtm_b200/csrc/gen_weideman.py > pylblrtm_b200/csrc/weideman_coeffs.h
 """
 
 import numpy as np
 
-N = 36
+SETS = (("LBL_WEIDEMAN", 36), ("LBL_WEIDEMAN28", 28))
 
 
 def coefficients(n: int):
@@ -28,16 +32,17 @@ def coefficients(n: int):
 
 
 def main():
-    big_l, a = coefficients(N)
     print("// Generated by gen_weideman.py: Weideman (1994) rational approximation of w(z).")
     print("#pragma once")
-    print(f"#define LBL_WEIDEMAN_N {N}")
-    print(f"#define LBL_WEIDEMAN_L {float(big_l)!r}")
-    print("// a_1 .. a_N (polynomial in Z: sum a_n Z^(n-1)), as an initializer list")
-    print("#define LBL_WEIDEMAN_COEFFS \\")
-    for i in range(0, N, 3):
-        tail = ", \\" if i + 3 < N else ""
-        print("    " + ", ".join(repr(float(v)) for v in a[i:i + 3]) + tail)
+    for name, n in SETS:
+        big_l, a = coefficients(n)
+        print(f"#define {name}_N {n}")
+        print(f"#define {name}_L {float(big_l)!r}")
+        print("// a_1 .. a_N (polynomial in Z: sum a_n Z^(n-1)), as an initializer list")
+        print(f"#define {name}_COEFFS \\")
+        for i in range(0, n, 3):
+            tail = ", \\" if i + 3 < n else ""
+            print("    " + ", ".join(repr(float(v)) for v in a[i:i + 3]) + tail)
 
 
 if __name__ == "__main__":

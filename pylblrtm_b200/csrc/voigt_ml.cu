@@ -59,7 +59,7 @@ __device__ __forceinline__ float line_value(float x, const MlLine& L) {
     return L.g.w * r * fmaf(fmaf(-2.0f * L.h.y, r, 1.5f), r, 1.0f);
   }
   if (z2 >= CORE_Z2 && L.h.x >= 0.f) return L.h.z * re_w_f32_mid(x, L.h.x, L.h.y, z2);
-  return (float)((double)L.h.z * weideman_re((double)x, (double)L.h.x));
+  return (float)((double)L.h.z * weideman_re_f32((double)x, (double)L.h.x));
 }
 
 // Five-term asymptotic form with |z|^2 clamped to >= MID_Z2 (the level-3 loop
@@ -126,7 +126,7 @@ static __device__ __noinline__ float far_node_general(float x, float y, float y2
     return amp_far * r * fmaf(fmaf(-2.0f * y2, r, 1.5f), r, 1.0f);
   }
   if (z2 >= CORE_Z2 && y >= 0.f) return amp * re_w_f32_mid(x, y, y2, z2);
-  return (float)((double)amp * weideman_re((double)x, (double)y));
+  return (float)((double)amp * weideman_re_f32((double)x, (double)y));
 }
 
 // Node sums of one level-1 line: nodes k and K-1-k sit at +xs[k] and -xs[k] from the chunk centre.
@@ -497,7 +497,7 @@ tau_ml_kernel(const LineF32* __restrict__ prep, int n_lines, const int2* __restr
         if (z2 >= MID_Z2) continue;
         float v;
         if (z2 >= CORE_Z2 && R.h.x >= 0.f) v = R.h.z * re_w_cf32(x, R.h.x, z2);
-        else v = (float)((double)R.h.z * weideman_re((double)x, (double)R.h.x));
+        else v = (float)((double)R.h.z * weideman_re_f32((double)x, (double)R.h.x));
         atomicAdd(&s_core[p], v - R.h.w);
       }
     } else {
@@ -525,7 +525,7 @@ tau_ml_kernel(const LineF32* __restrict__ prep, int n_lines, const int2* __restr
             const float z2 = fmaf(x, x, R.h.y);
             if (z2 < MID_Z2) {
               if (z2 >= CORE_Z2 && R.h.x >= 0.f) v = R.h.z * re_w_cf32(x, R.h.x, z2);
-              else v = (float)((double)R.h.z * weideman_re((double)x, (double)R.h.x));
+              else v = (float)((double)R.h.z * weideman_re_f32((double)x, (double)R.h.x));
               v -= R.h.w;
             }
           }

@@ -77,3 +77,27 @@ def test_f32_engine_real_part(host):
     re, _ = f32(x32, y32, 1)
     e = np.abs(re - ref) / np.abs(ref)
     assert np.max(e[y32 > 1e-4]) < 2e-6, np.max(e[y32 > 1e-4])
+
+
+def test_weideman_coefficient_sets():
+    """Both Weideman sets of weideman_coeffs.h inside |z|^2 < 36 (where the engines use
+    them) against wofz: the 36-term set to 2e-14 of |w|, the float32 engine's 28-term set
+    to 7e-7 of Re w for y >= 1e-4 and 1e-8 of Re w for y >= 0.01."""
+    lib = ctypes.CDLL(LIB)
+    P = ctypes.c_void_p
+    lib.lbl_host_weideman_re.argtypes = [P, P, ctypes.c_longlong, ctypes.c_int, P]
+    x1 = np.linspace(-6, 6, 1201)
+    for ymin, bound28 in ((1e-4, 7e-7), (1e-2, 1e-8)):
+        X, Y = np.meshgrid(x1, np.geomspace(ymin, 6, 120))
+        m = X ** 2 + Y ** 2 < 36
+        x, y = np.ascontiguousarray(X[m]), np.ascontiguousarray(Y[m])
+        ref = wofz(x + 1j * y)
+        for terms in (36, 28):
+            re = np.empty_like(x)
+            assert lib.lbl_host_weideman_re(x.ctypes.data, y.ctypes.data, x.size, terms, re.ctypes.data) == 0
+            rel = np.max(np.abs(re - ref.real) / np.abs(ref.real))
+            if terms == 28:
+                assert rel <= bound28, (ymin, rel)
+            else:
+                assert np.max(np.abs(re - ref.real) / np.abs(ref)) <= 2e-14
+    assert lib.lbl_host_weideman_re(x.ctypes.data, y.ctypes.data, 1, 30, re.ctypes.data) == -1
