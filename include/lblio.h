@@ -46,6 +46,11 @@ int lbl_line_pairs(const int* mol, const int* iso, const double* nu0, const doub
                    double lo_edge, double hi_edge, double p_max, int max_pairs, int* pair_mol, int* pair_iso,
                    long long* pair_band, int* n_pairs, int* pair_index, double* max_abs_shift);
 
+/* out[i] = lut[index[i]] for i < n (the group index of every line from its pair index
+ * and the pair -> group table of the group selection); LBL_EINVAL for an index outside
+ * [0, n_lut). */
+int lbl_map_index(const int* index, long long n, const int* lut, int n_lut, int* out);
+
 #ifdef __cplusplus
 }
 #endif

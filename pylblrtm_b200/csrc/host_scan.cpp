@@ -48,3 +48,15 @@ extern "C" int lbl_line_pairs(const int* mol, const int* iso, const double* nu0,
   *max_abs_shift = smax;
   return LBL_OK;
 }
+
+extern "C" int lbl_map_index(const int* index, long long n, const int* lut, int n_lut, int* out) {
+  if (n < 0 || n_lut < 0 || (n > 0 && (!index || !lut || !out))) return LBL_EINVAL;
+  unsigned bad = 0;
+  for (long long i = 0; i < n; ++i) {
+    const int k = index[i];
+    const bool ok = k >= 0 && k < n_lut;
+    bad |= !ok;
+    out[i] = lut[ok ? k : 0];
+  }
+  return bad ? LBL_EINVAL : LBL_OK;
+}

@@ -198,7 +198,8 @@ def select_groups(sd: SpectralData, profile_gases: Sequence[str], nu_first: floa
         lut = np.full(k, -1, dtype=np.int32)
         for j, g in lut_pairs.items():
             lut[j] = g
-        gid = lut[pair_index]
+        if host.lbl_map_index(pair_index.ctypes.data, n, lut.ctypes.data, k, gid.ctypes.data) != 0:
+            raise RuntimeError("lbl_map_index: pair index out of range")
     return groups, gid
 
 
@@ -458,12 +459,15 @@ class Job:
         od_dtype = torch.float32 if single else torch.float64
         self.launches = 0
 
+        # view cosines go up before any device stage: a pageable copy queued behind the
+        # summation would hold the host until the summation ends
+        mu_d = None
+        if want_tau or want_trans or channels is not None:
+            mu_d = torch.as_tensor(np.broadcast_to(np.asarray(1.0 if mu is None else mu, np.float64),
+                                                   (n_prof,)).copy()).to(dev)
+
         def finish(od):
             res.od = od if want_od else None
-            mu_d = None
-            if want_tau or want_trans or channels is not None:
-                mu_d = torch.as_tensor(np.broadcast_to(np.asarray(1.0 if mu is None else mu, np.float64),
-                                                       (n_prof,)).copy()).to(dev)
             if channels is not None:
                 width, n_ch = channels
                 out = torch.empty((n_prof, n_ch), dtype=torch.float64, device=dev)

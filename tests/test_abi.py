@@ -123,6 +123,19 @@ def test_line_pairs_scan_rejects_bad_arguments():
     assert n.value == 2 and list(idx) == [0, 1] and list(pb[:2]) == [1, 1] and smax.value == 0.003
 
 
+def test_map_index():
+    import numpy as np
+    host = _lib.load_host()
+    idx = np.array([2, 0, 1, 2, 0], np.int32)
+    lut = np.array([-1, 5, 7], np.int32)
+    out = np.zeros(5, np.int32)
+    assert host.lbl_map_index(idx.ctypes.data, 5, lut.ctypes.data, 3, out.ctypes.data) == 0
+    assert list(out) == [7, -1, 5, 7, -1]
+    bad = np.array([0, 3], np.int32)
+    assert host.lbl_map_index(bad.ctypes.data, 2, lut.ctypes.data, 3, out.ctypes.data) != 0
+    assert host.lbl_map_index(idx.ctypes.data, 0, None, 0, None) == 0
+
+
 def _declared_arities(header):
     """Parameter count of every lbl_* function declared in a header."""
     text = re.sub(r"/\*.*?\*/", "", open(header).read(), flags=re.S)
