@@ -29,6 +29,7 @@
 // level-1 lines among them.
 #include <math.h>
 
+#include "cheb_tables.h"
 #include "faddeeva.cuh"
 #include "lbl_common.cuh"
 #include "sum_common.cuh"
@@ -45,6 +46,13 @@ constexpr float ML_FAR1 = 5.f;                 // "far": more than (1 + ML_FAR1)
 constexpr float ML_MIN_H1 = 32.f;              // smallest chunk half-width (points) using level 1
 constexpr float ML_MIN_H2 = 16.f;              // smallest sub-chunk half-width using level 2
 constexpr int ML_NB = 2048;                    // near items buffered per batch
+
+// Chebyshev node offsets (fractions of the half-width) and DCT weights, row-major [k][j]
+static __constant__ float c_node16[ML_K] = {LBL_CHEB16_NODES};
+static __constant__ float c_node8[ML_KF] = {LBL_CHEB8_NODES};
+static __constant__ double c_dct16[ML_K * ML_K] = {LBL_DCT16};
+static __constant__ double c_dct8[ML_KF * ML_KF] = {LBL_DCT8};
+static_assert(ML_K == 16 && ML_KF == 8, "tables of cheb_tables.h");
 
 struct MlLine {
   float4 g;   // jf (centre index relative to the chunk start), a, b, amp_far
@@ -100,15 +108,18 @@ __device__ __forceinline__ float clenshaw16(const float* c, float t) {
 constexpr int MF_THREADS = 256;                // lines per round
 constexpr int MF_FLUSH = 8;                    // rounds summed in float before the double sums
 
-__device__ __forceinline__ LineF32 load_line(const LineF32* p) {
-  union {
-    float4 v[2];
-    LineF32 l;
-  } u;
-  const float4* q = reinterpret_cast<const float4*>(p);   // records are 32 B in a cudaMalloc'd array
-  u.v[0] = __ldg(q);
-  u.v[1] = __ldg(q + 1);
-  return u.l;
+constexpr int MF_STAGES = 3;                   // rounds of line records in flight per thread
+
+// Asynchronous 16-byte global -> shared copies (cp.async, L2 only); each thread copies
+// and later reads only its own slots, so its own wait_group orders them.
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
 }
 
 // amp * Re w by the far-wing form (amp_far = amp y / sqrt(pi)), added to f (|z|^2 >= FAR_Z2, y >= 0).
@@ -154,6 +165,7 @@ tau_far_kernel(const LineF32* __restrict__ prep, int n_lines, const int2* __rest
                double step, long long n_nu, int tile_samples, int chunks_per_tile, int chunk_pts, double cutoff,
                float* __restrict__ od, unsigned long long* evals, unsigned long long* work, int tile_first,
                long long out_first, long long out_stride) {
+  __shared__ __align__(16) LineF32 s_line[MF_STAGES][MF_THREADS];   // records are 32 B, 16-B aligned
   __shared__ double s_part[MF_THREADS / 32][ML_K + ML_KF];
   __shared__ float s_coef[ML_K + ML_KF];
   __shared__ unsigned s_cnt[2];
@@ -177,9 +189,9 @@ tau_far_kernel(const LineF32* __restrict__ prep, int n_lines, const int2* __rest
 
   float xa[ML_K / 2], xb[ML_KF / 2];                      // node offsets, as tau_ml_kernel places them
 #pragma unroll
-  for (int k = 0; k < ML_K / 2; ++k) xa[k] = H1 * (float)cospi((2.0 * k + 1.0) / (2.0 * ML_K));
+  for (int k = 0; k < ML_K / 2; ++k) xa[k] = H1 * c_node16[k];
 #pragma unroll
-  for (int k = 0; k < ML_KF / 2; ++k) xb[k] = H1 * (float)cospi((2.0 * k + 1.0) / (2.0 * ML_KF));
+  for (int k = 0; k < ML_KF / 2; ++k) xb[k] = H1 * c_node8[k];
 
   float f1[ML_K], ff[ML_KF];
   double d1[ML_K], df[ML_KF];
@@ -189,13 +201,30 @@ tau_far_kernel(const LineF32* __restrict__ prep, int n_lines, const int2* __rest
   for (int k = 0; k < ML_KF; ++k) { ff[k] = 0.f; df[k] = 0.0; }
   unsigned n1 = 0, nf = 0;
 
-  LineF32 nxt;
-  if (rng.x + tid < rng.y) nxt = load_line(lp + rng.x + tid);
-  int rounds = 0;
-  for (int base = rng.x; base < rng.y; base += MF_THREADS) {
-    const LineF32 L = nxt;
-    const bool have = base + tid < rng.y;
-    if (base + MF_THREADS + tid < rng.y) nxt = load_line(lp + base + MF_THREADS + tid);
+  // line records of round r (line rng.x + r * MF_THREADS + tid) go to stage r % MF_STAGES,
+  // MF_STAGES - 1 rounds ahead; every round commits one group (empty past the end), so
+  // waiting for all but the newest MF_STAGES - 1 groups completes the current round's copy
+  const int n_rounds = rng.y > rng.x ? (rng.y - rng.x + MF_THREADS - 1) / MF_THREADS : 0;
+  auto issue = [&](int r, int stage) {
+    const int li = rng.x + r * MF_THREADS + tid;
+    if (li < rng.y) {   // prep records: 32 B each in a 256-B aligned allocation
+      const float4* g = reinterpret_cast<const float4*>(lp + li);
+      float4* d = reinterpret_cast<float4*>(&s_line[stage][tid]);
+      cp_async16(d, g);
+      cp_async16(d + 1, g + 1);
+    }
+    cp_async_commit();
+  };
+#pragma unroll
+  for (int r = 0; r < MF_STAGES - 1; ++r) issue(r, r);
+  int rounds = 0, stage = 0;
+  for (int r = 0; r < n_rounds; ++r) {
+    issue(r + MF_STAGES - 1, stage == 0 ? MF_STAGES - 1 : stage - 1);   // the stage read last round
+    cp_async_wait<MF_STAGES - 1>();
+    const bool have = rng.x + r * MF_THREADS + tid < rng.y;
+    LineF32 L;
+    if (have) L = s_line[stage][tid];
+    stage = stage + 1 == MF_STAGES ? 0 : stage + 1;
     // the level-1 test of tau_ml_kernel, expression for expression
     const bool pass = have && (L.nuc >= wlo) && (L.nuc <= whi);
     const float jf = (float)(L.j0 - c0i);
@@ -222,6 +251,7 @@ tau_far_kernel(const LineF32* __restrict__ prep, int n_lines, const int2* __rest
       for (int k = 0; k < ML_KF; ++k) { df[k] += (double)ff[k]; ff[k] = 0.f; }
     }
   }
+  cp_async_wait<0>();                                      // only empty groups remain
 #pragma unroll
   for (int k = 0; k < ML_K; ++k) d1[k] += (double)f1[k];
 #pragma unroll
@@ -258,13 +288,13 @@ tau_far_kernel(const LineF32* __restrict__ prep, int n_lines, const int2* __rest
   // Chebyshev coefficients (DCT of the node values)
   if (tid < ML_K) {
     double c = 0.0;
-    for (int j = 0; j < ML_K; ++j) c += s_part[0][j] * cospi((double)tid * (2.0 * j + 1.0) / (2.0 * ML_K));
+    for (int j = 0; j < ML_K; ++j) c += s_part[0][j] * c_dct16[tid * ML_K + j];
     s_coef[tid] = (float)(c * (2.0 / ML_K));
   } else if (tid < ML_K + ML_KF) {
     const int k = tid - ML_K;
     double c = 0.0;
     for (int j = 0; j < ML_KF; ++j)
-      c += s_part[0][ML_K + j] * cospi((double)k * (2.0 * j + 1.0) / (2.0 * ML_KF));
+      c += s_part[0][ML_K + j] * c_dct8[k * ML_KF + j];
     s_coef[tid] = (float)(c * (2.0 / ML_KF));
   }
   if (tid < ML_K + ML_KF) od[(long long)row * out_stride + (c0 - out_first) + tid] = s_coef[tid];
@@ -326,8 +356,8 @@ tau_ml_kernel(const LineF32* __restrict__ prep, int n_lines, const int2* __restr
   const float H2 = 0.5f * (float)(n_w - 1), C2w = (float)w0 + H2;
   const bool use_l2 = H2 >= ML_MIN_H2;
   // level-2 Chebyshev nodes owned by this lane: (lane & 15), and (lane & 7) of the 8-node set
-  const float xn2 = H2 * (float)cospi((2.0 * (lane & 15) + 1.0) / (2.0 * ML_K));
-  const float xn2f = H2 * (float)cospi((2.0 * (lane & 7) + 1.0) / (2.0 * ML_KF));
+  const float xn2 = H2 * c_node16[lane & 15];
+  const float xn2f = H2 * c_node8[lane & 7];
   const float pf = (float)(w0 + lane * P);                   // this lane's first point
 
   for (int i = tid; i < ML_CHUNK; i += blockDim.x) s_core[i] = 0.f;
@@ -557,7 +587,7 @@ tau_ml_kernel(const LineF32* __restrict__ prep, int n_lines, const int2* __restr
     double c = 0.0;
     for (int j = 0; j < ML_K; ++j) {
       const float fj = __shfl_sync(0xffffffffu, f2, j);
-      c += (double)fj * cospi((double)(lane & 15) * (2.0 * j + 1.0) / (2.0 * ML_K));
+      c += (double)fj * c_dct16[(lane & 15) * ML_K + j];
     }
     if (lane < ML_K) s_c2[warp][lane] = use_l2 ? (float)(c * (2.0 / ML_K)) : 0.f;
     // 8-node set: lanes j, j+8, j+16, j+24 hold quarters of node j
@@ -567,7 +597,7 @@ tau_ml_kernel(const LineF32* __restrict__ prep, int n_lines, const int2* __restr
     double cf = 0.0;
     for (int j = 0; j < ML_KF; ++j) {
       const float gj = __shfl_sync(0xffffffffu, g2, j);
-      cf += (double)gj * cospi((double)(lane & 7) * (2.0 * j + 1.0) / (2.0 * ML_KF));
+      cf += (double)gj * c_dct8[(lane & 7) * ML_KF + j];
     }
     if (lane < ML_KF) s_c2f[warp][lane] = use_l2 ? (float)(cf * (2.0 / ML_KF)) : 0.f;
   }

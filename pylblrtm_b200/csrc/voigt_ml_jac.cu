@@ -21,6 +21,7 @@
 // w' = -2zw + 2i/sqrt(pi) there would cancel catastrophically).
 #include <math.h>
 
+#include "cheb_tables.h"
 #include "faddeeva.cuh"
 #include "lbl_common.cuh"
 #include "sum_common.cuh"
@@ -35,6 +36,11 @@ constexpr int MJ_K = 16;
 constexpr float MJ_MIN_H1 = 32.f;
 constexpr float MJ_MIN_H2 = 16.f;
 constexpr int MJ_NB = 1024;                        // near items buffered per batch (dynamic shared memory)
+
+// Chebyshev node offsets (fractions of the half-width) and DCT weights, row-major [k][j]
+static __constant__ float c_jnode16[MJ_K] = {LBL_CHEB16_NODES};
+static __constant__ double c_jdct16[MJ_K * MJ_K] = {LBL_DCT16};
+static_assert(MJ_K == 16, "tables of cheb_tables.h");
 
 struct JLine {
   float4 g;   // jf (or C1 - jf for level 1), a, b, amp
@@ -187,8 +193,8 @@ jac_ml_kernel(const LineF32* __restrict__ prep, const LineJac* __restrict__ jpre
   const int n_w = max(0, min(MJ_WARP_PTS, n_c - w0));
   const float H2 = 0.5f * (float)(n_w - 1), C2w = (float)w0 + H2;
   const bool use_l2 = H2 >= MJ_MIN_H2;
-  const float xn1 = H1 * (float)cospi((2.0 * (tid & 15) + 1.0) / (2.0 * MJ_K));
-  const float xn2 = H2 * (float)cospi((2.0 * (lane & 15) + 1.0) / (2.0 * MJ_K));
+  const float xn1 = H1 * c_jnode16[tid & 15];
+  const float xn2 = H2 * c_jnode16[lane & 15];
   const float pf = (float)(w0 + lane * P);
 
   for (int i = tid; i < 3 * MJ_CHUNK; i += blockDim.x) (&s_core[0][0])[i] = 0.f;
@@ -440,7 +446,7 @@ jac_ml_kernel(const LineF32* __restrict__ prep, const LineJac* __restrict__ jpre
   if (tid < 3 * MJ_K) {
     const int q = tid / MJ_K, k = tid % MJ_K;
     double c = 0.0;
-    for (int j = 0; j < MJ_K; ++j) c += s_red[q][j] * cospi((double)k * (2.0 * j + 1.0) / (2.0 * MJ_K));
+    for (int j = 0; j < MJ_K; ++j) c += s_red[q][j] * c_jdct16[k * MJ_K + j];
     s_c1[q][k] = use_l1 ? (float)(c * (2.0 / MJ_K)) : 0.f;
   }
   // level-2 node values of this warp: lanes j and j+16 hold halves of node j
@@ -451,7 +457,7 @@ jac_ml_kernel(const LineF32* __restrict__ prep, const LineJac* __restrict__ jpre
     double c = 0.0;
     for (int j = 0; j < MJ_K; ++j) {
       const float fj = __shfl_sync(0xffffffffu, f2, j);
-      c += (double)fj * cospi((double)(lane & 15) * (2.0 * j + 1.0) / (2.0 * MJ_K));
+      c += (double)fj * c_jdct16[(lane & 15) * MJ_K + j];
     }
     if (lane < MJ_K) s_c2[warp][q][lane] = use_l2 ? (float)(c * (2.0 / MJ_K)) : 0.f;
   }
