@@ -106,7 +106,7 @@ __device__ __forceinline__ float clenshaw16(const float* c, float t) {
 // in the first 24 floats of the chunk's own od slice (level 1 needs >= 65 points);
 // tau_ml_kernel reads them before it writes the slice.
 constexpr int MF_THREADS = 256;                // lines per round
-constexpr int MF_FLUSH = 8;                    // rounds summed in float before the double sums
+constexpr int MF_FLUSH = 32;                   // rounds summed in float before the double sums
 
 constexpr int MF_STAGES = 3;                   // rounds of line records in flight per thread
 
@@ -160,7 +160,20 @@ __device__ __forceinline__ void far_line_nodes(float (&f)[K], const float (&xs)[
   }
 }
 
-__global__ void __launch_bounds__(MF_THREADS, 2)
+// Adds the lanes' float node sums into the warp's float64 sums (lane 0 owns the row) and clears them.
+template <int K>
+__device__ __forceinline__ void flush_nodes(float (&f)[K], double* row, int lane) {
+#pragma unroll
+  for (int k = 0; k < K; ++k) {
+    double v = (double)f[k];
+#pragma unroll
+    for (int o = 16; o >= 1; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    if (lane == 0) row[k] += v;
+    f[k] = 0.f;
+  }
+}
+
+__global__ void __launch_bounds__(MF_THREADS, 4)
 tau_far_kernel(const LineF32* __restrict__ prep, int n_lines, const int2* __restrict__ ranges, double nu_min,
                double step, long long n_nu, int tile_samples, int chunks_per_tile, int chunk_pts, double cutoff,
                float* __restrict__ od, unsigned long long* evals, unsigned long long* work, int tile_first,
@@ -186,6 +199,8 @@ tau_far_kernel(const LineF32* __restrict__ prep, int n_lines, const int2* __rest
   const LineF32* lp = prep + (long long)row * n_lines;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   if (tid < 2) s_cnt[tid] = 0u;
+  if (lane == 0)                                           // this warp's node sums: lane 0 alone
+    for (int k = 0; k < ML_K + ML_KF; ++k) s_part[warp][k] = 0.0;   // writes and reads them
 
   float xa[ML_K / 2], xb[ML_KF / 2];                      // node offsets, as tau_ml_kernel places them
 #pragma unroll
@@ -194,11 +209,10 @@ tau_far_kernel(const LineF32* __restrict__ prep, int n_lines, const int2* __rest
   for (int k = 0; k < ML_KF / 2; ++k) xb[k] = H1 * c_node8[k];
 
   float f1[ML_K], ff[ML_KF];
-  double d1[ML_K], df[ML_KF];
 #pragma unroll
-  for (int k = 0; k < ML_K; ++k) { f1[k] = 0.f; d1[k] = 0.0; }
+  for (int k = 0; k < ML_K; ++k) f1[k] = 0.f;
 #pragma unroll
-  for (int k = 0; k < ML_KF; ++k) { ff[k] = 0.f; df[k] = 0.0; }
+  for (int k = 0; k < ML_KF; ++k) ff[k] = 0.f;
   unsigned n1 = 0, nf = 0;
 
   // line records of round r (line rng.x + r * MF_THREADS + tid) go to stage r % MF_STAGES,
@@ -243,35 +257,16 @@ tau_far_kernel(const LineF32* __restrict__ prep, int n_lines, const int2* __rest
         ++n1;
       }
     }
-    if (++rounds == MF_FLUSH) {
+    if (++rounds == MF_FLUSH) {                            // warp-uniform: every lane runs every round
       rounds = 0;
-#pragma unroll
-      for (int k = 0; k < ML_K; ++k) { d1[k] += (double)f1[k]; f1[k] = 0.f; }
-#pragma unroll
-      for (int k = 0; k < ML_KF; ++k) { df[k] += (double)ff[k]; ff[k] = 0.f; }
+      flush_nodes(f1, s_part[warp], lane);
+      flush_nodes(ff, s_part[warp] + ML_K, lane);
     }
   }
   cp_async_wait<0>();                                      // only empty groups remain
-#pragma unroll
-  for (int k = 0; k < ML_K; ++k) d1[k] += (double)f1[k];
-#pragma unroll
-  for (int k = 0; k < ML_KF; ++k) df[k] += (double)ff[k];
-
   // node sums over the CTA in double: warps, then across warps
-#pragma unroll
-  for (int k = 0; k < ML_K; ++k) {
-    double v = d1[k];
-#pragma unroll
-    for (int o = 16; o >= 1; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-    if (lane == 0) s_part[warp][k] = v;
-  }
-#pragma unroll
-  for (int k = 0; k < ML_KF; ++k) {
-    double v = df[k];
-#pragma unroll
-    for (int o = 16; o >= 1; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-    if (lane == 0) s_part[warp][ML_K + k] = v;
-  }
+  flush_nodes(f1, s_part[warp], lane);
+  flush_nodes(ff, s_part[warp] + ML_K, lane);
   n1 = __reduce_add_sync(0xffffffffu, n1);
   nf = __reduce_add_sync(0xffffffffu, nf);
   __syncthreads();                                         // s_cnt zeroed, s_part written
