@@ -57,6 +57,8 @@ static_assert(ML_K == 16 && ML_KF == 8, "tables of cheb_tables.h");
 struct MlLine {
   float4 g;   // jf (centre index relative to the chunk start), a, b, amp_far
   float4 h;   // y, y^2, amp, value the clamped far-wing loop adds inside the near zone
+  float4 p;   // amp_far * (B_1, B_2, B_3, B_4)
+  float4 q;   // amp_far * (B_5, B_6, B_7, B_8)
 };
 
 // Re w times the line amplitude at one point, any distance (fast far wing first).
@@ -70,11 +72,43 @@ __device__ __forceinline__ float line_value(float x, const MlLine& L) {
   return (float)((double)L.h.z * weideman_re_f32((double)x, (double)L.h.x));
 }
 
-// Five-term asymptotic form with |z|^2 clamped to >= MID_Z2 (the level-3 loop
-// body, times amp_far); inside the near zone it is the constant rc S(rc), rc = 1/MID_Z2.
-__device__ __forceinline__ float mid_clamped_term(float x, float y2) {
-  const float r = rcp_approx(fmaxf(fmaf(x, x, y2), MID_Z2));
-  return r * asym5_bracket(y2, r);
+// Five-term asymptotic real part regrouped by powers of r = 1/|z|^2 for one line:
+// with s = y^2 (fixed per line) and q = s r, 1 + sum_k r^k A_k(q) = sum_m B_m(s) r^m,
+//   B_0 = 1, B_1 = 1.5, B_2 = 3.75 - 2s, B_3 = 13.125 - 15s, B_4 = 59.0625 - 105s + 12s^2,
+//   B_5 = -787.5s + 210s^2, B_6 = 2835s^2 - 120s^3, B_7 = -3780s^3, B_8 = 1680s^4
+// (A_k from asym5_bracket). For s >= 4096, |z|^2 >= s gives r <= 1/4096 and the
+// r^5..r^8 terms stay below 1e-8 of the sum, so they are dropped (which also keeps
+// the coefficients far from float overflow). Float32 evaluation by Horner's rule
+// agrees with the grouped form to 6e-8 relative for s <= 1e4 and clamped r.
+__device__ __forceinline__ void asym5_line_coeffs(float s, float amp_far, float4& p, float4& q) {
+  const float b2 = fmaf(-2.0f, s, 3.75f), b3 = fmaf(-15.0f, s, 13.125f);
+  const float b4 = fmaf(fmaf(12.0f, s, -105.0f), s, 59.0625f);
+  p = make_float4(amp_far * 1.5f, amp_far * b2, amp_far * b3, amp_far * b4);
+  if (s < 4096.0f) {
+    const float s2 = s * s;
+    q = make_float4(amp_far * (fmaf(210.0f, s, -787.5f) * s), amp_far * (fmaf(-120.0f, s, 2835.0f) * s2),
+                    amp_far * (-3780.0f * s2 * s), amp_far * (1680.0f * s2 * s2));
+  } else {
+    q = make_float4(0.f, 0.f, 0.f, 0.f);
+  }
+}
+
+// amp_far * S at r (the level-3 loop body without the final r factor).
+__device__ __forceinline__ float asym5_scaled(float r, const MlLine& R) {
+  float v = fmaf(R.q.w, r, R.q.z);
+  v = fmaf(v, r, R.q.y);
+  v = fmaf(v, r, R.q.x);
+  v = fmaf(v, r, R.p.w);
+  v = fmaf(v, r, R.p.z);
+  v = fmaf(v, r, R.p.y);
+  v = fmaf(v, r, R.p.x);
+  return fmaf(v, r, R.g.w);
+}
+
+// r = 1/|z|^2 with |z|^2 clamped to >= MID_Z2: inside the near zone the loop adds the
+// constant r_c * asym5_scaled(r_c), r_c = rcp(MID_Z2).
+__device__ __forceinline__ float clamped_r(float x, float y2) {
+  return rcp_approx(fmaxf(fmaf(x, x, y2), MID_Z2));
 }
 
 __device__ __forceinline__ void kahan_add(float& sum, float& comp, float v) {
@@ -426,8 +460,9 @@ tau_ml_kernel(const LineF32* __restrict__ prep, int n_lines, const int2* __restr
     if (inner) {
       MlLine r;
       r.g = make_float4(jf, L.a, L.b, L.amp_far);
-      const float clamp_val = L.amp_far * mid_clamped_term(0.f, y2);   // r = 1/MID_Z2 when y2 < MID_Z2
-      r.h = make_float4(L.y, y2, L.amp, clamp_val);
+      asym5_line_coeffs(y2, L.amp_far, r.p, r.q);
+      const float rc = clamped_r(0.f, y2);                      // = rcp(MID_Z2) when y2 < MID_Z2
+      r.h = make_float4(L.y, y2, L.amp, rc * asym5_scaled(rc, r));
       const int slot = off2 + __popc(b2 & ((1u << lane) - 1u));
       s2[slot] = r;
       s_seg_start[slot] = off3 + near_scan - near_n;         // exclusive prefix in slot order
@@ -496,7 +531,10 @@ tau_ml_kernel(const LineF32* __restrict__ prep, int n_lines, const int2* __restr
       const MlLine R = s2[s_l3[warp][i]];
       const float x0 = fmaf(pf - R.g.x, R.g.y, -R.g.z);
 #pragma unroll
-      for (int m = 0; m < P; ++m) acc[m] = fmaf(R.g.w, mid_clamped_term(fmaf((float)m, R.g.y, x0), R.h.y), acc[m]);
+      for (int m = 0; m < P; ++m) {
+        const float r = clamped_r(fmaf((float)m, R.g.y, x0), R.h.y);
+        acc[m] = fmaf(r, asym5_scaled(r, R), acc[m]);
+      }
     }
     if (lane == 0) n_l3 += (unsigned long long)n3w * n_w;
     // ---- level 3, near part, spread over the CTA: near item i is point
