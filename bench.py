@@ -38,7 +38,7 @@ WORKLOAD = "three_gas_200k_lines_60_layers_600-2500cm-1_step0.001_cutoff25_tile2
 FLOPS_PER_EVAL_FAR = 12      # two-term far-wing form: 5 FFMA + 1 FMUL + 1 RCP (FMA = 2 flops)
 # multi-level kernel, per unit of each work category (FMA = 2 flops, RCP = 1):
 FLOPS_NODE = 12              # Chebyshev-node evaluation (two-term form)
-FLOPS_L3 = 38                # level-3 loop evaluation (clamped five-term form)
+FLOPS_L3 = 24                # level-3 loop evaluation (clamped five-term form by powers of 1/|z|^2: 2 FMA + max + RCP + 9 FMA)
 FLOPS_NEAR = 60              # near-zone point (float continued fraction / float64 rational, average)
 FLOPS_CHEB_PER_POINT = 144   # 16 + 8 Clenshaw terms for each of levels 1 and 2 (3 flops a term)
 CPU_SAMPLE = (1000.0, 1000.5)  # sub-window timed on the host (all 60 layers)

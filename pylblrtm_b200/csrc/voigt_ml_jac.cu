@@ -78,6 +78,22 @@ __device__ __forceinline__ U3 series5(float x, float y, float r) {
   return o;
 }
 
+// The same series cut after two terms, for |z|^2 >= FAR_Z2 (|p| <= 4e-4, so the dropped
+// terms are below 2e-7 of the kept ones): w = (i/sqrt(pi)) q (1 + p/2),
+// w' = -(i/sqrt(pi)) p (1 + 3p/2).
+__device__ __forceinline__ U3 series2(float x, float y, float r) {
+  const float qr = x * r, qi = -y * r;
+  const float pr = qr * qr - qi * qi, pi_ = 2.f * qr * qi;
+  const float ar = fmaf(0.5f, pr, 1.0f), ai = 0.5f * pi_;
+  const float br = fmaf(1.5f, pr, 1.0f), bi = 1.5f * pi_;
+  const float k = float(INV_SQRT_PI);
+  U3 o;
+  o.u = -k * (qr * ai + qi * ar);
+  o.ux = k * (pr * bi + pi_ * br);
+  o.uy = k * (pr * br - pi_ * bi);
+  return o;
+}
+
 // Accurate u, u_x, u_y for |z|^2 < MID_Z2 (continued fraction or Weideman).
 __device__ __noinline__ U3 near3(float x, float y, float z2) {
   double wr, wi;
@@ -115,6 +131,7 @@ __device__ __noinline__ U3 near3(float x, float y, float z2) {
 
 __device__ __forceinline__ U3 value3(float x, const JLine& L) {
   const float z2 = fmaf(x, x, L.h.y);
+  if (z2 >= FAR_Z2) return series2(x, L.h.x, rcp_approx(z2));
   if (z2 >= MID_Z2) return series5(x, L.h.x, rcp_approx(z2));
   return near3(x, L.h.x, z2);
 }
