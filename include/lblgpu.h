@@ -197,11 +197,19 @@ int lbl_tau_tiles_ml_f32(const LineF32* prep, int n_lines, const int* ranges, co
  * kernel writes nothing per point and instead adds sum_p g_tau * d_t (d_v) into
  * vjp_t[row] (vjp_v[row]) (caller zeroes them): the vector-Jacobian product,
  * recomputing every Voigt value instead of storing the Jacobian (its per-row
- * sums use global atomics). flags: LBL_DETERMINISTIC as for lbl_tau_tiles_ml_f32. */
-int lbl_jacobian_ml_f32(const LineF32* prep, const LineJac* jprep, int n_lines, const int* ranges,
+ * sums use global atomics). flags: LBL_DETERMINISTIC as for lbl_tau_tiles_ml_f32.
+ * Level 1 runs first as a line-per-thread kernel that leaves its Chebyshev
+ * coefficients in l1_work (lbl_jacobian_ml_work_floats floats, required); inner
+ * (nullable) are the ranges of lbl_ml_inner_ranges for the same grid, a superset of
+ * the inner lines of this kernel's smaller chunks. */
+int lbl_jacobian_ml_f32(const LineF32* prep, const LineJac* jprep, int n_lines, const int* ranges, const int* inner,
                         const double* t_layer, int n_rows, int n_lay, double nu_min, double step, long long n_nu,
-                        int tile_samples, double cutoff, float* od, float* d_t, float* d_v, const double* g_tau,
-                        double* vjp_t, double* vjp_v, int flags, void* stream);
+                        int tile_samples, double cutoff, float* l1_work, float* od, float* d_t, float* d_v,
+                        const double* g_tau, double* vjp_t, double* vjp_v, int flags, void* stream);
+
+/* Floats of the l1_work buffer lbl_jacobian_ml_f32 needs (level-1 Chebyshev
+ * coefficients per chunk and row); -1 for bad arguments. */
+long long lbl_jacobian_ml_work_floats(int n_rows, long long n_nu, int tile_samples);
 
 /* Column sums over layers and transmittance exp(-tau / mu); replaces
  * pylblrtm/forward.py:151 and config.py:266-270. od: [n_prof, n_lay, n_nu]

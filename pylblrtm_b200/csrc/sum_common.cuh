@@ -1,4 +1,4 @@
-// Device helpers shared by the summation kernels (voigt.cu, voigt_ml.cu).
+// Device helpers shared by the summation kernels (voigt.cu, voigt_ml.cu, voigt_ml_jac.cu).
 #pragma once
 
 #include "faddeeva.cuh"
@@ -44,6 +44,32 @@ __device__ __forceinline__ int stage_round(const Rec* __restrict__ lp, int li, i
   if (pass) emit(off + __popc(ballot & ((1u << lane) - 1u)), L);
   __syncthreads();
   return total;
+}
+
+// Asynchronous 16-byte global -> shared copies (cp.async, L2 only); a thread that
+// copies into and later reads only its own slots is ordered by its own wait_group.
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+
+// Adds the lanes' float node sums into the warp's float64 sums (lane 0 owns the row)
+// and clears them; every lane of the warp calls it.
+template <int K>
+__device__ __forceinline__ void flush_nodes(float (&f)[K], double* row, int lane) {
+#pragma unroll
+  for (int k = 0; k < K; ++k) {
+    double v = (double)f[k];
+#pragma unroll
+    for (int o = 16; o >= 1; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    if (lane == 0) row[k] += v;
+    f[k] = 0.f;
+  }
 }
 
 static __device__ __noinline__ float re_w_f32_mid(float x, float y, float y2, float z2) {

@@ -144,18 +144,6 @@ constexpr int MF_FLUSH = 32;                   // rounds summed in float before 
 
 constexpr int MF_STAGES = 3;                   // rounds of line records in flight per thread
 
-// Asynchronous 16-byte global -> shared copies (cp.async, L2 only); each thread copies
-// and later reads only its own slots, so its own wait_group orders them.
-__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
-  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
-  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
-template <int N>
-__device__ __forceinline__ void cp_async_wait() {
-  asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
-}
-
 // amp * Re w by the far-wing form (amp_far = amp y / sqrt(pi)), added to f (|z|^2 >= FAR_Z2, y >= 0).
 __device__ __forceinline__ void far_wing_add(float& f, float x, float y2, float ny2, float amp_far) {
   const float r = rcp_approx(fmaf(x, x, y2));
@@ -191,19 +179,6 @@ __device__ __forceinline__ void far_line_nodes(float (&f)[K], const float (&xs)[
       f[k] += far_node_general(fmaf(xs[k], L.a, xc), L.y, y2, L.amp, L.amp_far);
       f[K - 1 - k] += far_node_general(fmaf(xs[k], -L.a, xc), L.y, y2, L.amp, L.amp_far);
     }
-  }
-}
-
-// Adds the lanes' float node sums into the warp's float64 sums (lane 0 owns the row) and clears them.
-template <int K>
-__device__ __forceinline__ void flush_nodes(float (&f)[K], double* row, int lane) {
-#pragma unroll
-  for (int k = 0; k < K; ++k) {
-    double v = (double)f[k];
-#pragma unroll
-    for (int o = 16; o >= 1; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-    if (lane == 0) row[k] += v;
-    f[k] = 0.f;
   }
 }
 

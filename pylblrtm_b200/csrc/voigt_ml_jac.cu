@@ -14,11 +14,12 @@
 // (vector-Jacobian product), so backward passes need no Jacobian storage.
 //
 // The distance split is the one of tau_ml_kernel (voigt_ml.cu) with 4 points per
-// lane: Chebyshev nodes for lines far from the chunk (level 1) or from a warp's
-// 128-point sub-chunk (level 2), and a branch-free clamped loop plus a CTA-wide
-// near-zone correction for the rest (level 3). The far field uses the five-term
-// asymptotic series of w and its termwise derivative for w' (forming
-// w' = -2zw + 2i/sqrt(pi) there would cancel catastrophically).
+// lane: Chebyshev nodes for lines far from the chunk (level 1, a line-per-thread
+// kernel of its own, jac_far_kernel) or from a warp's 128-point sub-chunk (level 2),
+// and a branch-free clamped loop plus a CTA-wide near-zone correction for the rest
+// (level 3). The far field uses the asymptotic series of w and its termwise
+// derivative for w' (five terms; two where |z|^2 >= FAR_Z2); forming
+// w' = -2zw + 2i/sqrt(pi) there would cancel catastrophically.
 #include <math.h>
 
 #include "cheb_tables.h"
@@ -40,7 +41,15 @@ constexpr int MJ_NB = 1024;                        // near items buffered per ba
 // Chebyshev node offsets (fractions of the half-width) and DCT weights, row-major [k][j]
 static __constant__ float c_jnode16[MJ_K] = {LBL_CHEB16_NODES};
 static __constant__ double c_jdct16[MJ_K * MJ_K] = {LBL_DCT16};
-static_assert(MJ_K == 16, "tables of cheb_tables.h");
+constexpr int MJ_KF = 8;                           // nodes for level-1 lines beyond six half-widths
+constexpr float MJ_FAR1 = 5.f;                     // "far": more than (1 + MJ_FAR1) half-widths from the centre
+constexpr int MJ_NCOEF = 3 * (MJ_K + MJ_KF);       // level-1 coefficients per (chunk, row)
+constexpr int MJF_THREADS = 256;                   // lines per round of jac_far_kernel
+constexpr int MJF_STAGES = 2;                      // rounds of line records in flight per thread
+constexpr int MJF_FLUSH = 32;                      // rounds summed in float before the double sums
+static __constant__ float c_jnode8[MJ_KF] = {LBL_CHEB8_NODES};
+static __constant__ double c_jdct8[MJ_KF * MJ_KF] = {LBL_DCT8};
+static_assert(MJ_K == 16 && MJ_KF == 8, "tables of cheb_tables.h");
 
 struct JLine {
   float4 g;   // jf (or C1 - jf for level 1), a, b, amp
@@ -152,11 +161,12 @@ __device__ __forceinline__ void kahan3(float* sum, float* comp, const float* v) 
   }
 }
 
+template <int K = MJ_K>
 __device__ __forceinline__ float clenshaw_k(const float* c, float t) {
   float b1 = 0.f, b2 = 0.f;
   const float t2 = 2.f * t;
 #pragma unroll
-  for (int k = MJ_K - 1; k >= 1; --k) {
+  for (int k = K - 1; k >= 1; --k) {
     const float b0 = fmaf(t2, b1, c[k] - b2);
     b2 = b1;
     b1 = b0;
@@ -164,31 +174,194 @@ __device__ __forceinline__ float clenshaw_k(const float* c, float t) {
   return fmaf(t, b1, 0.5f * c[0] - b2);
 }
 
+// ---------------------------------------------------------------------------
+// Level 1 of the Jacobian sums as its own kernel (as tau_far_kernel for the optical
+// depth): one thread takes one level-1 line and evaluates u, u_x, u_y at all of the
+// chunk's Chebyshev nodes (16; 8 beyond six half-widths), adding the three weighted sums
+// in registers. It writes the chunk's 3 x (16 + 8) Chebyshev coefficients to l1_coef
+// ([row][chunk of the launch][MJ_NCOEF]), which jac_ml_kernel reads.
+struct JFarLine {
+  LineF32 l;
+  LineJac j;
+};
+
+static __device__ __noinline__ U3 jac_node_general(float x, float y, float y2) {
+  const float z2 = fmaf(x, x, y2);
+  if (z2 >= FAR_Z2) return series2(x, y, rcp_approx(z2));
+  if (z2 >= MID_Z2) return series5(x, y, rcp_approx(z2));
+  return near3(x, y, z2);
+}
+
+// The three sums of add3 for one line at one node.
+__device__ __forceinline__ void add3_line(float& s0, float& s1, float& s2, const U3& v, float x, const LineF32& L,
+                                          const LineJac& J) {
+  s0 = fmaf(L.amp, v.u, s0);
+  s1 = fmaf(J.jT_u, v.u, fmaf(-J.jT_x * x, v.ux, fmaf(-J.jT_y, v.uy, s1)));
+  s2 = fmaf(J.jv_u, v.u, fmaf(J.jv_y, v.uy, fmaf(-J.jv_x, v.ux, s2)));
+}
+
+// Node sums of one level-1 line: nodes k and K-1-k sit at +xs[k] and -xs[k] from the chunk centre.
+template <int K>
+__device__ __forceinline__ void jfar_line(float (&f)[3][K], const float (&xs)[K / 2], const LineF32& L,
+                                          const LineJac& J, float xc, float y2, bool fast) {
+  if (fast) {
+#pragma unroll
+    for (int k = 0; k < K / 2; ++k) {
+      const float xp = fmaf(xs[k], L.a, xc), xm = fmaf(-xs[k], L.a, xc);
+      add3_line(f[0][k], f[1][k], f[2][k], series2(xp, L.y, rcp_approx(fmaf(xp, xp, y2))), xp, L, J);
+      add3_line(f[0][K - 1 - k], f[1][K - 1 - k], f[2][K - 1 - k],
+                series2(xm, L.y, rcp_approx(fmaf(xm, xm, y2))), xm, L, J);
+    }
+  } else {
+#pragma unroll
+    for (int k = 0; k < K / 2; ++k) {
+      const float xp = fmaf(xs[k], L.a, xc), xm = fmaf(-xs[k], L.a, xc);
+      add3_line(f[0][k], f[1][k], f[2][k], jac_node_general(xp, L.y, y2), xp, L, J);
+      add3_line(f[0][K - 1 - k], f[1][K - 1 - k], f[2][K - 1 - k], jac_node_general(xm, L.y, y2), xm, L, J);
+    }
+  }
+}
+
+// One pass of jac_far_kernel over the tile's candidate lines for the lines of one node
+// class (K = MJ_K: level-1 lines within six half-widths; K = MJ_KF: beyond); the warp's
+// float64 sums of that class go to row[q * K + k]. Two passes keep 3 K accumulators live
+// instead of 3 (MJ_K + MJ_KF).
+template <int K>
+__device__ __forceinline__ void jfar_pass(JFarLine (*s_line)[MJF_THREADS], const LineF32* lp, const LineJac* jp,
+                                          int2 rng, double wlo, double whi, long long c0, float H1,
+                                          const float (&xs)[K / 2], double* row) {
+  const int tid = threadIdx.x, lane = tid & 31;
+  const float C1 = H1;
+  float f[3][K];
+#pragma unroll
+  for (int q = 0; q < 3; ++q)
+#pragma unroll
+    for (int k = 0; k < K; ++k) f[q][k] = 0.f;
+  // records of round r (line rng.x + r * MJF_THREADS + tid) go to stage r % 2, one round
+  // ahead; each thread copies into and reads only its own slots
+  const int n_rounds = rng.y > rng.x ? (rng.y - rng.x + MJF_THREADS - 1) / MJF_THREADS : 0;
+  auto issue = [&](int r, int stage) {
+    const int li = rng.x + r * MJF_THREADS + tid;
+    if (li < rng.y) {   // 32-B records in 256-B aligned allocations
+      const float4* g = reinterpret_cast<const float4*>(lp + li);
+      const float4* h = reinterpret_cast<const float4*>(jp + li);
+      float4* d = reinterpret_cast<float4*>(&s_line[stage][tid]);
+      cp_async16(d, g);
+      cp_async16(d + 1, g + 1);
+      cp_async16(d + 2, h);
+      cp_async16(d + 3, h + 1);
+    }
+    cp_async_commit();
+  };
+  issue(0, 0);
+  int rounds = 0;
+  for (int r = 0; r < n_rounds; ++r) {
+    const int stage = r & 1;
+    issue(r + 1, stage ^ 1);                                // the stage read last round
+    cp_async_wait<1>();
+    const bool have = rng.x + r * MJF_THREADS + tid < rng.y;
+    JFarLine R;
+    if (have) R = s_line[stage][tid];
+    // the level-1 test of jac_ml_kernel, expression for expression, then the node class
+    const bool pass = have && (R.l.nuc >= wlo) && (R.l.nuc <= whi);
+    const float jf = (float)((long long)R.l.j0 - c0);
+    const float dd = fabsf(jf - C1) - H1;
+    const bool far8 = dd > MJ_FAR1 * H1;
+    if (pass && dd > H1 + 1.f && far8 == (K == MJ_KF)) {
+      const float xc = fmaf(C1 - jf, R.l.a, -R.l.b);
+      const float y2 = R.l.y * R.l.y;
+      const float xm = fmaf(-H1 * c_jnode16[0], R.l.a, fabsf(xc));   // nearest node, as in tau_far_kernel
+      jfar_line<K>(f, xs, R.l, R.j, xc, y2, fmaf(xm, xm, y2) >= FAR_Z2);
+    }
+    if (++rounds == MJF_FLUSH) {
+      rounds = 0;
+#pragma unroll
+      for (int q = 0; q < 3; ++q) flush_nodes(f[q], row + q * K, lane);
+    }
+  }
+  cp_async_wait<0>();                                      // only empty groups remain
+#pragma unroll
+  for (int q = 0; q < 3; ++q) flush_nodes(f[q], row + q * K, lane);
+}
+
+__global__ void __launch_bounds__(MJF_THREADS, 2)
+jac_far_kernel(const LineF32* __restrict__ prep, const LineJac* __restrict__ jprep, int n_lines,
+               const int2* __restrict__ ranges, double nu_min, double step, long long n_nu, int tile_samples,
+               int chunks_per_tile, int chunk_pts, double cutoff, float* __restrict__ l1_coef) {
+  __shared__ __align__(16) JFarLine s_line[MJF_STAGES][MJF_THREADS];   // records 64 B, 16-B aligned
+  __shared__ double s_part[MJF_THREADS / 32][MJ_NCOEF];                 // [q][16] then [q][8] per warp
+
+  const int row = blockIdx.y;
+  const int tile = blockIdx.x / chunks_per_tile, chunk = blockIdx.x % chunks_per_tile;
+  const long long t0 = (long long)tile * tile_samples;
+  const long long t1 = min(t0 + (long long)tile_samples, n_nu);
+  const long long c0 = t0 + (long long)chunk * chunk_pts;
+  if (c0 >= t1) return;
+  const int n_c = (int)(min(c0 + (long long)chunk_pts, t1) - c0);
+  const float H1 = 0.5f * (float)(n_c - 1);               // same chunk geometry as jac_ml_kernel
+  if (!(H1 >= MJ_MIN_H1)) return;                         // no level 1: jac_ml_kernel takes every line
+  const double wlo = __dsub_rn(grid_nu(nu_min, step, t0), cutoff);
+  const double whi = __dadd_rn(grid_nu(nu_min, step, t1 - 1), cutoff);
+  const int2 rng = ranges[tile];
+  const LineF32* lp = prep + (long long)row * n_lines;
+  const LineJac* jp = jprep + (long long)row * n_lines;
+  const int tid = threadIdx.x, warp = tid >> 5;
+  if ((tid & 31) == 0)
+    for (int k = 0; k < MJ_NCOEF; ++k) s_part[warp][k] = 0.0;
+
+  float xa[MJ_K / 2], xb[MJ_KF / 2];
+#pragma unroll
+  for (int k = 0; k < MJ_K / 2; ++k) xa[k] = H1 * c_jnode16[k];
+#pragma unroll
+  for (int k = 0; k < MJ_KF / 2; ++k) xb[k] = H1 * c_jnode8[k];
+  jfar_pass<MJ_K>(s_line, lp, jp, rng, wlo, whi, c0, H1, xa, s_part[warp]);
+  jfar_pass<MJ_KF>(s_line, lp, jp, rng, wlo, whi, c0, H1, xb, s_part[warp] + 3 * MJ_K);
+  __syncthreads();
+  if (tid < MJ_NCOEF) {                                    // column tid: only this thread touches it
+    double v = 0.0;
+    for (int w = 0; w < MJF_THREADS / 32; ++w) v += s_part[w][tid];
+    s_part[0][tid] = v;
+  }
+  __syncthreads();
+  if (tid < MJ_NCOEF) {                                    // Chebyshev coefficients (DCT)
+    double c = 0.0;
+    if (tid < 3 * MJ_K) {
+      const int q = tid / MJ_K, k = tid % MJ_K;
+      for (int j = 0; j < MJ_K; ++j) c += s_part[0][q * MJ_K + j] * c_jdct16[k * MJ_K + j];
+      c *= 2.0 / MJ_K;
+    } else {
+      const int q = (tid - 3 * MJ_K) / MJ_KF, k = (tid - 3 * MJ_K) % MJ_KF;
+      for (int j = 0; j < MJ_KF; ++j) c += s_part[0][3 * MJ_K + q * MJ_KF + j] * c_jdct8[k * MJ_KF + j];
+      c *= 2.0 / MJ_KF;
+    }
+    l1_coef[((long long)row * gridDim.x + blockIdx.x) * MJ_NCOEF + tid] = (float)c;
+  }
+}
+
 template <bool DET>
 __global__ void __launch_bounds__(MJ_THREADS, 2)
 jac_ml_kernel(const LineF32* __restrict__ prep, const LineJac* __restrict__ jprep, int n_lines,
-              const int2* __restrict__ ranges, const double* __restrict__ t_layer, double nu_min, double step,
-              long long n_nu, int tile_samples, int chunks_per_tile, double cutoff, float* __restrict__ od,
+              const int2* __restrict__ ranges, const int2* __restrict__ inner_ranges,
+              const double* __restrict__ t_layer, double nu_min, double step, long long n_nu, int tile_samples,
+              int chunks_per_tile, double cutoff, const float* __restrict__ l1_coef, float* __restrict__ od,
               float* __restrict__ d_t, float* __restrict__ d_v, int n_lay, const double* __restrict__ g_tau,
               double* __restrict__ vjp_t, double* __restrict__ vjp_v) {
   constexpr int P = MJ_P;
-  __shared__ JLine s1[MJ_THREADS];
   __shared__ JLine s2[MJ_THREADS];
   __shared__ unsigned char s_l2[MJ_THREADS / 32][MJ_THREADS];
   __shared__ unsigned char s_l3[MJ_THREADS / 32][MJ_THREADS];
   __shared__ unsigned char s_nl[MJ_THREADS / 32][MJ_THREADS];   // per-warp slots with near points in it
-  __shared__ int s_cnt[3][MJ_THREADS / 32];
+  __shared__ int s_cnt[2][MJ_THREADS / 32];
   __shared__ int s_seg_start[MJ_THREADS + 1];
   __shared__ short s_seg_lo[MJ_THREADS];
   __shared__ unsigned char s_seg_mask[MJ_THREADS];
   __shared__ float s_core[3][MJ_CHUNK];              // near corrections (each point owned by one thread)
   extern __shared__ float s_nbuf_dyn[];              // near-item values of one batch: [3][MJ_NB]
   float (*s_nbuf)[MJ_NB] = reinterpret_cast<float (*)[MJ_NB]>(s_nbuf_dyn);
-  __shared__ float s_c1[3][MJ_K];
+  __shared__ float s_c1[MJ_NCOEF];                  // level-1 coefficients from jac_far_kernel
   __shared__ float s_c2[MJ_THREADS / 32][3][MJ_K];
-  // the level-1 line records are dead after the last round; their space holds the reductions
-  double (*s_red)[MJ_THREADS] = reinterpret_cast<double (*)[MJ_THREADS]>(&s1[0]);
-  static_assert(sizeof(s1) >= 3 * MJ_THREADS * sizeof(double), "reduction buffer");
+  __shared__ float s_c2f[MJ_THREADS / 32][3][MJ_KF];
+  __shared__ double s_vjp[2][MJ_THREADS / 32];
 
   const int row = blockIdx.y;
   const int tile = blockIdx.x / chunks_per_tile, chunk = blockIdx.x % chunks_per_tile;
@@ -199,19 +372,25 @@ jac_ml_kernel(const LineF32* __restrict__ prep, const LineJac* __restrict__ jpre
   const int n_c = (int)(min(c0 + (long long)(blockDim.x * P), t1) - c0);
   const double wlo = __dsub_rn(grid_nu(nu_min, step, t0), cutoff);
   const double whi = __dadd_rn(grid_nu(nu_min, step, t1 - 1), cutoff);
-  const int2 rng = ranges[tile];
   const LineF32* lp = prep + (long long)row * n_lines;
   const LineJac* jp = jprep + (long long)row * n_lines;
 
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, n_warps = blockDim.x >> 5;
   const float H1 = 0.5f * (float)(n_c - 1), C1 = H1;
   const bool use_l1 = H1 >= MJ_MIN_H1;
+  // with level 1 (jac_far_kernel) only the inner range can hold inner lines of this chunk
+  int2 rng = ranges[tile];
+  if (use_l1 && inner_ranges) {
+    const int2 q = inner_ranges[tile];
+    rng = make_int2(max(rng.x, q.x), min(rng.y, q.y));
+  }
+  if (use_l1 && tid < MJ_NCOEF) s_c1[tid] = l1_coef[((long long)row * gridDim.x + blockIdx.x) * MJ_NCOEF + tid];
   const int w0 = warp * MJ_WARP_PTS;
   const int n_w = max(0, min(MJ_WARP_PTS, n_c - w0));
   const float H2 = 0.5f * (float)(n_w - 1), C2w = (float)w0 + H2;
   const bool use_l2 = H2 >= MJ_MIN_H2;
-  const float xn1 = H1 * c_jnode16[tid & 15];
   const float xn2 = H2 * c_jnode16[lane & 15];
+  const float xn2f = H2 * c_jnode8[lane & 7];
   const float pf = (float)(w0 + lane * P);
 
   for (int i = tid; i < 3 * MJ_CHUNK; i += blockDim.x) (&s_core[0][0])[i] = 0.f;
@@ -221,8 +400,7 @@ jac_ml_kernel(const LineF32* __restrict__ prep, const LineJac* __restrict__ jpre
   for (int q = 0; q < 3; ++q)
 #pragma unroll
     for (int m = 0; m < P; ++m) acc[q][m] = 0.f;
-  float sum1[3] = {0.f, 0.f, 0.f}, comp1[3] = {0.f, 0.f, 0.f};
-  float sum2[3] = {0.f, 0.f, 0.f}, comp2[3] = {0.f, 0.f, 0.f};
+  float sum2[3] = {0.f, 0.f, 0.f}, comp2[3] = {0.f, 0.f, 0.f}, sum2f[3] = {0.f, 0.f, 0.f};
 
   for (int base = rng.x; base < rng.y; base += blockDim.x) {
     const int li = base + tid;
@@ -235,7 +413,7 @@ jac_ml_kernel(const LineF32* __restrict__ prep, const LineJac* __restrict__ jpre
     }
     const bool pass = have && (L.nuc >= wlo) && (L.nuc <= whi);
     const float jf = (float)((long long)L.j0 - c0);
-    const bool lev1 = pass && use_l1 && (fabsf(jf - C1) - H1 > H1 + 1.f);
+    const bool lev1 = pass && use_l1 && (fabsf(jf - C1) - H1 > H1 + 1.f);   // jac_far_kernel's line
     const bool inner = pass && !lev1;
     const float y2 = L.y * L.y;
     const float hw = (y2 >= MID_Z2 && L.y >= 0.f) ? -1.0f : sqrtf(fmaxf(MID_Z2 - y2, 0.f)) / L.a + 1.0f;
@@ -265,71 +443,57 @@ jac_ml_kernel(const LineF32* __restrict__ prep, const LineJac* __restrict__ jpre
       const int t = __shfl_up_sync(0xffffffffu, near_scan, o);
       if (lane >= o) near_scan += t;
     }
-    const unsigned b1 = __ballot_sync(0xffffffffu, lev1), b2 = __ballot_sync(0xffffffffu, inner);
-    if (lane == 0) {
-      s_cnt[0][warp] = __popc(b1);
-      s_cnt[1][warp] = __popc(b2);
-    }
-    if (lane == 31) s_cnt[2][warp] = near_scan;
+    const unsigned b2 = __ballot_sync(0xffffffffu, inner);
+    if (lane == 0) s_cnt[0][warp] = __popc(b2);
+    if (lane == 31) s_cnt[1][warp] = near_scan;
     __syncthreads();
-    int off1 = 0, off2 = 0, off3 = 0, n1 = 0, n2 = 0, n_near = 0;
+    int off2 = 0, off3 = 0, n2 = 0, n_near = 0;
     for (int w = 0; w < n_warps; ++w) {
-      const int a1 = s_cnt[0][w], a2 = s_cnt[1][w], a3 = s_cnt[2][w];
-      off1 += (w < warp) ? a1 : 0;
+      const int a2 = s_cnt[0][w], a3 = s_cnt[1][w];
       off2 += (w < warp) ? a2 : 0;
       off3 += (w < warp) ? a3 : 0;
-      n1 += a1;
       n2 += a2;
       n_near += a3;
     }
-    if (pass) {
+    if (inner) {
       JLine r;
-      r.g = make_float4(lev1 ? C1 - jf : jf, L.a, L.b, L.amp);
+      r.g = make_float4(jf, L.a, L.b, L.amp);
       r.h = make_float4(L.y, y2, J.jT_u, J.jT_x);
       r.k = make_float4(J.jT_y, J.jv_u, J.jv_y, J.jv_x);
-      const unsigned lt = (1u << lane) - 1u;
-      if (lev1) {
-        s1[off1 + __popc(b1 & lt)] = r;
-      } else {
-        const int slot = off2 + __popc(b2 & lt);
-        s2[slot] = r;
-        s_seg_start[slot] = off3 + near_scan - near_n;
-        s_seg_lo[slot] = (short)near_lo;
-        s_seg_mask[slot] = (unsigned char)l3mask;
-      }
+      const int slot = off2 + __popc(b2 & ((1u << lane) - 1u));
+      s2[slot] = r;
+      s_seg_start[slot] = off3 + near_scan - near_n;
+      s_seg_lo[slot] = (short)near_lo;
+      s_seg_mask[slot] = (unsigned char)l3mask;
     }
     if (tid == 0) s_seg_start[n2] = n_near;
     __syncthreads();
 
-    // level 1: thread (tid & 15) evaluates its node for lines tid>>4, +16, ...
-    {
-      float a[3] = {0.f, 0.f, 0.f};
-      for (int l = tid >> 4; l < n1; l += (blockDim.x >> 4)) {
-        const JLine R = s1[l];
-        const float x = fmaf(xn1 + R.g.x, R.g.y, -R.g.z);
-        add3(a, value3(x, R), x, R);
-      }
-      kahan3(sum1, comp1, a);
-    }
-    // per-warp split of the inner lines into level 2 and level 3
-    int n2w = 0, n3w = 0, nnw = 0;
+    // per-warp split of the inner lines into level 2 (16 nodes; 8 beyond six sub-chunk
+    // half-widths, listed from the back of s_l2) and level 3
+    int n2w = 0, n2fw = 0, n3w = 0, nnw = 0;
     for (int k = 0; k < n2; k += 32) {
       const int l = k + lane;
-      bool is2 = false, is3 = false, nz = false;
+      bool is2 = false, is2f = false, is3 = false, nz = false;
       if (l < n2) {
         const float d = fabsf(s2[l].g.x - C2w) - H2;
-        is2 = use_l2 && d > H2 + 1.f;
-        is3 = !is2 && n_w > 0;
+        const bool lev2 = use_l2 && d > H2 + 1.f;
+        is2f = lev2 && d > MJ_FAR1 * H2;
+        is2 = lev2 && !is2f;
+        is3 = !lev2 && n_w > 0;
         if constexpr (DET) {   // near points of slot l inside this warp's sub-chunk (level 3 here)
           const int st = s_seg_start[l], len = s_seg_start[l + 1] - st, lo = s_seg_lo[l];
           nz = len > 0 && ((s_seg_mask[l] >> warp) & 1u) && lo < w0 + n_w && lo + len > w0;
         }
       }
       const unsigned q2 = __ballot_sync(0xffffffffu, is2), q3 = __ballot_sync(0xffffffffu, is3);
+      const unsigned q2f = __ballot_sync(0xffffffffu, is2f);
       const unsigned lt = (1u << lane) - 1u;
       if (is2) s_l2[warp][n2w + __popc(q2 & lt)] = (unsigned char)l;
+      if (is2f) s_l2[warp][MJ_THREADS - 1 - (n2fw + __popc(q2f & lt))] = (unsigned char)l;
       if (is3) s_l3[warp][n3w + __popc(q3 & lt)] = (unsigned char)l;
       n2w += __popc(q2);
+      n2fw += __popc(q2f);
       n3w += __popc(q3);
       if constexpr (DET) {
         const unsigned qn = __ballot_sync(0xffffffffu, nz);
@@ -347,6 +511,12 @@ jac_ml_kernel(const LineF32* __restrict__ prep, const LineJac* __restrict__ jpre
         add3(a, value3(x, R), x, R);
       }
       kahan3(sum2, comp2, a);
+      // far level-2 lines: quarter-warps take one line each, lane (& 7) = node
+      for (int i = lane >> 3; i < n2fw; i += 4) {
+        const JLine R = s2[s_l2[warp][MJ_THREADS - 1 - i]];
+        const float x = fmaf(xn2f + (C2w - R.g.x), R.g.y, -R.g.z);
+        add3(sum2f, value3(x, R), x, R);
+      }
     }
     // level 3, clamped loop (branch-free)
     for (int i = 0; i < n3w; ++i) {
@@ -447,25 +617,8 @@ jac_ml_kernel(const LineF32* __restrict__ prep, const LineJac* __restrict__ jpre
     // No barrier here: the next round writes the staging arrays only after its first
     // barrier, which every warp reaches after finishing this round.
   }
-  __syncthreads();   // every warp is done with s1 (aliased by s_red)
+  __syncthreads();
 
-  // level-1 node values (reduce the 16-thread groups) and Chebyshev coefficients
-#pragma unroll
-  for (int q = 0; q < 3; ++q) s_red[q][tid] = (double)sum1[q] - (double)comp1[q];
-  __syncthreads();
-  if (tid < 3 * MJ_K) {
-    const int q = tid / MJ_K, j = tid % MJ_K;
-    double f = 0.0;
-    for (int i = j; i < (int)blockDim.x; i += MJ_K) f += s_red[q][i];
-    s_red[q][j] = f;   // read back after the barrier, only entries < MJ_K
-  }
-  __syncthreads();
-  if (tid < 3 * MJ_K) {
-    const int q = tid / MJ_K, k = tid % MJ_K;
-    double c = 0.0;
-    for (int j = 0; j < MJ_K; ++j) c += s_red[q][j] * c_jdct16[k * MJ_K + j];
-    s_c1[q][k] = use_l1 ? (float)(c * (2.0 / MJ_K)) : 0.f;
-  }
   // level-2 node values of this warp: lanes j and j+16 hold halves of node j
 #pragma unroll
   for (int q = 0; q < 3; ++q) {
@@ -477,6 +630,16 @@ jac_ml_kernel(const LineF32* __restrict__ prep, const LineJac* __restrict__ jpre
       c += (double)fj * c_jdct16[(lane & 15) * MJ_K + j];
     }
     if (lane < MJ_K) s_c2[warp][q][lane] = use_l2 ? (float)(c * (2.0 / MJ_K)) : 0.f;
+    // 8-node set: lanes j, j+8, j+16, j+24 hold quarters of node j
+    float g2 = sum2f[q];
+    g2 += __shfl_xor_sync(0xffffffffu, g2, 16);
+    g2 += __shfl_xor_sync(0xffffffffu, g2, 8);
+    double cf = 0.0;
+    for (int j = 0; j < MJ_KF; ++j) {
+      const float gj = __shfl_sync(0xffffffffu, g2, j);
+      cf += (double)gj * c_jdct8[(lane & 7) * MJ_KF + j];
+    }
+    if (lane < MJ_KF) s_c2f[warp][q][lane] = use_l2 ? (float)(cf * (2.0 / MJ_KF)) : 0.f;
   }
   __syncthreads();
 
@@ -492,8 +655,14 @@ jac_ml_kernel(const LineF32* __restrict__ prep, const LineJac* __restrict__ jpre
 #pragma unroll
     for (int q = 0; q < 3; ++q) {
       float s = s_core[q][pl];
-      if (use_l1) s += clenshaw_k(s_c1[q], ((float)pl - C1) * inv_h1);
-      if (use_l2) s += clenshaw_k(s_c2[warp][q], ((float)pl - C2w) * inv_h2);
+      if (use_l1) {
+        const float t1 = ((float)pl - C1) * inv_h1;
+        s += clenshaw_k(s_c1 + q * MJ_K, t1) + clenshaw_k<MJ_KF>(s_c1 + 3 * MJ_K + q * MJ_KF, t1);
+      }
+      if (use_l2) {
+        const float t2 = ((float)pl - C2w) * inv_h2;
+        s += clenshaw_k(s_c2[warp][q], t2) + clenshaw_k<MJ_KF>(s_c2f[warp][q], t2);
+      }
       v[q] = (double)acc[q][m] + (double)s;
     }
     const long long p = c0 + pl;
@@ -519,15 +688,15 @@ jac_ml_kernel(const LineF32* __restrict__ prep, const LineJac* __restrict__ jpre
       pv += __shfl_xor_sync(0xffffffffu, pv, o);
     }
     if (lane == 0) {
-      s_red[0][warp] = pt;
-      s_red[1][warp] = pv;
+      s_vjp[0][warp] = pt;
+      s_vjp[1][warp] = pv;
     }
     __syncthreads();
     if (tid == 0) {
       double a = 0.0, b = 0.0;
       for (int w = 0; w < n_warps; ++w) {
-        a += s_red[0][w];
-        b += s_red[1][w];
+        a += s_vjp[0][w];
+        b += s_vjp[1][w];
       }
       atomicAdd(&vjp_t[row], a);
       atomicAdd(&vjp_v[row], b);
@@ -539,23 +708,41 @@ jac_ml_kernel(const LineF32* __restrict__ prep, const LineJac* __restrict__ jpre
 
 using namespace lbl;
 
+static void jac_geometry(int tile_samples, long long n_nu, int* threads, int* cp, long long* n_tiles,
+                         long long* chunks) {
+  const int per_tile = tile_samples < MJ_CHUNK ? tile_samples : MJ_CHUNK;
+  *threads = 32 * ((per_tile + MJ_WARP_PTS - 1) / MJ_WARP_PTS);
+  *cp = *threads * MJ_P;
+  *n_tiles = (n_nu + tile_samples - 1) / tile_samples;
+  *chunks = (tile_samples + *cp - 1) / *cp;
+}
+
+extern "C" long long lbl_jacobian_ml_work_floats(int n_rows, long long n_nu, int tile_samples) {
+  if (n_rows < 1 || n_nu < 1 || tile_samples < 1) return -1;
+  int threads, cp;
+  long long n_tiles, chunks;
+  jac_geometry(tile_samples, n_nu, &threads, &cp, &n_tiles, &chunks);
+  return (long long)n_rows * n_tiles * chunks * MJ_NCOEF;
+}
+
 extern "C" int lbl_jacobian_ml_f32(const LineF32* prep, const LineJac* jprep, int n_lines, const int* ranges,
-                                   const double* t_layer, int n_rows, int n_lay, double nu_min, double step,
-                                   long long n_nu, int tile_samples, double cutoff, float* od, float* d_t,
-                                   float* d_v, const double* g_tau, double* vjp_t, double* vjp_v, int flags,
-                                   void* stream) {
+                                   const int* inner, const double* t_layer, int n_rows, int n_lay, double nu_min,
+                                   double step, long long n_nu, int tile_samples, double cutoff, float* l1_work,
+                                   float* od, float* d_t, float* d_v, const double* g_tau, double* vjp_t,
+                                   double* vjp_v, int flags, void* stream) {
   const bool vjp = g_tau != nullptr;
-  if (!prep || !jprep || !ranges || !t_layer || n_lines < 1 || n_rows < 1 || n_lay < 1 || n_rows % n_lay ||
-      n_rows > 65535 || n_nu < 1 || tile_samples < 1 || !(step > 0) || !(cutoff >= 0) ||
+  if (!prep || !jprep || !ranges || !t_layer || !l1_work || n_lines < 1 || n_rows < 1 || n_lay < 1 ||
+      n_rows % n_lay || n_rows > 65535 || n_nu < 1 || tile_samples < 1 || !(step > 0) || !(cutoff >= 0) ||
       (vjp ? (!vjp_t || !vjp_v) : (!od || !d_t || !d_v)))
     return lbl_set_error(LBL_EINVAL, "lbl_jacobian_ml_f32: bad arguments");
-  const int per_tile = tile_samples < MJ_CHUNK ? tile_samples : MJ_CHUNK;
-  const int threads = 32 * ((per_tile + MJ_WARP_PTS - 1) / MJ_WARP_PTS);
-  const int cp = threads * MJ_P;
-  const long long n_tiles = (n_nu + tile_samples - 1) / tile_samples;
-  const long long chunks = (tile_samples + cp - 1) / cp;
+  int threads, cp;
+  long long n_tiles, chunks;
+  jac_geometry(tile_samples, n_nu, &threads, &cp, &n_tiles, &chunks);
   if (n_tiles * chunks > 0x7fffffffLL) return lbl_set_error(LBL_EINVAL, "lbl_jacobian_ml_f32: grid too large");
   dim3 grid((unsigned)(n_tiles * chunks), (unsigned)n_rows);
+  cudaStream_t st = (cudaStream_t)stream;
+  jac_far_kernel<<<grid, MJF_THREADS, 0, st>>>(prep, jprep, n_lines, (const int2*)ranges, nu_min, step, n_nu,
+                                               tile_samples, (int)chunks, cp, cutoff, l1_work);
   if (flags & LBL_DETERMINISTIC) {
     constexpr int dyn_bytes = 3 * MJ_NB * (int)sizeof(float);   // near-item buffer
     int dev = 0;
@@ -568,13 +755,13 @@ extern "C" int lbl_jacobian_ml_f32(const LineF32* prep, const LineJac* jprep, in
         return lbl_check_launch("lbl_jacobian_ml_f32 (shared memory attribute)");
       attr_set[dev] = 1;
     }
-    jac_ml_kernel<true><<<grid, threads, dyn_bytes, (cudaStream_t)stream>>>(
-        prep, jprep, n_lines, (const int2*)ranges, t_layer, nu_min, step, n_nu, tile_samples, (int)chunks, cutoff,
-        od, d_t, d_v, n_lay, g_tau, vjp_t, vjp_v);
+    jac_ml_kernel<true><<<grid, threads, dyn_bytes, st>>>(
+        prep, jprep, n_lines, (const int2*)ranges, (const int2*)inner, t_layer, nu_min, step, n_nu, tile_samples,
+        (int)chunks, cutoff, l1_work, od, d_t, d_v, n_lay, g_tau, vjp_t, vjp_v);
   } else {
-    jac_ml_kernel<false><<<grid, threads, 0, (cudaStream_t)stream>>>(
-        prep, jprep, n_lines, (const int2*)ranges, t_layer, nu_min, step, n_nu, tile_samples, (int)chunks, cutoff,
-        od, d_t, d_v, n_lay, g_tau, vjp_t, vjp_v);
+    jac_ml_kernel<false><<<grid, threads, 0, st>>>(
+        prep, jprep, n_lines, (const int2*)ranges, (const int2*)inner, t_layer, nu_min, step, n_nu, tile_samples,
+        (int)chunks, cutoff, l1_work, od, d_t, d_v, n_lay, g_tau, vjp_t, vjp_v);
   }
   return lbl_check_launch("lbl_jacobian_ml_f32");
 }
