@@ -87,9 +87,9 @@ __device__ __forceinline__ U3 series5(float x, float y, float r) {
   return o;
 }
 
-// The same series cut after two terms, for |z|^2 >= FAR_Z2 (|p| <= 4e-4, so the dropped
-// terms are below 2e-7 of the kept ones): w = (i/sqrt(pi)) q (1 + p/2),
-// w' = -(i/sqrt(pi)) p (1 + 3p/2).
+// The same series cut after two terms, for |z|^2 >= FAR_Z2 (|p| <= 4e-4; against
+// scipy.special.wofz and w' = -2zw + 2i/sqrt(pi): 1.2e-7 of |w|, 6e-7 of |w'|):
+// w = (i/sqrt(pi)) q (1 + p/2), w' = -(i/sqrt(pi)) p (1 + 3p/2).
 __device__ __forceinline__ U3 series2(float x, float y, float r) {
   const float qr = x * r, qi = -y * r;
   const float pr = qr * qr - qi * qi, pi_ = 2.f * qr * qi;
@@ -100,6 +100,24 @@ __device__ __forceinline__ U3 series2(float x, float y, float r) {
   o.u = -k * (qr * ai + qi * ar);
   o.ux = k * (pr * bi + pi_ * br);
   o.uy = k * (pr * br - pi_ * bi);
+  return o;
+}
+
+// The series cut after three terms, for |z|^2 >= TIER3_Z2 (|p| <= 1/400; measured as
+// above: 3e-8 of |w|, 2.1e-7 of |w'|): P1 = 1 + p/2 + 3p^2/4, P2 = 1 + 3p/2 + 15p^2/4.
+constexpr float TIER3_Z2 = 400.0f;
+__device__ __forceinline__ U3 series3(float x, float y, float r) {
+  const float qr = x * r, qi = -y * r;
+  const float pr = qr * qr - qi * qi, pi_ = 2.f * qr * qi;
+  const float ar = fmaf(0.75f, pr, 0.5f), ai = 0.75f * pi_;            // 1/2 + 3p/4
+  const float a1r = fmaf(ar, pr, -ai * pi_ + 1.0f), a1i = fmaf(ar, pi_, ai * pr);
+  const float br = fmaf(3.75f, pr, 1.5f), bi = 3.75f * pi_;            // 3/2 + 15p/4
+  const float b1r = fmaf(br, pr, -bi * pi_ + 1.0f), b1i = fmaf(br, pi_, bi * pr);
+  const float k = float(INV_SQRT_PI);
+  U3 o;
+  o.u = -k * (qr * a1i + qi * a1r);
+  o.ux = k * (pr * b1i + pi_ * b1r);
+  o.uy = k * (pr * b1r - pi_ * b1i);
   return o;
 }
 
@@ -120,11 +138,11 @@ __device__ __noinline__ U3 near3(float x, float y, float z2) {
     wi = TWO_INV_SQRT_PI * ri;
     if (y < 0.1f) wr += exp(fmin((double)y * y - (double)x * x, 0.0)) * cos(2.0 * x * y);
   } else if (y >= 0.f) {
-    const cpx<double> w = weideman_upper(x, y);
+    const cpx<double> w = weideman_upper_n<LBL_WEIDEMAN28_N>(x, y);
     wr = w.re;
     wi = w.im;
   } else {
-    const cpx<double> wm = weideman_upper(-(double)x, -(double)y);
+    const cpx<double> wm = weideman_upper_n<LBL_WEIDEMAN28_N>(-(double)x, -(double)y);
     const double e = 2.0 * exp((double)y * y - (double)x * x);
     wr = e * cos(2.0 * x * y) - wm.re;
     wi = -e * sin(2.0 * x * y) - wm.im;
@@ -339,7 +357,7 @@ jac_far_kernel(const LineF32* __restrict__ prep, const LineJac* __restrict__ jpr
 }
 
 template <bool DET>
-__global__ void __launch_bounds__(MJ_THREADS, 2)
+__global__ void __launch_bounds__(MJ_THREADS, 3)
 jac_ml_kernel(const LineF32* __restrict__ prep, const LineJac* __restrict__ jprep, int n_lines,
               const int2* __restrict__ ranges, const int2* __restrict__ inner_ranges,
               const double* __restrict__ t_layer, double nu_min, double step, long long n_nu, int tile_samples,
@@ -518,19 +536,37 @@ jac_ml_kernel(const LineF32* __restrict__ prep, const LineJac* __restrict__ jpre
         add3(sum2f, value3(x, R), x, R);
       }
     }
-    // level 3, clamped loop (branch-free)
+    // level 3, clamped loop (branch-free per line). A line whose nearest point of the
+    // warp's sub-chunk has |z|^2 >= TIER3_Z2 (no near point here) takes the three-term
+    // series at every point; the choice is uniform across the warp.
     for (int i = 0; i < n3w; ++i) {
       const JLine R = s2[s_l3[warp][i]];
       const float x0 = fmaf(pf - R.g.x, R.g.y, -R.g.z);
+      const float xl = fmaf((float)w0 - R.g.x, R.g.y, -R.g.z);       // x at the sub-chunk's first point
+      const float xh = fmaf((float)(n_w - 1), R.g.y, xl);            // and at its last (x grows with p)
+      const float xmin = xl > 0.f ? xl : (xh < 0.f ? -xh : 0.f);
+      if (fmaf(xmin, xmin, R.h.y) >= TIER3_Z2) {
 #pragma unroll
-      for (int m = 0; m < P; ++m) {
-        const float x = fmaf((float)m, R.g.y, x0);
-        const U3 v = series5(x, R.h.x, rcp_approx(fmaxf(fmaf(x, x, R.h.y), MID_Z2)));
-        float a3[3] = {acc[0][m], acc[1][m], acc[2][m]};
-        add3(a3, v, x, R);
-        acc[0][m] = a3[0];
-        acc[1][m] = a3[1];
-        acc[2][m] = a3[2];
+        for (int m = 0; m < P; ++m) {
+          const float x = fmaf((float)m, R.g.y, x0);
+          const U3 v = series3(x, R.h.x, rcp_approx(fmaf(x, x, R.h.y)));
+          float a3[3] = {acc[0][m], acc[1][m], acc[2][m]};
+          add3(a3, v, x, R);
+          acc[0][m] = a3[0];
+          acc[1][m] = a3[1];
+          acc[2][m] = a3[2];
+        }
+      } else {
+#pragma unroll
+        for (int m = 0; m < P; ++m) {
+          const float x = fmaf((float)m, R.g.y, x0);
+          const U3 v = series5(x, R.h.x, rcp_approx(fmaxf(fmaf(x, x, R.h.y), MID_Z2)));
+          float a3[3] = {acc[0][m], acc[1][m], acc[2][m]};
+          add3(a3, v, x, R);
+          acc[0][m] = a3[0];
+          acc[1][m] = a3[1];
+          acc[2][m] = a3[2];
+        }
       }
     }
     // level 3, near correction (accurate - clamped) spread over the CTA; x is formed
