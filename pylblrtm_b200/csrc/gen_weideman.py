@@ -8,8 +8,8 @@ Numer. Anal. 31(5):1497-1518: for Im z >= 0,
 
 where a_n are the Fourier coefficients of (L^2 + t^2) exp(-t^2) under the map
 t = L tan(theta/2), obtained here by an FFT on 4N points. Two sets: N = 36 (|w|
-relative error <= 2e-14 for |z| <= 6; the float64 engine and the Jacobians) and
-N = 28 (the float32 multi-level engine's near zone: Re w relative error <= 7e-7
+relative error <= 2e-14 for |z| <= 6; the float64 engine) and
+N = 28 (the near zones of the float32 multi-level engine and its Jacobians: Re w relative error <= 7e-7
 for y >= 1e-4 and <= 1e-8 for y >= 0.01 inside |z|^2 < 36, against
 scipy.special.wofz; float32 rounding of the sums is ~1e-7). Run:
 
