@@ -44,11 +44,12 @@ FLOPS_CHEB_PER_POINT = 144   # 16 + 8 Clenshaw terms for each of levels 1 and 2 
 CPU_SAMPLE = (1000.0, 1000.5)  # sub-window timed on the host (all 60 layers)
 
 
-# DRAM traffic of one tau_ml_kernel launch on the default workload (200k lines, 60 layers,
-# 600-2500 cm^-1), from a single-pass ncu capture of that launch
-# (dram__bytes_read.sum 386.22 MB + dram__bytes_write.sum 419.19 MB): the 384 MB of line
-# records read once and the 456 MB optical-depth output, part of which stays in L2.
-TAU_ML_DRAM_BYTES = 386.22e6 + 419.19e6
+# DRAM traffic of one lbl_tau_tiles_ml_f32 call on the default workload (200k lines, 60
+# layers, 600-2500 cm^-1), from a single-pass ncu capture of its two launches:
+# tau_far_kernel 386.88 MB read + 9.25 MB written, tau_ml_kernel 398.33 MB read + 411.22 MB
+# written. Each kernel reads the 384 MB of line records once; tau_ml_kernel writes the 456 MB
+# optical depth, part of which stays in L2.
+TAU_ML_DRAM_BYTES = 386.88e6 + 9.25e6 + 398.33e6 + 411.22e6
 
 
 def parse():
@@ -485,11 +486,12 @@ def main():
                      "frac": achieved / peak,
                      "traffic": TAU_ML_DRAM_BYTES if (a.precision == "fp32" and (a.nu_min, a.nu_max) ==
                                                       (600.0, 2500.0)) else None,
-                     "traffic_unit": "bytes per launch (ncu dram__bytes_read.sum + dram__bytes_write.sum)",
+                     "traffic_unit": "bytes per call of both kernels (ncu dram__bytes_read.sum + dram__bytes_write.sum)",
                      "algorithmic_bytes": r0_lines_bytes + job.n_prof * job.n_lay * grid.n_nu * 4,
                      "algorithmic_bytes_rule": "32-B prepared line record per (layer, line) read once + "
                                                "float32 od written once per (layer, point)",
-                     "kernel": {"fp32": "tau_ml_kernel", "fp32-direct": "tau_f32_kernel",
+                     "kernel": {"fp32": "tau_far_kernel + tau_ml_kernel<0> (one lbl_tau_tiles_ml_f32 call)",
+                                "fp32-direct": "tau_f32_kernel",
                                 "fp64": "tau_f64_kernel"}[a.precision],
                      "faddeeva_evals_per_launch": work_per_step,
                      "kernel_ms": tau_avg,
