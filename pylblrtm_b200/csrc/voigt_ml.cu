@@ -11,7 +11,7 @@
 //           chunk, so it is evaluated at K1 = 16 Chebyshev nodes and interpolated
 //           (interpolation error ~rho^-16 ~ 1e-9 of the level-1 sum; lines more than
 //           six half-widths out use 8 nodes). A separate kernel (tau_far_kernel)
-//           computes this level and writes its interpolant into od;
+//           computes this level and hands its coefficients over through od;
 //  level 2  the other lines farther than one sub-chunk half-width from a warp's
 //           256-point sub-chunk: 16 Chebyshev nodes per sub-chunk, same geometry
 //           (8 beyond six sub-chunk half-widths);
