@@ -319,30 +319,50 @@ class Job:
         span = (self.nu_last - self.nu_first + 2 * self.cutoff) / grid.step + 2 * grid.n_nu
         if not math.isfinite(span) or span > 1.5e9:
             raise ValueError("grid index range exceeds the engine's 32-bit line index")
-        up = self._up
-        dev = self.dev
-        if layers.levels_p is not None:
-            self.lv = (up(layers.levels_p, np.float64), up(layers.levels_t, np.float64),
-                       up(layers.levels_vmr, np.float64))
-            self.lay = None
-        else:
-            self.lv = None
-            self.lay = (up(layers.layer_p, np.float64), up(layers.layer_t, np.float64),
-                        up(layers.layer_vmr, np.float64), up(layers.layer_col, np.float64))
+        # the small inputs go up together: one page-locked buffer, one copy, typed views
         gas_index = {g: i for i, g in enumerate(layers.gases)}
         offs = np.cumsum([0] + [g.tips_t.size for g in self.groups[:-1]])
-        self.grp = (up([gas_index[g.gas] for g in self.groups], np.int32),
-                    up([g.molar_mass for g in self.groups], np.float64),
-                    up(offs, np.int32), up([g.tips_t.size for g in self.groups], np.int32),
-                    up(np.concatenate([g.tips_t for g in self.groups]), np.float64),
-                    up(np.concatenate([g.tips_q for g in self.groups]), np.float64))
-        self.gid = up(gid, np.int32)
+        if layers.levels_p is not None:
+            lay = [(layers.levels_p, np.float64), (layers.levels_t, np.float64), (layers.levels_vmr, np.float64)]
+        else:
+            lay = [(layers.layer_p, np.float64), (layers.layer_t, np.float64), (layers.layer_vmr, np.float64),
+                   (layers.layer_col, np.float64)]
+        grp = [([gas_index[g.gas] for g in self.groups], np.int32), ([g.molar_mass for g in self.groups], np.float64),
+               (offs, np.int32), ([g.tips_t.size for g in self.groups], np.int32),
+               (np.concatenate([g.tips_t for g in self.groups]), np.float64),
+               (np.concatenate([g.tips_q for g in self.groups]), np.float64)]
+        views = self._up_packed(lay + grp + [(gid, np.int32)])
+        if layers.levels_p is not None:
+            self.lv, self.lay = tuple(views[:3]), None
+        else:
+            self.lv, self.lay = None, tuple(views[:4])
+        self.grp = tuple(views[len(lay):len(lay) + 6])
+        self.gid = views[-1]
         self.pad = float(st["max_abs_shift"]) * self.p_max * (1 + 1e-9) + 1e-9
 
     def _up(self, a, dtype, non_blocking: bool = False):
         t = _upload(self.torch, a, dtype, self.dev, non_blocking)
         self.h2d_bytes += t.numel() * t.element_size()
         return t
+
+    def _up_packed(self, items):
+        """Upload [(array, dtype), ...] through one page-locked buffer and one asynchronous
+        copy; returns contiguous device tensors (views of one allocation, 256-B aligned)."""
+        torch = self.torch
+        arrs = [np.ascontiguousarray(a, dtype=dt) for a, dt in items]
+        offs, total = [], 0
+        for a in arrs:
+            offs.append(total)
+            total += -(-max(a.nbytes, 1) // 256) * 256
+        host = torch.empty(total, dtype=torch.uint8, pin_memory=True)
+        hb = host.numpy()
+        for a, o in zip(arrs, offs):
+            hb[o:o + a.nbytes] = a.reshape(-1).view(np.uint8)
+        dev = torch.empty(total, dtype=torch.uint8, device=self.dev)
+        dev.copy_(host, non_blocking=True)        # the caching host allocator keeps host alive until done
+        self.h2d_bytes += sum(a.nbytes for a in arrs)
+        tdt = {np.dtype(np.float64): torch.float64, np.dtype(np.int32): torch.int32}
+        return [dev[o:o + a.nbytes].view(tdt[a.dtype]).reshape(a.shape) for a, o in zip(arrs, offs)]
 
     def _device_lines(self, stream):
         """Layers, per-(layer, group) records, band mask + sort, gather and tile ranges.
