@@ -201,11 +201,19 @@ int lbl_tau_tiles_ml_f32(const LineF32* prep, int n_lines, const int* ranges, co
  * Level 1 runs first as a line-per-thread kernel that leaves its Chebyshev
  * coefficients in l1_work (lbl_jacobian_ml_work_floats floats, required); inner
  * (nullable) are the ranges of lbl_ml_inner_ranges for the same grid, a superset of
- * the inner lines of this kernel's smaller chunks. */
+ * the inner lines of this kernel's smaller chunks; near (nullable) those of
+ * lbl_jac_near_ranges, which limit the level-1 pass over lines within six chunk
+ * half-widths. NULL scans every candidate (same results, slower). */
 int lbl_jacobian_ml_f32(const LineF32* prep, const LineJac* jprep, int n_lines, const int* ranges, const int* inner,
-                        const double* t_layer, int n_rows, int n_lay, double nu_min, double step, long long n_nu,
+                        const int* near, const double* t_layer, int n_rows, int n_lay, double nu_min, double step, long long n_nu,
                         int tile_samples, double cutoff, float* l1_work, float* od, float* d_t, float* d_v,
                         const double* g_tau, double* vjp_t, double* vjp_v, int flags, void* stream);
+
+/* Per-tile candidate range [near[2t], near[2t+1]) of the level-1 lines of
+ * lbl_jacobian_ml_f32 that lie within six chunk half-widths of a chunk (same search as
+ * lbl_tile_ranges, pad as there). No reference counterpart: an index of the summation. */
+int lbl_jac_near_ranges(const LineIn* lines, const int* n_kept, double nu_min, double step, long long n_nu,
+                        int tile_samples, double pad, int n_tiles, int* near, void* stream);
 
 /* Floats of the l1_work buffer lbl_jacobian_ml_f32 needs (level-1 Chebyshev
  * coefficients per chunk and row); -1 for bad arguments. */

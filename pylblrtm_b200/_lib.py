@@ -48,8 +48,9 @@ SIGNATURES = {
     "lbl_ml_inner_ranges": (_I, [_P, _P, _D, _D, _L, _I, _D, _I, _P, _P]),
     "lbl_tau_tiles_ml_f32": (_I, [_P, _I, _P, _P, _P, _I, _D, _D, _L, _I, _D, _I, _P, _P, _P, _P, _I, _I, _I, _P]),
     "lbl_line_prep_jac": (_I, [_P, _I, _P, _I, _I, _P, _P, _P, _P, _I, _P, _P, _P]),
-    "lbl_jacobian_ml_f32": (_I, [_P, _P, _I, _P, _P, _P, _I, _I, _D, _D, _L, _I, _D, _P, _P, _P, _P, _P, _P, _P,
-                                 _I, _P]),
+    "lbl_jacobian_ml_f32": (_I, [_P, _P, _I, _P, _P, _P, _P, _I, _I, _D, _D, _L, _I, _D, _P, _P, _P, _P, _P, _P,
+                                 _P, _I, _P]),
+    "lbl_jac_near_ranges": (_I, [_P, _P, _D, _D, _L, _I, _D, _I, _P, _P]),
     "lbl_jacobian_ml_work_floats": (_L, [_I, _L, _I]),
     "lbl_layer_sum_exp_f32": (_I, [_P, _I, _I, _L, _P, _P, _P, _P]),
     "lbl_layer_sum_exp_f64": (_I, [_P, _I, _I, _L, _P, _P, _P, _P]),

@@ -304,8 +304,9 @@ __device__ __forceinline__ void jfar_pass(JFarLine (*s_line)[MJF_THREADS], const
 
 __global__ void __launch_bounds__(MJF_THREADS, 2)
 jac_far_kernel(const LineF32* __restrict__ prep, const LineJac* __restrict__ jprep, int n_lines,
-               const int2* __restrict__ ranges, double nu_min, double step, long long n_nu, int tile_samples,
-               int chunks_per_tile, int chunk_pts, double cutoff, float* __restrict__ l1_coef) {
+               const int2* __restrict__ ranges, const int2* __restrict__ near_ranges, double nu_min, double step,
+               long long n_nu, int tile_samples, int chunks_per_tile, int chunk_pts, double cutoff,
+               float* __restrict__ l1_coef) {
   __shared__ __align__(16) JFarLine s_line[MJF_STAGES][MJF_THREADS];   // records 64 B, 16-B aligned
   __shared__ double s_part[MJF_THREADS / 32][MJ_NCOEF];                 // [q][16] then [q][8] per warp
 
@@ -332,7 +333,14 @@ jac_far_kernel(const LineF32* __restrict__ prep, const LineJac* __restrict__ jpr
   for (int k = 0; k < MJ_K / 2; ++k) xa[k] = H1 * c_jnode16[k];
 #pragma unroll
   for (int k = 0; k < MJ_KF / 2; ++k) xb[k] = H1 * c_jnode8[k];
-  jfar_pass<MJ_K>(s_line, lp, jp, rng, wlo, whi, c0, H1, xa, s_part[warp]);
+  // the 16-node class lies within six half-widths of the chunk: its pass reads only the
+  // tile's near range (lbl_jac_near_ranges) when one is given
+  int2 rng16 = rng;
+  if (near_ranges) {
+    const int2 q = near_ranges[tile];
+    rng16 = make_int2(max(rng.x, q.x), min(rng.y, q.y));
+  }
+  jfar_pass<MJ_K>(s_line, lp, jp, rng16, wlo, whi, c0, H1, xa, s_part[warp]);
   jfar_pass<MJ_KF>(s_line, lp, jp, rng, wlo, whi, c0, H1, xb, s_part[warp] + 3 * MJ_K);
   __syncthreads();
   if (tid < MJ_NCOEF) {                                    // column tid: only this thread touches it
@@ -761,8 +769,23 @@ extern "C" long long lbl_jacobian_ml_work_floats(int n_rows, long long n_nu, int
   return (long long)n_rows * n_tiles * chunks * MJ_NCOEF;
 }
 
+extern "C" int lbl_jac_near_ranges(const LineIn* lines, const int* n_kept, double nu_min, double step, long long n_nu,
+                                   int tile_samples, double pad, int n_tiles, int* near, void* stream) {
+  if (tile_samples < 1 || !(step > 0) || n_nu < 1)
+    return lbl_set_error(LBL_EINVAL, "lbl_jac_near_ranges: bad arguments");
+  // A 16-node level-1 line of a chunk (half-width H) has |j0 - centre| <= 6H, so its centre
+  // lies within 5H + 1.5 grid steps of the chunk; chunks lie inside their tile and have at
+  // most min(tile_samples, chunk size) points. Two further steps absorb rounding.
+  int threads, cp;
+  long long n_all, chunks;
+  jac_geometry(tile_samples, n_nu, &threads, &cp, &n_all, &chunks);
+  const int n_c_max = tile_samples < cp ? tile_samples : cp;
+  const double reach = (2.5 * (n_c_max - 1) + 3.5) * step;
+  return lbl_tile_ranges(lines, n_kept, nu_min, step, n_nu, tile_samples, reach, pad, n_tiles, near, stream);
+}
+
 extern "C" int lbl_jacobian_ml_f32(const LineF32* prep, const LineJac* jprep, int n_lines, const int* ranges,
-                                   const int* inner, const double* t_layer, int n_rows, int n_lay, double nu_min,
+                                   const int* inner, const int* near, const double* t_layer, int n_rows, int n_lay, double nu_min,
                                    double step, long long n_nu, int tile_samples, double cutoff, float* l1_work,
                                    float* od, float* d_t, float* d_v, const double* g_tau, double* vjp_t,
                                    double* vjp_v, int flags, void* stream) {
@@ -777,8 +800,8 @@ extern "C" int lbl_jacobian_ml_f32(const LineF32* prep, const LineJac* jprep, in
   if (n_tiles * chunks > 0x7fffffffLL) return lbl_set_error(LBL_EINVAL, "lbl_jacobian_ml_f32: grid too large");
   dim3 grid((unsigned)(n_tiles * chunks), (unsigned)n_rows);
   cudaStream_t st = (cudaStream_t)stream;
-  jac_far_kernel<<<grid, MJF_THREADS, 0, st>>>(prep, jprep, n_lines, (const int2*)ranges, nu_min, step, n_nu,
-                                               tile_samples, (int)chunks, cp, cutoff, l1_work);
+  jac_far_kernel<<<grid, MJF_THREADS, 0, st>>>(prep, jprep, n_lines, (const int2*)ranges, (const int2*)near, nu_min,
+                                               step, n_nu, tile_samples, (int)chunks, cp, cutoff, l1_work);
   if (flags & LBL_DETERMINISTIC) {
     constexpr int dyn_bytes = 3 * MJ_NB * (int)sizeof(float);   // near-item buffer
     int dev = 0;

@@ -614,11 +614,15 @@ def _jacobian_impl(job: Job, gas: str, g_tau=None, deterministic: bool = False):
     inner = torch.empty_like(ranges)
     _lib.call("lbl_ml_inner_ranges", lines.data_ptr(), job._kept.data_ptr(), grid.nu_min, grid.step, n_nu,
               grid.tile_samples, job.pad, ranges.shape[0], inner.data_ptr(), stream)
+    near = torch.empty_like(ranges)         # level-1 lines within six chunk half-widths
+    _lib.call("lbl_jac_near_ranges", lines.data_ptr(), job._kept.data_ptr(), grid.nu_min, grid.step, n_nu,
+              grid.tile_samples, job.pad, ranges.shape[0], near.data_ptr(), stream)
     l1_work = torch.empty((_lib.load().lbl_jacobian_ml_work_floats(n_rows, n_nu, grid.tile_samples),),
                           dtype=torch.float32, device=dev)
-    job.launches += 2                       # the inner ranges and the Jacobian's level-1 kernel
-    common = (prep.data_ptr(), jprep.data_ptr(), n_kept, ranges.data_ptr(), inner.data_ptr(), t_lay.data_ptr(),
-              n_rows, n_lay, grid.nu_min, grid.step, n_nu, grid.tile_samples, job.cutoff, l1_work.data_ptr())
+    job.launches += 3                       # the two range searches and the Jacobian's level-1 kernel
+    common = (prep.data_ptr(), jprep.data_ptr(), n_kept, ranges.data_ptr(), inner.data_ptr(), near.data_ptr(),
+              t_lay.data_ptr(), n_rows, n_lay, grid.nu_min, grid.step, n_nu, grid.tile_samples, job.cutoff,
+              l1_work.data_ptr())
     if g_tau is not None:
         g = torch.as_tensor(g_tau).to(device=dev, dtype=torch.float64).reshape(n_prof, n_nu).contiguous()
         vt = torch.zeros((n_prof, n_lay), dtype=torch.float64, device=dev)

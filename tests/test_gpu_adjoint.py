@@ -148,3 +148,34 @@ def test_batched_jacobians_match_single_profiles_and_stream(cuda):
         adjoint.layer_jacobians_batch(sd, lv["p"], lv["t"], vmr, lo, hi, gas="CH4")
     with pytest.raises(ValueError, match="mu_view"):
         adjoint.layer_jacobians_batch(sd, lv["p"], lv["t"], vmr, lo, hi, mu_view=1.5)
+
+
+@pytest.mark.parametrize("tile", [2.0, 5.0, 0.05, 0.3])
+def test_jacobian_ranges_select_every_line(cuda, tile, monkeypatch):
+    """Jacobians computed with the inner-line and near level-1 ranges equal, to float
+    rounding, those of a scan of every candidate line (inner = near = NULL), with pressure
+    shifts 40x the synthetic ones; tiles of one chunk, several chunks and below level 1's
+    minimum size. A line lost by a range would change whole line profiles."""
+    from pylblrtm_b200 import _lib
+    sd = synthetic.restrict(synthetic.three_gas_lines(20000, 1490.0, 1520.0, seed=4), 1490.0, 1520.0)
+    lines = {k: v.copy() for k, v in sd.lines.items()}
+    lines["shift"] = lines["shift"] * 40.0
+    sd = SpectralData(lines, dict(sd.tips), dict(sd.molar_masses), sd.molecule)
+    lv = synthetic.perturbed_levels(synthetic.logp_levels(7), 2, seed=8)
+    gases = ["H2O", "CO2", "O3"]
+    li = engine.LayerInput(gases=gases, levels_p=lv["p"], levels_t=lv["t"],
+                           levels_vmr=np.stack([lv[g] for g in gases], axis=1))
+    job = engine.Job(sd, li, engine.make_grid(1500.0, 1510.3, 0.001, tile), 5.0)
+    with_ranges = job.jacobian("H2O", deterministic=True)
+    real_call = _lib.call
+
+    def scan_all(name, *args):
+        if name == "lbl_jacobian_ml_f32":
+            args = args[:4] + (0, 0) + args[6:]
+        return real_call(name, *args)
+
+    monkeypatch.setattr(_lib, "call", scan_all)
+    every = job.jacobian("H2O", deterministic=True)
+    for a, b in zip(with_ranges, every):
+        scale = b.abs().amax(dim=-1, keepdim=True).clamp_min(1e-30)
+        assert ((a - b).abs() / scale).max().item() <= 1e-6
