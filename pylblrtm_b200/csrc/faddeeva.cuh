@@ -180,7 +180,7 @@ LBL_HD cpx<T> faddeeva(T x, T y) {
 // (weideman_re reflects w(z) = 2 exp(-z^2) - w(-z) below the real axis). Fixed cost
 // and no data-dependent loop. N = 36: |w| relative error <= 2e-14 for |z| <= 6
 // against scipy.special.wofz; N = 28 below (coefficients: gen_weideman.py).
-template <int N>
+template <int N, bool HORNER = false>
 LBL_HD cpx<double> weideman_upper_n(double x, double y) {
   static_assert(N == LBL_WEIDEMAN_N || N == LBL_WEIDEMAN28_N, "coefficient set");
   constexpr double L = N == LBL_WEIDEMAN_N ? LBL_WEIDEMAN_L : LBL_WEIDEMAN28_L;
@@ -200,15 +200,29 @@ LBL_HD cpx<double> weideman_upper_n(double x, double y) {
   // leaves a linear remainder, which equals p at Z0; its recurrence
   // b_k = a_k + 2 Re(Z) b_{k+1} - |Z|^2 b_{k+2} costs 2 multiply-adds per coefficient where
   // complex Horner costs 4 (as accurate here: the error is the approximation's own).
-  const double t2 = 2.0 * zr, s2 = zr * zr + zi * zi;
-  double b1 = 0.0, b2 = 0.0;
+  // HORNER selects complex Horner instead (4 per term, fewer live registers).
+  double pr, pi;
+  if constexpr (HORNER) {
+    pr = a[N - 1];
+    pi = 0.0;
 #pragma unroll
-  for (int k = N - 1; k >= 1; --k) {
-    const double b0 = fma(-s2, b2, fma(t2, b1, a[k]));
-    b2 = b1;
-    b1 = b0;
+    for (int k = N - 2; k >= 0; --k) {
+      const double tr = pr * zr - pi * zi + a[k];
+      pi = pr * zi + pi * zr;
+      pr = tr;
+    }
+  } else {
+    const double t2 = 2.0 * zr, s2 = zr * zr + zi * zi;
+    double b1 = 0.0, b2 = 0.0;
+#pragma unroll
+    for (int k = N - 1; k >= 1; --k) {
+      const double b0 = fma(-s2, b2, fma(t2, b1, a[k]));
+      b2 = b1;
+      b1 = b0;
+    }
+    pr = fma(zr, b1, fma(-s2, b2, a[0]));
+    pi = zi * b1;
   }
-  const double pr = fma(zr, b1, fma(-s2, b2, a[0])), pi = zi * b1;
   const double er = dr * inv, ei = -di * inv;           // 1 / (L - iz)
   const double e2r = er * er - ei * ei, e2i = 2.0 * er * ei;
   cpx<double> w;
@@ -219,10 +233,10 @@ LBL_HD cpx<double> weideman_upper_n(double x, double y) {
 
 LBL_HD cpx<double> weideman_upper(double x, double y) { return weideman_upper_n<LBL_WEIDEMAN_N>(x, y); }
 
-template <int N = LBL_WEIDEMAN_N>
+template <int N = LBL_WEIDEMAN_N, bool HORNER = false>
 LBL_HD double weideman_re(double x, double y) {
-  if (y >= 0.0) return weideman_upper_n<N>(x, y).re;
-  const cpx<double> wm = weideman_upper_n<N>(-x, -y);
+  if (y >= 0.0) return weideman_upper_n<N, HORNER>(x, y).re;
+  const cpx<double> wm = weideman_upper_n<N, HORNER>(-x, -y);
   return 2.0 * exp(y * y - x * x) * cos(2.0 * x * y) - wm.re;
 }
 
@@ -230,6 +244,8 @@ LBL_HD double weideman_re(double x, double y) {
 // (Re w relative error <= 7e-7 for y >= 1e-4, <= 1e-8 for y >= 0.01), a quarter
 // fewer float64 steps than the 36-term set.
 LBL_HD double weideman_re_f32(double x, double y) { return weideman_re<LBL_WEIDEMAN28_N>(x, y); }
+// The same by complex Horner, for rarely taken paths of kernels at their register limit.
+LBL_HD double weideman_re_f32_compact(double x, double y) { return weideman_re<LBL_WEIDEMAN28_N, true>(x, y); }
 
 // |z|^2 below which the engine evaluates Re w in double precision (Weideman's
 // approximation): inside it a float complex evaluation loses relative accuracy

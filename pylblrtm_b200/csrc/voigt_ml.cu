@@ -159,7 +159,7 @@ static __device__ __noinline__ float far_node_general(float x, float y, float y2
     return amp_far * r * fmaf(fmaf(-2.0f * y2, r, 1.5f), r, 1.0f);
   }
   if (z2 >= CORE_Z2 && y >= 0.f) return amp * re_w_f32_mid(x, y, y2, z2);
-  return (float)((double)amp * weideman_re_f32((double)x, (double)y));
+  return (float)((double)amp * weideman_re_f32_compact((double)x, (double)y));
 }
 
 // Node sums of one level-1 line: nodes k and K-1-k sit at +xs[k] and -xs[k] from the chunk centre.
