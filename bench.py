@@ -46,10 +46,10 @@ CPU_SAMPLE = (1000.0, 1000.5)  # sub-window timed on the host (all 60 layers)
 
 # DRAM traffic of one lbl_tau_tiles_ml_f32 call on the default workload (200k lines, 60
 # layers, 600-2500 cm^-1), from a single-pass ncu capture of its two launches:
-# tau_far_kernel 386.88 MB read + 9.25 MB written, tau_ml_kernel 398.33 MB read + 411.22 MB
+# tau_far_kernel 386.85 MB read + 9.53 MB written, tau_ml_kernel 397.28 MB read + 410.90 MB
 # written. Each kernel reads the 384 MB of line records once; tau_ml_kernel writes the 456 MB
 # optical depth, part of which stays in L2.
-TAU_ML_DRAM_BYTES = 386.88e6 + 9.25e6 + 398.33e6 + 411.22e6
+TAU_ML_DRAM_BYTES = 386.85e6 + 9.53e6 + 397.28e6 + 410.90e6
 
 
 def parse():
