@@ -78,6 +78,18 @@ def test_host_queries_and_argument_errors():
         _lib.call("lbl_tau_tiles_f32", 0, 0, 0, 0, 0, 700.0, 0.001, 10, 2000, 25.0, 1, 0, 0, 0, 0)
     with pytest.raises(RuntimeError, match="bad arguments"):
         _lib.call("lbl_faddeeva_f32", 0, 0, 5, 0, 0, 3, 0)
+    # Jacobian level-1 workspace: 3 x (16 + 8) coefficients per chunk and row; chunks of at
+    # most 1,024 points, so a 2,000-point tile has two and a 5,000-point tile five
+    assert lib.lbl_jacobian_ml_work_floats(60, 200001, 2000) == 60 * 101 * 2 * 72
+    assert lib.lbl_jacobian_ml_work_floats(2, 10000, 5000) == 2 * 2 * 5 * 72
+    assert lib.lbl_jacobian_ml_work_floats(1, 100, 50) == 2 * 72
+    assert lib.lbl_jacobian_ml_work_floats(0, 100, 50) == -1
+    for name in ("lbl_ml_inner_ranges", "lbl_jac_near_ranges"):
+        with pytest.raises(RuntimeError, match="bad arguments"):
+            _lib.call(name, 0, 0, 700.0, 0.0, 10, 2000, 0.0, 1, 0, 0)
+    with pytest.raises(RuntimeError, match="bad arguments"):     # no level-1 workspace
+        _lib.call("lbl_jacobian_ml_f32", 1, 1, 10, 1, 0, 0, 1, 60, 60, 700.0, 0.001, 100, 50, 25.0, 0,
+                  1, 1, 1, 0, 0, 0, 0, 0)
 
 
 def test_engine_without_cuda_raises():
