@@ -369,7 +369,8 @@ tau_ml_kernel(const LineF32* __restrict__ prep, int n_lines, const int2* __restr
   if (use_l1 && tid < ML_K + ML_KF) s_c1[tid] = od[(long long)row * out_stride + (c0 - out_first) + tid];
 
   // level-3 sums hold only the lines within ~2 sub-chunk widths (tens of terms), so
-  // plain float accumulation suffices; the long node sums use Kahan compensation.
+  // plain float accumulation suffices; the 16-node level-2 sums are Kahan-compensated
+  // across rounds, the 8-node ones (far lines, smaller terms) are plain float.
   float acc[P];
 #pragma unroll
   for (int m = 0; m < P; ++m) acc[m] = 0.f;
