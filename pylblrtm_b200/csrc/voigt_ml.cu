@@ -321,9 +321,16 @@ tau_ml_kernel(const LineF32* __restrict__ prep, int n_lines, const int2* __restr
   __shared__ unsigned char s_l2[ML_THREADS / 32][ML_THREADS];   // per-warp level-2 slots
   __shared__ unsigned char s_l3[ML_THREADS / 32][ML_THREADS];   // per-warp level-3 slots
   __shared__ unsigned char s_nl[ML_THREADS / 32][ML_THREADS];   // per-warp slots with near points in it
-  __shared__ int s_cnt[2][ML_THREADS / 32];
-  __shared__ int s_seg_start[ML_THREADS + 1];       // near-item prefix per inner slot
-  __shared__ short s_seg_lo[ML_THREADS];            // first near point per inner slot
+  __shared__ int s_cnt[3][ML_THREADS / 32];
+  __shared__ int s_seg_start[ML_THREADS + 1];       // near-item prefix per inner slot (default: middles)
+  __shared__ short s_seg_lo[ML_THREADS];            // first near point per inner slot (default: of the middle)
+  // default mode: the near zone of a slot is split into its middle (|z|^2 < CORE_Z2, the
+  // float64 core) and its two tails (the float continued fraction), each kind in an item
+  // space of its own, so that a warp's consecutive items take the same branch
+  __shared__ int s_segc_start[ML_THREADS + 1];      // tail-item prefix per inner slot
+  __shared__ short s_segc_lo[ML_THREADS];           // first point of the left tail
+  __shared__ short s_segc_nl[ML_THREADS];           // points in the left tail
+  __shared__ short s_segc_rlo[ML_THREADS];          // first point of the right tail
   __shared__ unsigned char s_seg_mask[ML_THREADS];  // warps treating the inner line directly (level 3)
   __shared__ float s_core[ML_CHUNK];               // near-zone corrections (each point owned by one thread)
   __shared__ float s_nbuf[ML_NB];                   // near-item values of one batch
@@ -415,23 +422,49 @@ tau_ml_kernel(const LineF32* __restrict__ prep, int n_lines, const int2* __restr
         near_n = (int)hi_f - near_lo + 1;
       }
     }
-    int near_scan = near_n;                                  // inclusive warp scan
+    // default mode: the middle [mid_lo, mid_lo + mid_n) of the near range, where |z|^2 may be
+    // below CORE_Z2 (one point of margin; each item still picks its formula from its own |z|^2)
+    int mid_lo = near_lo, mid_n = 0;
+    if constexpr (!DET) {
+      if (near_n > 0 && y2 < CORE_Z2 && L.y >= 0.f) {
+        const float hw36 = sqrtf(CORE_Z2 - y2) / L.a + 1.0f;
+        const float q = jf + L.b / L.a;
+        const float a0 = fmaxf(ceilf(q - hw36), (float)near_lo);           // clamped before the
+        const float a1 = fminf(floorf(q + hw36), (float)(near_lo + near_n - 1));   // int conversion
+        if (a0 <= a1) {
+          mid_lo = (int)a0;
+          mid_n = (int)a1 - mid_lo + 1;
+        }
+      }
+    }
+    const int tail_n = near_n - mid_n;
+    // inclusive warp scans: DET the whole near range; default the middles and the tails
+    int near_scan = DET ? near_n : mid_n, tail_scan = tail_n;
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
       const int t = __shfl_up_sync(0xffffffffu, near_scan, o);
-      if (lane >= o) near_scan += t;
+      const int u = __shfl_up_sync(0xffffffffu, tail_scan, o);
+      if (lane >= o) {
+        near_scan += t;
+        tail_scan += u;
+      }
     }
     const unsigned b2 = __ballot_sync(0xffffffffu, inner);
     if (lane == 0) s_cnt[0][warp] = __popc(b2);
-    if (lane == 31) s_cnt[1][warp] = near_scan;
+    if (lane == 31) {
+      s_cnt[1][warp] = near_scan;
+      s_cnt[2][warp] = tail_scan;
+    }
     __syncthreads();
-    int off2 = 0, off3 = 0, n2 = 0, n_near = 0;
+    int off2 = 0, off3 = 0, offc = 0, n2 = 0, n_near = 0, n_tail = 0;
     for (int w = 0; w < n_warps; ++w) {
-      const int a2 = s_cnt[0][w], a3 = s_cnt[1][w];
+      const int a2 = s_cnt[0][w], a3 = s_cnt[1][w], a4 = s_cnt[2][w];
       off2 += (w < warp) ? a2 : 0;
       off3 += (w < warp) ? a3 : 0;
+      offc += (w < warp) ? a4 : 0;
       n2 += a2;
       n_near += a3;
+      n_tail += a4;
     }
     if (inner) {
       MlLine r;
@@ -441,11 +474,23 @@ tau_ml_kernel(const LineF32* __restrict__ prep, int n_lines, const int2* __restr
       r.h = make_float4(L.y, y2, L.amp, rc * asym5_scaled(rc, r));
       const int slot = off2 + __popc(b2 & ((1u << lane) - 1u));
       s2[slot] = r;
-      s_seg_start[slot] = off3 + near_scan - near_n;         // exclusive prefix in slot order
-      s_seg_lo[slot] = (short)near_lo;
       s_seg_mask[slot] = (unsigned char)l3mask;
+      if constexpr (DET) {
+        s_seg_start[slot] = off3 + near_scan - near_n;       // exclusive prefix in slot order
+        s_seg_lo[slot] = (short)near_lo;
+      } else {
+        s_seg_start[slot] = off3 + near_scan - mid_n;
+        s_seg_lo[slot] = (short)mid_lo;
+        s_segc_start[slot] = offc + tail_scan - tail_n;
+        s_segc_lo[slot] = (short)near_lo;
+        s_segc_nl[slot] = (short)(mid_n > 0 ? mid_lo - near_lo : tail_n);
+        s_segc_rlo[slot] = (short)(mid_lo + mid_n);
+      }
     }
-    if (tid == 0) s_seg_start[n2] = n_near;
+    if (tid == 0) {
+      s_seg_start[n2] = n_near;
+      if constexpr (!DET) s_segc_start[n2] = n_tail;
+    }
     __syncthreads();
     n_pass += (unsigned long long)n2;
 
@@ -521,23 +566,35 @@ tau_ml_kernel(const LineF32* __restrict__ prep, int n_lines, const int2* __restr
     // zones of several lines overlap, the shared-memory atomics add in scheduling
     // order (results reproducible to rounding, ~1e-9 relative).
     if constexpr (!DET) {
+      auto near_item = [&](int l, int p) {
+        if (!((s_seg_mask[l] >> (p >> 8)) & 1u)) return;   // level 2 for the owning warp
+        const MlLine R = s2[l];
+        const float x0 = fmaf((float)(p & ~(P - 1)) - R.g.x, R.g.y, -R.g.z);
+        const float x = fmaf((float)(p & (P - 1)), R.g.y, x0);
+        const float z2 = fmaf(x, x, R.h.y);
+        if (z2 >= MID_Z2) return;
+        float v;
+        if (z2 >= CORE_Z2 && R.h.x >= 0.f) v = R.h.z * re_w_cf32(x, R.h.x, z2);
+        else v = (float)((double)R.h.z * weideman_re_f32((double)x, (double)R.h.x));
+        atomicAdd(&s_core[p], v - R.h.w);
+      };
+      // the middles (float64 core), then the tails (continued fraction)
       for (int i = tid; i < n_near; i += blockDim.x) {
         int l = 0, hi = n2;                               // largest l with s_seg_start[l] <= i
         while (hi - l > 1) {
           const int mid = (l + hi) >> 1;
           if (s_seg_start[mid] <= i) l = mid; else hi = mid;
         }
-        const int p = s_seg_lo[l] + (i - s_seg_start[l]);
-        if (!((s_seg_mask[l] >> (p >> 8)) & 1u)) continue;   // level 2 for the owning warp
-        const MlLine R = s2[l];
-        const float x0 = fmaf((float)(p & ~(P - 1)) - R.g.x, R.g.y, -R.g.z);
-        const float x = fmaf((float)(p & (P - 1)), R.g.y, x0);
-        const float z2 = fmaf(x, x, R.h.y);
-        if (z2 >= MID_Z2) continue;
-        float v;
-        if (z2 >= CORE_Z2 && R.h.x >= 0.f) v = R.h.z * re_w_cf32(x, R.h.x, z2);
-        else v = (float)((double)R.h.z * weideman_re_f32((double)x, (double)R.h.x));
-        atomicAdd(&s_core[p], v - R.h.w);
+        near_item(l, s_seg_lo[l] + (i - s_seg_start[l]));
+      }
+      for (int i = tid; i < n_tail; i += blockDim.x) {
+        int l = 0, hi = n2;                               // largest l with s_segc_start[l] <= i
+        while (hi - l > 1) {
+          const int mid = (l + hi) >> 1;
+          if (s_segc_start[mid] <= i) l = mid; else hi = mid;
+        }
+        const int k = i - s_segc_start[l], nl = s_segc_nl[l];
+        near_item(l, k < nl ? s_segc_lo[l] + k : s_segc_rlo[l] + (k - nl));
       }
     } else {
       // Bit-reproducible variant, in two phases so that the sums do not depend on thread
@@ -583,7 +640,7 @@ tau_ml_kernel(const LineF32* __restrict__ prep, int n_lines, const int2* __restr
         if (nb1 < n_near) __syncthreads();                  // the buffer is refilled
       }
     }
-    if (tid == 0) n_near_items += (unsigned long long)n_near;
+    if (tid == 0) n_near_items += (unsigned long long)(DET ? n_near : n_near + n_tail);
     // No barrier here: the next round writes the staging arrays only after its first
     // barrier, which every warp reaches after finishing this round.
   }
