@@ -10,10 +10,13 @@ levels and line parameters resident in HBM to the transmittance in HBM.
     python bench.py [--gpus N] [--steps K] [--warmup W] [--precision fp32|fp32-direct|fp64]
     python bench.py --impl reference     # the reference's CPU path on this host
 
-Under torchrun each rank computes its own spectrum (rank r uses a profile with
-seeded temperature/H2O perturbations), so per-GPU work is fixed (weak scaling)
-and there is no data-path collective; `value` is all ranks' evaluations divided
-by the slowest rank's time.
+Under torchrun (``--shard wavenumber``, the default for more than one rank) the
+one spectrum is split by reference tiles: rank r computes a contiguous range of
+tiles from only the lines that reach them, and the transmittance pieces are
+all-gathered over NCCL inside every step (strong scaling); `value` is the
+spectrum's evaluations divided by the slowest rank's time. ``--shard replicas``
+instead gives every rank its own spectrum (rank r uses a profile with seeded
+temperature/H2O perturbations; weak scaling, no collective in the step).
 """
 
 from __future__ import annotations
@@ -64,6 +67,9 @@ def parse():
     ap.add_argument("--no-adjoint", action="store_true", help="skip the Jacobian timing")
     ap.add_argument("--no-surrogate", action="store_true", help="skip the gated-surrogate timing")
     ap.add_argument("--no-accuracy", action="store_true", help="skip the accuracy checks")
+    ap.add_argument("--shard", default="auto", choices=["auto", "wavenumber", "replicas"],
+                    help="multi-rank mode (auto: wavenumber for more than one rank)")
+    ap.add_argument("--no-plain", action="store_true", help="skip the float64 / direct float32 timings")
     ap.add_argument("--nu-min", type=float, default=600.0, help="grid start (smaller cases for profiling)")
     ap.add_argument("--nu-max", type=float, default=2500.0, help="grid end (smaller cases for profiling)")
     return ap.parse_args()
@@ -266,30 +272,71 @@ def _errors(torch, t_test, t_ref, tau_test, tau_ref):
             "median_rel_tau": float(rel.median()), "points": int(t_ref.numel())}
 
 
-def accuracy(torch, job):
-    """Accuracy of the engines: the float32 engine against the float64 engine on the full
-    200k-line spectrum, and both against the reference's own outputs (golden vectors made
-    by running the reference) for the 2,000-line CO2 band at full strength (saturated) and
-    x 1e-3."""
+def _timed_ms(torch, fn, reps):
+    """Mean CUDA-event milliseconds of ``reps`` calls of fn (on the current stream)."""
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(reps):
+        fn()
+    e1.record()
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / reps
+
+
+def plain_and_accuracy(torch, job, sd, prof, grid, evals, fp32_value):
+    """The comparison engines and the accuracy of the default one, on the full workload.
+
+    (1) The plain float64 method (every admitted line at every point, Gautschi-type
+    Faddeeva in float64, the reference's ``_voigt``/``phi @ S`` work done directly) and
+    the direct float32 method: line-evals/s from CUDA-event times of whole spectra, and
+    the default engine's ratio to each. (2) The default float32 engine against the
+    float64 engine on the full 200k-line, 60-layer, 1.9M-point spectrum at full
+    strength (saturated: T ~ 0 almost everywhere) and with line strengths x 1e-3 and
+    x 1e-5, where T spans (0, 1) and |dT| tests something. (3) Both engines against the
+    reference's own outputs (golden vectors made by running the reference) for the
+    2,000-line CO2 band at full strength and x 1e-3.
+    """
     from pylblrtm_b200 import engine, synthetic
-    r64 = job.run("fp64", mu=[0.8], want_od=False, want_tau=True, want_trans=True)
-    r32 = job.run("fp32", mu=[0.8], want_od=False, want_tau=True, want_trans=True)
-    out = {"three_gas_200k_fp32_vs_fp64": _errors(torch, r32.trans[0], r64.trans[0], r32.tau[0], r64.tau[0])}
+    out_plain, acc = {}, {}
+    run = lambda j, prec: j.run(prec, mu=[0.8], want_od=False, want_tau=True, want_trans=True)
+    r64 = run(job, "fp64")                                   # also the float64 warm-up
+    ms64 = _timed_ms(torch, lambda: job.run("fp64", mu=[0.8], want_od=False, want_trans=True), 1)
+    out_plain["fp64_plain"] = {"ms_per_spectrum": ms64, "line_evals_per_s": evals / (ms64 * 1e-3), "steps": 1,
+                               "kernel": "tau_f64_kernel (lbl_tau_tiles_f64)"}
+    r32 = run(job, "fp32")
+    acc["three_gas_200k_fp32_vs_fp64"] = _errors(torch, r32.trans[0], r64.trans[0], r32.tau[0], r64.tau[0])
+    rd = run(job, "fp32-direct")                             # also the direct warm-up
+    msd = _timed_ms(torch, lambda: job.run("fp32-direct", mu=[0.8], want_od=False, want_trans=True), 2)
+    out_plain["fp32_direct"] = {"ms_per_spectrum": msd, "line_evals_per_s": evals / (msd * 1e-3), "steps": 2,
+                                "kernel": "tau_f32_kernel (lbl_tau_tiles_f32)"}
+    acc["three_gas_200k_fp32_direct_vs_fp64"] = _errors(torch, rd.trans[0], r64.trans[0], rd.tau[0], r64.tau[0])
+    out_plain["fp32_over_fp64"] = fp32_value / out_plain["fp64_plain"]["line_evals_per_s"]
+    out_plain["fp32_over_direct"] = fp32_value / out_plain["fp32_direct"]["line_evals_per_s"]
+    del r64, r32, rd
+    for scale in (1e-3, 1e-5):
+        js = engine.Job(synthetic.scale_strengths(sd, scale), engine.layer_input_from_profile(prof), grid, 25.0)
+        a64, a32 = run(js, "fp64"), run(js, "fp32")
+        e = _errors(torch, a32.trans[0], a64.trans[0], a32.tau[0], a64.tau[0])
+        e["T_min"], e["T_max"] = float(a64.trans[0].min()), float(a64.trans[0].max())
+        e["points_T_0.01_0.99"] = int(((a64.trans[0] > 0.01) & (a64.trans[0] < 0.99)).sum())
+        acc[f"three_gas_200k_x{scale:g}_fp32_vs_fp64"] = e
+        del js, a64, a32
     gold_dir = os.path.join(os.path.dirname(os.path.abspath(__file__)), "tests", "golden")
     for name, scale in (("co2_band_full", 1.0), ("co2_band_mid", 1e-3)):
         g = np.load(os.path.join(gold_dir, f"{name}.npz"))
-        sd = synthetic.co2_band()
+        sdc = synthetic.co2_band()
         if scale != 1.0:
-            sd = synthetic.scale_strengths(sd, scale)
-        grid = engine.make_grid(float(g["nu_min"]), float(g["nu_max"]), float(g["step"]), float(g["tile"]))
-        j = engine.Job(sd, engine.layer_input_from_profile(synthetic.us_standard_atmosphere(["CO2"])), grid,
+            sdc = synthetic.scale_strengths(sdc, scale)
+        gc = engine.make_grid(float(g["nu_min"]), float(g["nu_max"]), float(g["step"]), float(g["tile"]))
+        j = engine.Job(sdc, engine.layer_input_from_profile(synthetic.us_standard_atmosphere(["CO2"])), gc,
                        float(g["cutoff"]))
         res = {}
         for prec in ("fp32", "fp64"):
             r = j.run(prec, mu=[float(g["mu"])], want_od=False, want_tau=True, want_trans=True)
             res[prec] = _errors(torch, r.trans[0], g["T"], r.tau[0], g["tau"])
-        out[f"{name}_vs_reference"] = res
-    return out
+        acc[f"{name}_vs_reference"] = res
+    return out_plain, acc
 
 
 def surrogate_timing():
@@ -337,6 +384,25 @@ def fp32_peak(torch):
     return blocks * 256 * 8 * iters * 2 / (best * 1e-3) / 1e12
 
 
+def _e2e_leg(torch, barrier, world, steps, warmup, call, h2d, d2h, api):
+    """Times ``call()`` through the public API (copies and the result read-back inside),
+    max over ranks; returns the e2e record without its value."""
+    for _ in range(warmup):        # like the timed loop: each result lives until the next call returns
+        call()
+    barrier()
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        call()
+    barrier()
+    dt = time.perf_counter() - t0
+    if world > 1:
+        import torch.distributed as dist
+        t = torch.tensor([dt], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        dt = float(t.item())
+    return dt, {"unit": UNIT, "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h), "api": api}
+
+
 def main():
     a = parse()
     if a.impl == "reference":
@@ -352,19 +418,51 @@ def main():
     if world > 1:
         import datetime
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    mode = a.shard if a.shard != "auto" else ("wavenumber" if world > 1 else "replicas")
+    if mode == "wavenumber" and a.precision != "fp32":
+        raise SystemExit("--shard wavenumber needs --precision fp32")
 
     import pylblrtm_b200 as lbl
-    from pylblrtm_b200 import engine
+    from pylblrtm_b200 import engine, shard
 
-    sd, prof = workload(rank)
+    sd, prof = workload(rank if mode == "replicas" else 0)
     grid = engine.make_grid(a.nu_min, a.nu_max, 0.001, 2.0)
-    job = engine.Job(sd, engine.layer_input_from_profile(prof), grid, 25.0)
-    # evaluation count of one spectrum (the reference tile rule), from the kernel's own counter
-    r0 = job.run(a.precision, mu=[0.8], want_od=False, want_trans=True, count_evals=True)
-    evals_per_step = r0.evals
+    n_tiles = -(-grid.n_nu // grid.tile_samples)
+    tiles = None
+    if mode == "wavenumber":
+        span = shard.tile_span(n_tiles, world, rank)
+        tiles = (span.start, span.stop - span.start)
+        job = shard.shard_job(sd, prof, grid, 25.0, *tiles)
+        counts = [max(0, min(grid.n_nu, sp.stop * grid.tile_samples) - sp.start * grid.tile_samples)
+                  for sp in (shard.tile_span(n_tiles, world, r) for r in range(world))]
+        piece_max = max(counts)
+        gathered = torch.empty((world, piece_max), dtype=torch.float64, device="cuda")
+        piece = torch.zeros(piece_max, dtype=torch.float64, device="cuda")
+    else:
+        job = engine.Job(sd, engine.layer_input_from_profile(prof), grid, 25.0)
+
+    def step(timer=None, count_evals=False):
+        r = job.run(a.precision, mu=[0.8], want_od=False, want_trans=True, timer=timer, count_evals=count_evals,
+                    tiles=tiles)
+        if mode == "wavenumber" and world > 1:       # the exchange: every rank gets the whole spectrum
+            piece[: r.trans.shape[1]].copy_(r.trans[0])
+            dist.all_gather_into_tensor(gathered, piece)
+        return r
+
+    # evaluation count of one step (the reference tile rule), from the kernel's own counter
+    r0 = step(count_evals=True)
+    evals_local = r0.evals
+    if world > 1:
+        t = torch.tensor([evals_local], device="cuda", dtype=torch.int64)
+        dist.all_reduce(t)
+        evals_all = int(t.item())
+    else:
+        evals_all = evals_local
+    # one spectrum's evaluations (every rank's share in the wavenumber split)
+    evals_per_spectrum = evals_all if mode == "wavenumber" else evals_local
     r0_lines_bytes = int(getattr(job, "last_prep_bytes", 0))
     work_per_step = r0.work          # Faddeeva evaluations the kernel actually performs
-    launches_per_step = job.launches
+    launches_per_step = job.launches + (1 if mode == "wavenumber" and world > 1 else 0)
 
     def barrier():
         if world > 1:
@@ -372,14 +470,14 @@ def main():
         torch.cuda.synchronize()
 
     for _ in range(a.warmup):
-        job.run(a.precision, mu=[0.8], want_od=False, want_trans=True)
+        step()
     timer = {}
     barrier()
     with ClockSampler(local) as clocks:
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record()
         for _ in range(a.steps):
-            job.run(a.precision, mu=[0.8], want_od=False, want_trans=True, timer=timer)
+            step(timer=timer)
         e1.record()
         barrier()
     ms = e0.elapsed_time(e1)
@@ -388,31 +486,35 @@ def main():
         t = torch.tensor([ms], device="cuda", dtype=torch.float64)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         ms = float(t.item())
-    total_evals = evals_per_step * a.steps * world
+    # spectra per step: one shared spectrum (wavenumber split) or one per rank (replicas)
+    spectra_per_step = 1 if mode == "wavenumber" else world
+    total_evals = evals_per_spectrum * spectra_per_step * a.steps
     value = total_evals / (ms * 1e-3)
 
-    # end to end through the public API: host arrays in pinned memory, copies and the
-    # device->host transmittance read inside the timed region
-    e2e = None
+    # end to end through the public API, inputs as a caller passes them (pageable NumPy
+    # arrays); host->device copies and the device->host transmittance read inside the timed
+    # region. The pinned variant (line arrays in page-locked memory) is reported beside it.
+    e2e = e2e_pinned = None
     if not a.no_e2e:
+        h2d = sum(np.asarray(v).nbytes for v in sd.lines.values()) + prof.pressure_hpa.nbytes * (2 + len(prof.vmr))
+        if mode == "wavenumber":
+            call = lambda s_: shard.compute_transmittance_sharded(s_, prof, a.nu_min, a.nu_max, mu_view=0.8,
+                                                                  deterministic=False)
+            api = "pylblrtm_b200.shard.compute_transmittance_sharded"
+        else:
+            call = lambda s_: lbl.compute_transmittance(s_, prof, a.nu_min, a.nu_max, mu_view=0.8)
+            api = "pylblrtm_b200.compute_transmittance"
+        d2h = grid.n_nu * 8                     # every rank returns the whole spectrum
+        dt, e2e = _e2e_leg(torch, barrier, world, a.steps, a.warmup, lambda: call(sd), h2d, d2h + 8, api)
+        e2e["value"] = evals_per_spectrum * spectra_per_step * a.steps / dt
+        e2e["spectra_per_s"] = spectra_per_step * a.steps / dt
+        e2e["inputs"] = "pageable NumPy arrays (as a caller passes them)"
         pin = {k: torch.from_numpy(np.ascontiguousarray(v)).pin_memory().numpy() for k, v in sd.lines.items()}
         sd_pin = lbl.SpectralData(pin, sd.tips, sd.molar_masses, sd.molecule)
-        for _ in range(a.warmup):      # like the timed loop: each result lives until the next call returns
-            nu, T = lbl.compute_transmittance(sd_pin, prof, a.nu_min, a.nu_max, mu_view=0.8)
-        barrier()
-        t0 = time.perf_counter()
-        for _ in range(a.steps):
-            nu, T = lbl.compute_transmittance(sd_pin, prof, a.nu_min, a.nu_max, mu_view=0.8)
-        barrier()
-        e2e_s = time.perf_counter() - t0
-        if world > 1:
-            t = torch.tensor([e2e_s], device="cuda", dtype=torch.float64)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            e2e_s = float(t.item())
-        h2d = sum(v.nbytes for v in pin.values()) + prof.pressure_hpa.nbytes * (2 + len(prof.vmr))
-        e2e = {"value": evals_per_step * a.steps * world / e2e_s, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
-               "d2h_bytes_per_step": int(T.nbytes + 8), "spectra_per_s": a.steps * world / e2e_s,
-               "api": "pylblrtm_b200.compute_transmittance"}
+        dtp, e2e_pinned = _e2e_leg(torch, barrier, world, a.steps, a.warmup, lambda: call(sd_pin), h2d, d2h + 8, api)
+        e2e_pinned["value"] = evals_per_spectrum * spectra_per_step * a.steps / dtp
+        e2e_pinned["spectra_per_s"] = spectra_per_step * a.steps / dtp
+        e2e_pinned["inputs"] = "line arrays in page-locked host memory"
 
     if rank != 0:
         if world > 1:
@@ -423,17 +525,28 @@ def main():
     if a.precision == "fp32" and world == 1:
         dtimer = {}
         for _ in range(2):
-            job.run(a.precision, mu=[0.8], want_od=False, want_trans=True, deterministic=True)
+            job.run(a.precision, mu=[0.8], want_od=False, want_trans=True, deterministic=True, tiles=tiles)
         for _ in range(3):
-            job.run(a.precision, mu=[0.8], want_od=False, want_trans=True, deterministic=True, timer=dtimer)
+            job.run(a.precision, mu=[0.8], want_od=False, want_trans=True, deterministic=True, timer=dtimer,
+                    tiles=tiles)
         torch.cuda.synchronize()
         dms = [b.elapsed_time(c) for b, c in dtimer["tau_events"]]
         det = {"kernel_ms": sum(dms) / len(dms),
                "note": "bit-reproducible near-zone sums (deterministic=True); the timed default adds them "
                        "with shared-memory atomics (reproducible to ~1e-9 relative)"}
+    full_size = (a.nu_min, a.nu_max) == (600.0, 2500.0)
+    plain = acc = None
+    if world == 1 and a.precision == "fp32" and not (a.no_plain and a.no_accuracy):
+        if mode == "wavenumber":       # the comparison engines run on an unrestricted job
+            job_full = engine.Job(sd, engine.layer_input_from_profile(prof), grid, 25.0)
+        else:
+            job_full = job
+        plain, acc = plain_and_accuracy(torch, job_full, sd, prof, grid, evals_per_spectrum, value)
+        if not full_size:
+            acc = {k: v for k, v in acc.items() if not k.startswith("co2_band")}
+        del job_full
     adj = None if (a.no_adjoint or world > 1) else adjoint_timing(torch)
     sur = None if (a.no_surrogate or world > 1) else surrogate_timing()
-    acc = None if (a.no_accuracy or world > 1 or (a.nu_min, a.nu_max) != (600.0, 2500.0)) else accuracy(torch, job)
     tau_avg = sum(tau_ms) / len(tau_ms)
     # HBM-bound stages: algorithmic bytes / CUDA-event time
     try:
@@ -446,8 +559,9 @@ def main():
     n_rows_, n_kept_, n_grp_, rec_ = timer["prep_shape"]
     prep_ms = sum(b.elapsed_time(c) for b, c in timer["prep_events"]) / len(timer["prep_events"])
     sum_ms = sum(b.elapsed_time(c) for b, c in timer["sum_events"]) / len(timer["sum_events"])
+    n_out = r0.trans.shape[1]
     prep_bytes = n_rows_ * n_kept_ * rec_ + n_kept_ * 64 + n_rows_ * n_grp_ * 48
-    sum_bytes = n_rows_ * grid.n_nu * (4 if a.precision != "fp64" else 8) + grid.n_nu * 8
+    sum_bytes = n_rows_ * n_out * (4 if a.precision != "fp64" else 8) + n_out * 8
     hbm = {"peak_gbs": hbm_peak, "peak_source": hbm_source,
            "line_prep": {"ms": prep_ms, "bytes": prep_bytes, "gbs": prep_bytes / prep_ms / 1e6,
                          "frac": prep_bytes / prep_ms / 1e6 / hbm_peak,
@@ -458,7 +572,7 @@ def main():
                              "bytes_rule": "od read once (4 B x layers per point) + f64 T written"}}
     if a.precision == "fp32":
         nodes, l3, near = r0.work_split
-        flops = nodes * FLOPS_NODE + l3 * FLOPS_L3 + near * FLOPS_NEAR + FLOPS_CHEB_PER_POINT * grid.n_nu * 60
+        flops = nodes * FLOPS_NODE + l3 * FLOPS_L3 + near * FLOPS_NEAR + FLOPS_CHEB_PER_POINT * n_out * 60
         flops_note = (f"{nodes:.3e} node evals x {FLOPS_NODE} + {l3:.3e} level-3 evals x {FLOPS_L3} + "
                       f"{near:.3e} near points x {FLOPS_NEAR} + Chebyshev {FLOPS_CHEB_PER_POINT}/point/layer")
     else:
@@ -472,22 +586,24 @@ def main():
         cpu = {"value": n / dt, "unit": UNIT, "cores": 1, "kind": "port",
                "sample": f"oracle port, {CPU_SAMPLE[0]}-{CPU_SAMPLE[1]} cm^-1 x 60 layers ({n:.3e} evals, "
                          f"{dt:.1f} s), 1 process; CPU {model}"}
+    parallelism = "single" if world == 1 else (f"wavenumber{world}" if mode == "wavenumber" else f"replicas{world}")
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": a.steps, "warmup": a.warmup,
-        "ms_per_step": ms / a.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "ms_per_step": ms / a.steps, "higher_is_better": True,
+        "scaling": "strong" if mode == "wavenumber" else "weak", "vs_baseline": None,
         "dtype": "f64" if a.precision == "fp64" else "f32", "data": "synthetic",
-        "spectra_per_s": a.steps * world / (ms * 1e-3),
-        "evals_per_spectrum": evals_per_step,
-        "config": {"workload": WORKLOAD if (a.nu_min, a.nu_max) == (600.0, 2500.0)
-                   else f"{WORKLOAD} restricted to grid {a.nu_min}-{a.nu_max} cm^-1", "precision": a.precision, "lines": 200000, "layers": 60,
-                   "grid_points": grid.n_nu, "parallelism": f"replicas{world}" if world > 1 else "single",
+        "spectra_per_s": spectra_per_step * a.steps / (ms * 1e-3),
+        "evals_per_spectrum": evals_per_spectrum,
+        "config": {"workload": WORKLOAD if full_size
+                   else f"{WORKLOAD} restricted to grid {a.nu_min}-{a.nu_max} cm^-1", "precision": a.precision,
+                   "lines": 200000, "layers": 60, "grid_points": grid.n_nu, "parallelism": parallelism,
+                   "tiles_per_rank": tiles[1] if tiles else n_tiles,
                    "l2": "inputs and outputs larger than L2 (line records 384 MB, od 456 MB)"},
         "roofline": {"bound": "fp32", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                      "frac": achieved / peak,
-                     "traffic": TAU_ML_DRAM_BYTES if (a.precision == "fp32" and (a.nu_min, a.nu_max) ==
-                                                      (600.0, 2500.0)) else None,
+                     "traffic": TAU_ML_DRAM_BYTES if (a.precision == "fp32" and full_size and world == 1) else None,
                      "traffic_unit": "bytes per call of both kernels (ncu dram__bytes_read.sum + dram__bytes_write.sum)",
-                     "algorithmic_bytes": r0_lines_bytes + job.n_prof * job.n_lay * grid.n_nu * 4,
+                     "algorithmic_bytes": r0_lines_bytes + job.n_prof * job.n_lay * n_out * 4,
                      "algorithmic_bytes_rule": "32-B prepared line record per (layer, line) read once + "
                                                "float32 od written once per (layer, point)",
                      "kernel": {"fp32": "tau_far_kernel + tau_ml_kernel<0> (one lbl_tau_tiles_ml_f32 call)",
@@ -500,7 +616,9 @@ def main():
         "gpu_launches": launches_per_step * a.steps,
         "clocks": clocks.summary(),
         "e2e": e2e,
+        "e2e_pinned": e2e_pinned,
         "cpu_baseline": cpu,
+        "plain_engines": plain,
         "deterministic_mode": det,
         "accuracy": acc,
         "hbm_kernels": hbm,

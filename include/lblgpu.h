@@ -104,9 +104,12 @@ int lbl_sort_lines(const double* nu0, const double* shift, const int* gid, int n
  * whose memory pool owns the whole GPU and forbids further cudaMalloc calls).
  * No counterpart in the reference. The scratch is a static device array inside
  * the library (3 MiB on every GPU that loads it, held until the process exits),
- * so n_lines may not exceed 262,144 (LBL_EINVAL otherwise). The first call on a
- * device looks up the array's device address (cudaGetSymbolAddress) with that
- * device current; make that first call before any stream capture. All calls
+ * so n_lines may not exceed 262,144 (LBL_EINVAL otherwise). The first call in a
+ * CUDA context looks up the array's device address (cudaGetSymbolAddress) with
+ * that context's device current and caches it under the context's unique id
+ * (cuCtxGetId), so a cudaDeviceReset or another context current on the thread
+ * gets a fresh lookup instead of a stale address; make the first call in each
+ * context before any stream capture. All calls
  * share the one array: calls that overlap on the GPU (different streams, or
  * threads on one device) race and must be serialised by the caller. Allocates
  * nothing; same outputs as lbl_sort_lines. */
@@ -114,7 +117,10 @@ int lbl_sort_lines_noalloc(const double* nu0, const double* shift, const int* gi
                            double mask_hi, double p_max, int* order, int* n_kept, double* max_shift_bound,
                            void* stream);
 
-/* Gathers the sorted lines into LineIn records (out[0 .. *n_kept)). */
+/* Gathers the sorted lines into LineIn records (out[0 .. *n_kept)). n_lines is the
+ * record count of out and may exceed the device count *n_kept (a bound the caller
+ * knows on the host, so nothing waits for the count): slots *n_kept .. n_lines-1
+ * receive inactive records (nu0 = NaN, gid = 0, src = -1) that no tile range holds. */
 int lbl_gather_lines(const double* nu0, const double* sref, const double* g_air, const double* g_self,
                      const double* elow, const double* n_air, const double* shift, const int* gid,
                      const int* order, const int* n_kept, int n_lines, LineIn* out, void* stream);

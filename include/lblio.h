@@ -51,6 +51,14 @@ int lbl_line_pairs(const int* mol, const int* iso, const double* nu0, const doub
  * [0, n_lut). */
 int lbl_map_index(const int* index, long long n, const int* lut, int n_lut, int* out);
 
+/* Number of lines that lbl_sort_lines (lblgpu.h) keeps for these band edges: gid >= 0
+ * and finite nu0 in [lo_edge - |shift| p_max, hi_edge + |shift| p_max], compared in the
+ * same order as the device (the same count). No reference counterpart: it sizes the
+ * buffers of a wavenumber shard, whose band edges are narrowed to the shard's lines,
+ * before the device has counted. -1 for bad arguments. */
+long long lbl_count_band(const double* nu0, const double* shift, const int* gid, long long n, double lo_edge,
+                         double hi_edge, double p_max);
+
 #ifdef __cplusplus
 }
 #endif

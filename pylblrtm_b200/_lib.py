@@ -89,6 +89,7 @@ HOST_SIGNATURES = {
     "lbl_par_parse": (_I, [ctypes.c_char_p, _L, _L, _P, _P, _P]),
     "lbl_line_pairs": (_I, [_P, _P, _P, _P, _L, _D, _D, _D, _I, _P, _P, _P, _P, _P, _P]),
     "lbl_map_index": (_I, [_P, _L, _P, _I, _P]),
+    "lbl_count_band": (_L, [_P, _P, _P, _L, _D, _D, _D]),
 }
 
 _lock = threading.Lock()

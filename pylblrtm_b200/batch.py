@@ -110,7 +110,11 @@ def transmittance_batch(
         res = job.run(precision, mu=mu[b0:b1], want_od=False, want_trans=channels is None, channels=channels,
                       deterministic=deterministic)
         outs.append(res.channels if channels is not None else res.trans)
-    out = torch.cat(outs, dim=0) if len(outs) > 1 else outs[0]
+    if not outs:                    # no profiles (e.g. a rank's empty share): an empty result
+        n_out = channels[1] if channels is not None else grid.n_nu
+        out = engine._torch().empty((0, n_out), dtype=torch.float64, device="cuda")
+    else:
+        out = torch.cat(outs, dim=0) if len(outs) > 1 else outs[0]
     if channels is not None:
         width, n_ch = channels
         axis = grid.nu_min + (np.arange(n_ch) * width + 0.5 * (width - 1)) * grid.step

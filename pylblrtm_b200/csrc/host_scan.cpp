@@ -60,3 +60,20 @@ extern "C" int lbl_map_index(const int* index, long long n, const int* lut, int 
   }
   return bad ? LBL_EINVAL : LBL_OK;
 }
+
+// Host count of the lines the device sort keeps (lbl_sort_lines): gid >= 0, finite nu0
+// inside [lo_edge - |shift| p_max, hi_edge + |shift| p_max], the same comparisons in the
+// same order, so the count equals the device's. Sizes a wavenumber shard's buffers when
+// the band edges are narrowed to the shard's line window.
+extern "C" long long lbl_count_band(const double* nu0, const double* shift, const int* gid, long long n,
+                                    double lo_edge, double hi_edge, double p_max) {
+  if (n < 0 || (n > 0 && (!nu0 || !shift || !gid))) return -1;
+  long long c = 0;
+  for (long long i = 0; i < n; ++i) {
+    if (gid[i] < 0) continue;
+    const double sb = fabs(shift[i]) * p_max;
+    const double v = nu0[i];
+    c += isfinite(v) && (v >= lo_edge - sb) && (v <= hi_edge + sb);
+  }
+  return c;
+}

@@ -169,7 +169,9 @@ __global__ void bitonic_global_kernel(double* __restrict__ keys, int* __restrict
   }
 }
 
-// Sorted structure-of-records copy of the kept lines.
+// Sorted structure-of-records copy of the kept lines. Slots past the device's kept
+// count (the caller may size the output for an upper bound it knows on the host)
+// get an inactive record: nu0 = NaN, group 0, src = -1.
 __global__ void gather_lines_kernel(const double* __restrict__ nu0, const double* __restrict__ sref,
                                     const double* __restrict__ g_air, const double* __restrict__ g_self,
                                     const double* __restrict__ elow, const double* __restrict__ n_air,
@@ -177,9 +179,15 @@ __global__ void gather_lines_kernel(const double* __restrict__ nu0, const double
                                     const int* __restrict__ order, const int* __restrict__ n_kept,
                                     int n_lines, LineIn* __restrict__ out) {
   const int j = blockIdx.x * blockDim.x + threadIdx.x;
-  if (j >= n_lines || j >= *n_kept) return;
-  const int i = order[j];
+  if (j >= n_lines) return;
   LineIn r;
+  if (j >= *n_kept) {
+    r.nu0 = CUDART_NAN; r.sref = 0.0; r.g_air = 0.0; r.g_self = 0.0;
+    r.elow = 0.0; r.n_air = 0.0; r.shift = 0.0; r.gid = 0; r.src = -1;
+    out[j] = r;
+    return;
+  }
+  const int i = order[j];
   r.nu0 = nu0[i]; r.sref = sref[i]; r.g_air = g_air[i]; r.g_self = g_self[i];
   r.elow = elow[i]; r.n_air = n_air[i]; r.shift = shift[i]; r.gid = gid[i]; r.src = i;
   out[j] = r;
@@ -419,30 +427,75 @@ constexpr int NOALLOC_MAX_LINES = 1 << 18;                                   // 
 constexpr size_t NOALLOC_SCRATCH_BYTES = (size_t)NOALLOC_MAX_LINES * (sizeof(double) + sizeof(int));  // 3 MiB
 static __device__ __align__(256) unsigned char g_sort_scratch[NOALLOC_SCRATCH_BYTES];
 
+#include <cuda.h>   // CUcontext / CUresult types only; the two driver calls are resolved at run time
+
 #include <mutex>
 static std::mutex g_scratch_mutex;
-constexpr int NOALLOC_MAX_DEVICES = 64;
-static void* g_scratch_addr[NOALLOC_MAX_DEVICES] = {};
+constexpr int NOALLOC_MAX_CONTEXTS = 64;
+struct ScratchAddr {
+  unsigned long long ctx_id;   // process-unique id of the CUDA context (cuCtxGetId), 0 = empty slot
+  void* addr;
+};
+static ScratchAddr g_scratch_addr[NOALLOC_MAX_CONTEXTS] = {};
+static int g_scratch_next = 0;   // next slot to (re)use once the table is full
 
-// Device address of g_sort_scratch on the current device. The name is only a
-// host-side stand-in; the real address comes from cudaGetSymbolAddress, queried
-// once per device with that device current and then cached.
-static int sort_scratch_address(void** out) {
-  int dev = -1;
-  cudaError_t e = cudaGetDevice(&dev);
-  if (e != cudaSuccess) return lbl_set_error(LBL_ECUDA, "lbl_sort_lines_noalloc: %s", cudaGetErrorString(e));
-  if (dev < 0 || dev >= NOALLOC_MAX_DEVICES)
-    return lbl_set_error(LBL_EINVAL, "lbl_sort_lines_noalloc: device %d out of range", dev);
-  std::lock_guard<std::mutex> lock(g_scratch_mutex);
-  if (!g_scratch_addr[dev]) {
-    void* p = nullptr;
-    e = cudaGetSymbolAddress(&p, g_sort_scratch);
-    if (e != cudaSuccess || !p)
-      return lbl_set_error(LBL_ECUDA, "lbl_sort_lines_noalloc: cudaGetSymbolAddress failed: %s",
-                           cudaGetErrorString(e));
-    g_scratch_addr[dev] = p;
+typedef CUresult (*CtxGetCurrentFn)(CUcontext*);
+typedef CUresult (*CtxGetIdFn)(CUcontext, unsigned long long*);
+
+// Process-unique id of the calling thread's current CUDA context, or 0 when the
+// driver offers no such query (the caller then looks the address up every time).
+// The id of a context is never reused, so an address cached under it cannot go
+// stale: after cudaDeviceReset, or when a host application makes a context of its
+// own current, the id differs and the address is looked up again.
+static unsigned long long current_context_id() {
+  static CtxGetCurrentFn get_current = nullptr;
+  static CtxGetIdFn get_id = nullptr;
+  static bool resolved = false;
+  if (!resolved) {                                   // under g_scratch_mutex
+    resolved = true;
+    void* f = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPointByVersion("cuCtxGetCurrent", &f, 12000, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      get_current = (CtxGetCurrentFn)f;
+    f = nullptr;
+    if (cudaGetDriverEntryPointByVersion("cuCtxGetId", &f, 12000, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      get_id = (CtxGetIdFn)f;
   }
-  *out = g_scratch_addr[dev];
+  if (!get_current || !get_id) return 0;
+  CUcontext ctx = nullptr;
+  unsigned long long id = 0;
+  if (get_current(&ctx) != CUDA_SUCCESS || !ctx || get_id(ctx, &id) != CUDA_SUCCESS) return 0;
+  return id;
+}
+
+// Device address of g_sort_scratch in the current context. The name is only a
+// host-side stand-in; the real address comes from cudaGetSymbolAddress, called
+// with the device current the first time a context uses this entry point and then
+// cached under the context's unique id.
+static int sort_scratch_address(void** out) {
+  std::lock_guard<std::mutex> lock(g_scratch_mutex);
+  void* p = nullptr;
+  unsigned long long id = current_context_id();
+  if (id != 0) {
+    for (const ScratchAddr& s : g_scratch_addr)
+      if (s.ctx_id == id) {
+        *out = s.addr;
+        return LBL_OK;
+      }
+  }
+  // first use in this context (the lookup also binds the runtime's primary context
+  // when the thread has none current yet, so read the id again afterwards)
+  cudaError_t e = cudaGetSymbolAddress(&p, g_sort_scratch);
+  if (e != cudaSuccess || !p)
+    return lbl_set_error(LBL_ECUDA, "lbl_sort_lines_noalloc: cudaGetSymbolAddress failed: %s", cudaGetErrorString(e));
+  if (id == 0) id = current_context_id();
+  if (id != 0) {
+    g_scratch_addr[g_scratch_next] = ScratchAddr{id, p};
+    g_scratch_next = (g_scratch_next + 1) % NOALLOC_MAX_CONTEXTS;
+  }
+  *out = p;
   return LBL_OK;
 }
 
@@ -510,9 +563,13 @@ __global__ void line_prep_jac_kernel(const LineIn* __restrict__ lines, int n_lin
   const int row = blockIdx.y;
   if (j >= n_lines || row >= n_rows) return;
   const LineIn L = lines[j];
+  LineJac r = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+  if (L.src < 0) {                                   // inactive slot of lbl_gather_lines
+    out[(long long)row * n_lines + j] = r;
+    return;
+  }
   const long long gi = (long long)row * n_grp + L.gid;
   const LayerGroup G = lg[gi];
-  LineJac r = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
   const ScaledLine s = scale_line(L, G, nullptr, 0);
   if (s.active) {
     const double T = G.T;

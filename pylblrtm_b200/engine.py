@@ -118,7 +118,9 @@ def select_groups(sd: SpectralData, profile_gases: Sequence[str], nu_first: floa
     Returns the contributing groups in sorted (mol_id, iso_id) order and the
     group index of every line (-1 for lines of skipped groups). Emits the same
     RuntimeWarnings and raises the same KeyError as the reference. ``stats``
-    (a dict) receives "max_abs_shift", the largest finite |shift| (0 if none).
+    (a dict) receives "max_abs_shift", the largest finite |shift| (0 if none), and
+    "band_lines", how many lines of the contributing groups pass the band mask (the
+    host's count of the device sort's kept lines: the same comparisons, so never fewer).
     """
     lines = sd.lines
     mol = np.asarray(lines["mol_id"])
@@ -127,6 +129,7 @@ def select_groups(sd: SpectralData, profile_gases: Sequence[str], nu_first: floa
     gid = np.full(n, -1, dtype=np.int32)
     if stats is not None:
         stats["max_abs_shift"] = 0.0
+        stats["band_lines"] = 0
     if n == 0:
         return [], gid
     # one native pass: distinct (mol, iso) pairs, band-mask counts (forward.py:190-191)
@@ -192,6 +195,8 @@ def select_groups(sd: SpectralData, profile_gases: Sequence[str], nu_first: floa
             raise ValueError("array of sample points is empty" if np.asarray(t_arr).size == 0
                              else "fp and xp are not of the same length.")
         lut_pairs[int(order[pi])] = len(groups)
+        if stats is not None:
+            stats["band_lines"] += int(cnt)
         groups.append(Group(int(m), int(i), gas, float(mm), np.asarray(t_arr, np.float64),
                             np.asarray(q_arr, np.float64)))
     if groups:
@@ -201,6 +206,17 @@ def select_groups(sd: SpectralData, profile_gases: Sequence[str], nu_first: floa
         if host.lbl_map_index(pair_index.ctypes.data, n, lut.ctypes.data, k, gid.ctypes.data) != 0:
             raise RuntimeError("lbl_map_index: pair index out of range")
     return groups, gid
+
+
+def band_edges(nu_first: float, nu_last: float, cutoff: float,
+               line_window: Optional[Tuple[float, float]] = None) -> Tuple[float, float]:
+    """Edges of the device sort's band mask: the reference's nu[0] - cutoff and
+    nu[-1] + cutoff (``forward.py:190-191, 215-220``), narrowed to a shard's line
+    window when one is given."""
+    lo, hi = nu_first - cutoff, nu_last + cutoff
+    if line_window is not None:
+        lo, hi = max(lo, float(line_window[0])), min(hi, float(line_window[1]))
+    return lo, hi
 
 
 @dataclass
@@ -289,10 +305,21 @@ class Job:
 
     Construction does the host part (group selection with the reference's
     warnings/errors, grid sizes) and uploads lines, levels and partition tables;
-    :meth:`run` then does only device work.
+    :meth:`run` then does only device work, with no host read-back before the
+    results.
+
+    ``line_window = (lo, hi)`` narrows the device sort's band mask (``forward.py:190-220``)
+    to [max(nu_first - cutoff, lo), min(nu_last + cutoff, hi)], so only the lines of a
+    wavenumber shard are gathered and prepared (its tiles' windows widened by the
+    cut-off and the largest pressure shift, as ``shard.line_window`` gives). Every line
+    the full job keeps inside that window is kept, in the same order, and group
+    selection, warnings and the shift pad still come from the whole line list, so the
+    shard's tiles see the same candidate lines as in the full job and their sums are
+    identical.
     """
 
-    def __init__(self, sd: SpectralData, layers: LayerInput, grid: Grid, cutoff: float, warn_level: int = 4):
+    def __init__(self, sd: SpectralData, layers: LayerInput, grid: Grid, cutoff: float, warn_level: int = 4,
+                 line_window: Optional[Tuple[float, float]] = None):
         _lib.load()
         torch = _torch()
         self.torch = torch
@@ -311,7 +338,18 @@ class Job:
         self.groups, gid = select_groups(sd, layers.gases, self.nu_first, self.nu_last, self.cutoff,
                                          self.p_max, warn_level + 1, stats=st)
         self.n_lines = int(gid.size)
-        self.empty = not self.groups or self.n_lay == 0
+        self.mask_lo, self.mask_hi = band_edges(self.nu_first, self.nu_last, self.cutoff, line_window)
+        band_lines = int(st["band_lines"])
+        if line_window is not None and self.groups:
+            c = lambda k: np.ascontiguousarray(L[k], dtype=np.float64)
+            nu0, shift = c("nu0"), c("shift")
+            band_lines = int(_lib.load_host().lbl_count_band(nu0.ctypes.data, shift.ctypes.data, gid.ctypes.data,
+                                                             self.n_lines, self.mask_lo, self.mask_hi,
+                                                             float(self.p_max)))
+        # device records are sized for this host count (a bound on the sort's kept count),
+        # so no stage waits for the device count; slots past the device count are inactive
+        self.n_bound = band_lines
+        self.empty = not self.groups or self.n_lay == 0 or band_lines <= 0
         if self.empty:
             return
         if self.n_lines > (1 << 30):
@@ -367,8 +405,9 @@ class Job:
     def _device_lines(self, stream):
         """Layers, per-(layer, group) records, band mask + sort, gather and tile ranges.
 
-        Returns (t_layer, layer_groups, lines, n_kept, ranges, n_grp), or None when
-        no line lies in the band.
+        Returns (t_layer, layer_groups, lines, n_rec, ranges, n_grp): n_rec is the host's
+        bound on the kept lines, the record count of every per-line buffer (the device
+        count stays on the device).
         """
         torch, dev = self.torch, self.dev
         grid = self.grid
@@ -404,13 +443,11 @@ class Job:
         kept = torch.empty(1, dtype=torch.int32, device=dev)
         max_sb = torch.empty(1, dtype=torch.float64, device=dev)
         _lib.call("lbl_sort_lines", d_nu0.data_ptr(), d_shift.data_ptr(), self.gid.data_ptr(), n_lines,
-                  self.nu_first - self.cutoff, self.nu_last + self.cutoff, self.p_max, ws.data_ptr(), ws_bytes,
+                  self.mask_lo, self.mask_hi, self.p_max, ws.data_ptr(), ws_bytes,
                   order.data_ptr(), kept.data_ptr(), max_sb.data_ptr(), stream)
         self.launches += sort_launches(n_lines)
         self._kept = kept
-        n_kept = int(kept.item())                      # one small device->host read
-        if n_kept == 0:
-            return None
+        n_kept = self.n_bound                          # >= the device's kept count
         lines = torch.empty((n_kept * _lib.SIZEOF_LINE_IN // 8,), dtype=torch.float64, device=dev)
         _lib.call("lbl_gather_lines", d_nu0.data_ptr(), d_sref.data_ptr(), d_gair.data_ptr(), d_gself.data_ptr(),
                   d_elow.data_ptr(), d_nair.data_ptr(), d_shift.data_ptr(), self.gid.data_ptr(), order.data_ptr(),

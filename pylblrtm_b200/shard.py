@@ -2,13 +2,17 @@
 
 The forward model shards without any data-path exchange: profiles of a batch are
 independent, so each rank computes a contiguous slice of them
-(:func:`profile_slice`) and the results are gathered once at the end
-(:func:`transmittance_batch_sharded`, an all-gather over NCCL / NVLink, or over gloo
-on CPU). One spectrum splits by wavenumber (:func:`compute_transmittance_sharded`):
-each rank computes a contiguous range of the grid's reference tiles with the grid
-values of the full grid (every line list and layer on every rank; the tile-window
-rule makes the tiles independent), and the pieces are all-gathered; with the
-deterministic sums the result equals the single-GPU spectrum bit for bit.
+(:func:`profile_slice`; a rank may get none) and the results are gathered once at the
+end (:func:`transmittance_batch_sharded`, an all-gather over NCCL / NVLink, or over
+gloo on CPU). One spectrum splits by wavenumber (:func:`compute_transmittance_sharded`):
+each rank computes a contiguous range of the grid's reference tiles
+(:func:`tile_span`) with the grid values of the full grid, from only the lines that
+can reach those tiles (:func:`line_window`: the tiles widened by the cut-off and the
+largest pressure shift), so line preparation and its memory shrink with the rank
+count. The tile-window rule (``pylblrtm/forward.py:295-301``) makes the tiles
+independent, every tile sees the same candidate lines in the same order as in the
+full job, and the pieces are all-gathered; with the deterministic sums the result
+equals the single-GPU spectrum bit for bit.
 
 The surrogate's training has one real exchange step: data-parallel ranks sum their
 weight and bias gradients (:func:`allreduce_gradients`) between the backward pass and
@@ -43,6 +47,28 @@ def profile_slice(n: int, world: int, rank: int) -> slice:
     base, extra = divmod(int(n), world)
     start = rank * base + min(rank, extra)
     return slice(start, start + base + (1 if rank < extra else 0))
+
+
+def tile_span(n_tiles: int, world: int, rank: int) -> slice:
+    """Contiguous share of the reference tiles [0, n_tiles) for ``rank``."""
+    return profile_slice(n_tiles, world, rank)
+
+
+def line_window(spectral_data, grid, cutoff: float, p_max: float, first: int, count: int):
+    """Unshifted line centres [lo, hi] that reference tiles [first, first + count) of
+    ``grid`` can use: the tiles' first and last grid values widened by the larger of the
+    cut-off and the tile width (the summation's inner-line reach), plus the largest
+    finite |shift| x p_max and a few grid steps of margin. Every candidate line of those
+    tiles (``forward.py:295-301``, unshifted centres within cut-off + shift bound) lies
+    inside it."""
+    shift = np.abs(np.asarray(spectral_data.lines["shift"], dtype=np.float64))
+    shift = shift[np.isfinite(shift)]
+    pad = (float(shift.max()) if shift.size else 0.0) * float(p_max) * (1 + 1e-6) + 1e-6
+    ts = grid.tile_samples
+    i0 = first * ts
+    i1 = min(grid.n_nu, (first + count) * ts) - 1
+    reach = max(float(cutoff), ts * grid.step) + pad + 8 * grid.step
+    return grid.nu_at(i0) - reach, grid.nu_at(i1) + reach
 
 
 def gather_rows(local, n_total: int, group=None):
@@ -105,14 +131,24 @@ def gather_pieces(local, counts: Sequence[int], group=None):
     return torch.cat([p[:c] for p, c in zip(parts, counts)])
 
 
+def shard_job(spectral_data, profile, grid, cutoff: float, first: int, count: int, warn_level: int = 4):
+    """``engine.Job`` of one wavenumber shard: only the lines of :func:`line_window`
+    go to the device; group selection and warnings use the whole line list."""
+    from . import engine
+    li = engine.layer_input_from_profile(profile)
+    win = line_window(spectral_data, grid, cutoff, li.p_max_atm(), first, count)
+    return engine.Job(spectral_data, li, grid, float(cutoff), warn_level=warn_level, line_window=win)
+
+
 def compute_transmittance_sharded(spectral_data, profile, nu_min_cm1: float, nu_max_cm1: float, *,
                                   step_cm1: float = 0.001, line_cutoff_cm1: float = 25.0,
                                   tile_width_cm1: float = 2.0, mu_view: float = 1.0, deterministic: bool = True,
                                   group=None, compute: Optional[Callable] = None):
     """``compute_transmittance`` with the reference tiles of the grid split across the
-    ranks of ``group`` (multi-level float32 engine). Every rank returns the full
-    ``(nu, T)``. ``compute(first, count)`` replaces the device computation of a tile
-    range (tests); it returns that range's transmittance as a 1-D tensor.
+    ranks of ``group`` (multi-level float32 engine); each rank prepares only the lines
+    its tiles can use. Every rank returns the full ``(nu, T)``. ``compute(first,
+    count)`` replaces the device computation of a tile range (tests); it returns that
+    range's transmittance as a 1-D tensor.
     """
     import torch
     from . import engine
@@ -133,13 +169,12 @@ def compute_transmittance_sharded(spectral_data, profile, nu_min_cm1: float, nu_
     ts = grid.tile_samples
     n_tiles = -(-grid.n_nu // ts)
     world, rank = world_and_rank(group)
-    spans = [profile_slice(n_tiles, world, r) for r in range(world)]
+    spans = [tile_span(n_tiles, world, r) for r in range(world)]
     counts = [max(0, min(grid.n_nu, sl.stop * ts) - sl.start * ts) if sl.stop > sl.start else 0 for sl in spans]
     sl = spans[rank]
     if compute is None:
         def compute(first, count):
-            job = engine.Job(spectral_data, engine.layer_input_from_profile(profile), grid,
-                             float(line_cutoff_cm1), warn_level=3)
+            job = shard_job(spectral_data, profile, grid, float(line_cutoff_cm1), first, count, warn_level=3)
             res = job.run("fp32", mu=[float(mu_view)], want_od=False, want_trans=True,
                           deterministic=deterministic, tiles=(first, count))
             return res.trans[0]

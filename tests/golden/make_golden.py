@@ -2,7 +2,7 @@
 
 Run in a container where the reference source is present:
 
-    python tests/golden/make_golden.py --reference /root/reference
+    python tests/golden/make_golden.py --reference <source tree of the reference package>
 
 Each case builds seeded synthetic inputs with ``pylblrtm_b200.synthetic``,
 converts them to the reference's own SpectralData / AtmosphericProfile objects
@@ -165,7 +165,7 @@ def run_case(args):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--reference", default="/root/reference")
+    ap.add_argument("--reference", required=True, help="source tree that holds the pylblrtm package")
     ap.add_argument("--only", nargs="*")
     ap.add_argument("--jobs", type=int, default=os.cpu_count())
     a = ap.parse_args()

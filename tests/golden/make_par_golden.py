@@ -1,6 +1,6 @@
 """Golden vectors for the HITRAN text readers, made by running the REFERENCE's readers.
 
-    python tests/golden/make_par_golden.py --reference /root/reference
+    python tests/golden/make_par_golden.py --reference <source tree of the reference package>
 
 Writes seeded synthetic ``.par`` and TIPS ``.txt`` files under ``tests/golden/hitran/``
 (clean 160-character records with LF endings, and a mixed file with CRLF / CR endings,

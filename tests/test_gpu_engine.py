@@ -293,6 +293,13 @@ def test_wavenumber_shards_equal_the_full_spectrum(cuda):
     nu, t = shard.compute_transmittance_sharded(sd, prof, 1500.0, 1507.3, mu_view=0.8)
     _, t_ref = lbl.compute_transmittance(sd, prof, 1500.0, 1507.3, mu_view=0.8, deterministic=True)
     assert np.array_equal(t, t_ref) and t.min() < 0.99
+    # shard jobs: each range from only the lines of its window, bit for bit the full job's
+    for first, count in ((0, 1), (1, 2), (3, 1)):
+        sj = shard.shard_job(sd, prof, grid, 25.0, first, count)
+        assert sj.n_bound < job.n_bound
+        piece = sj.run("fp32", mu=[0.8], want_od=True, want_trans=True, deterministic=True, tiles=(first, count))
+        ref = job.run("fp32", mu=[0.8], want_od=True, want_trans=True, deterministic=True, tiles=(first, count))
+        assert torch.equal(piece.od, ref.od) and torch.equal(piece.trans, ref.trans)
     with pytest.raises(ValueError, match="outside the grid"):
         job.run("fp32", tiles=(3, 2))
     with pytest.raises(ValueError, match="tiles needs"):
@@ -329,3 +336,16 @@ def test_inner_ranges_select_every_inner_line(cuda, tile, step, monkeypatch):
     assert with_inner.evals == scan_all.evals and with_inner.work_split == scan_all.work_split
     rel = ((with_inner.od - scan_all.od).abs() / scan_all.od.abs().clamp_min(1e-30)).max().item()
     assert rel <= 2e-6, rel
+
+
+def test_batch_of_zero_profiles(cuda):
+    """A rank whose share of a sharded batch is empty gets an empty [0, n] result."""
+    from pylblrtm_b200 import batch
+    sd = synthetic.restrict(synthetic.three_gas_lines(3000, 990.0, 1030.0, seed=3), 990.0, 1030.0)
+    lv = synthetic.perturbed_levels(synthetic.logp_levels(9), 2, seed=5)
+    vmr = {g: lv[g][:0] for g in ("H2O", "CO2", "O3")}
+    nu, t = batch.transmittance_batch(sd, lv["p"][:0], lv["t"][:0], vmr, 1000.0, 1003.0)
+    assert t.shape == (0, nu.size) and nu.size == 3001
+    ax, ch = batch.transmittance_batch(sd, lv["p"][:0], lv["t"][:0], vmr, 1000.0, 1003.0, channel_width_cm1=0.25,
+                                       as_numpy=False)
+    assert tuple(ch.shape) == (0, ax.size) and ch.is_cuda
