@@ -311,10 +311,13 @@ int lbl_rowsum_bf16(const void* x, int rows, int cols, int ld, float* out, void*
 int lbl_pack_inputs_bf16(const float* raw, int rows, int cols, const float* mean, const float* inv_std, void* x,
                          int ld, void* x_t, int ld_t, void* stream);
 /* Ensemble gate: for each sample b, mean[b, c] over the n_mem members' predictions
- * pred[m * member_stride + b * ld + c], est[b] = max_c of their standard deviation and
- * flag[b] = (scale * est[b] > gate). */
+ * pred[m * member_stride + b * ld + c], est[b] = max_c of their standard deviation,
+ * weighted by ch_scale[c] when ch_scale (device, [n_ch]) is not NULL, and
+ * flag[b] = (scale * est[b] > gate). The weights and the gate come from a calibration
+ * split (pylblrtm_b200.surrogate.calibrate_gate). */
 int lbl_ensemble_gate(const float* pred, int n_mem, long long member_stride, int n_samples, int ld, int n_ch,
-                      float scale, float gate, float* mean, float* est, int* flag, void* stream);
+                      const float* ch_scale, float scale, float gate, float* mean, float* est, int* flag,
+                      void* stream);
 
 /* Measurement probe (no reference counterpart): `blocks` CTAs of 256 threads
  * each run 8 chains of `iters` dependent float32 FMAs, i.e.

@@ -65,7 +65,7 @@ SIGNATURES = {
     "lbl_adam_step": (_I, [_P, _P, _P, _P, _I, _L, _I, _I, _I, _F, _F, _F, _F, _I, _P, _P, _I, _P]),
     "lbl_rowsum_bf16": (_I, [_P, _I, _I, _I, _P, _P]),
     "lbl_pack_inputs_bf16": (_I, [_P, _I, _I, _P, _P, _P, _I, _P, _I, _P]),
-    "lbl_ensemble_gate": (_I, [_P, _I, _L, _I, _I, _I, _F, _F, _P, _P, _P, _P]),
+    "lbl_ensemble_gate": (_I, [_P, _I, _L, _I, _I, _I, _P, _F, _F, _P, _P, _P, _P]),
 }
 
 # epilogue modes of lbl_gemm_bf16

@@ -455,8 +455,8 @@ __global__ void pack_inputs_kernel(const float* __restrict__ raw, int rows, int 
 // and the error estimate est[b] = max over channels of the members' standard deviation
 // (population form); flag[b] = (scale * est[b] > gate).
 __global__ void ensemble_gate_kernel(const float* __restrict__ pred, int n_mem, long long member_stride, int ld,
-                                     int n_ch, float scale, float gate, float* __restrict__ mean,
-                                     float* __restrict__ est, int* __restrict__ flag) {
+                                     int n_ch, const float* __restrict__ ch_scale, float scale, float gate,
+                                     float* __restrict__ mean, float* __restrict__ est, int* __restrict__ flag) {
   const int b = blockIdx.x;
   float worst = 0.0f;
   for (int c = threadIdx.x; c < n_ch; c += blockDim.x) {
@@ -470,7 +470,8 @@ __global__ void ensemble_gate_kernel(const float* __restrict__ pred, int n_mem, 
       s2 += d * d;
     }
     mean[(long long)b * n_ch + c] = mu;
-    worst = fmaxf(worst, sqrtf(s2 / n_mem));
+    const float sd = sqrtf(s2 / n_mem);
+    worst = fmaxf(worst, ch_scale ? ch_scale[c] * sd : sd);
   }
   for (int o = 16; o > 0; o >>= 1) worst = fmaxf(worst, __shfl_xor_sync(0xffffffffu, worst, o));
   __shared__ float part[32];
@@ -607,12 +608,12 @@ extern "C" int lbl_pack_inputs_bf16(const float* raw, int rows, int cols, const 
 }
 
 extern "C" int lbl_ensemble_gate(const float* pred, int n_mem, long long member_stride, int n_samples, int ld,
-                                 int n_ch, float scale, float gate, float* mean, float* est, int* flag,
-                                 void* stream) {
+                                 int n_ch, const float* ch_scale, float scale, float gate, float* mean, float* est,
+                                 int* flag, void* stream) {
   if (!pred || !mean || !est || !flag || n_mem < 1 || n_samples < 1 || n_ch < 1 || ld < n_ch ||
       (n_mem > 1 && member_stride < (long long)n_samples * ld))
     return lbl_set_error(LBL_EINVAL, "lbl_ensemble_gate: bad arguments");
-  ensemble_gate_kernel<<<n_samples, 256, 0, (cudaStream_t)stream>>>(pred, n_mem, member_stride, ld, n_ch, scale,
-                                                                     gate, mean, est, flag);
+  ensemble_gate_kernel<<<n_samples, 256, 0, (cudaStream_t)stream>>>(pred, n_mem, member_stride, ld, n_ch, ch_scale,
+                                                                     scale, gate, mean, est, flag);
   return lbl_check_launch("lbl_ensemble_gate");
 }

@@ -269,35 +269,89 @@ __global__ void line_prep_f64_kernel(const LineIn* __restrict__ lines, const int
   out[(long long)row * n_lines + j] = r;
 }
 
-__global__ void line_prep_f32_kernel(const LineIn* __restrict__ lines, const int* __restrict__ n_kept,
-                                     int n_lines, const LayerGroup* __restrict__ lg, int n_rows, int n_grp,
-                                     double nu_min, double step, LineF32* __restrict__ out, int* err) {
+// Float32-engine line prep: one thread per line over PREP_ROWS rows (profile-layers), so
+// a line's record is read once and its layer-independent factors are formed once: the
+// stimulated-emission denominator -expm1(-c2 nu0 / 296), c2 E'' and 1/(nu0 * 3.581e-7).
+// Per (row, group) the CTA stages 1/T, 1/T - 1/296, 0.5 c2 / T, ln(296/T) and 1/sqrt(T/M)
+// in shared memory. The Boltzmann and stimulated-emission factors stay float64
+// (exp, expm1), the strength is divided by R(nuc, T) in float64 as in forward.py:277;
+// the Lorentz width's (296/T)^n_air is a float exponential (the record holds y in
+// float anyway). Same records and error word as before; the float64 engine's prep
+// (line_prep_f64_kernel) keeps the reference's operation order.
+constexpr int PREP_ROWS = 8;
+constexpr int PREP_THREADS = 128;
+
+struct RowGroupF32 {
+  double p_self, p_air, col_q, dinv, minus_c2_inv_t, half_c2_inv_t, inv_dop;
+  float log_t296;
+  int active;
+};
+
+__global__ void __launch_bounds__(PREP_THREADS)
+line_prep_f32_kernel(const LineIn* __restrict__ lines, const int* __restrict__ n_kept, int n_lines,
+                     const LayerGroup* __restrict__ lg, int n_rows, int n_grp, double nu_min, double step,
+                     LineF32* __restrict__ out, int* err) {
+  extern __shared__ RowGroupF32 s_rg[];                         // [PREP_ROWS][n_grp]
+  const int r0 = blockIdx.y * PREP_ROWS;
+  const int nr = min(PREP_ROWS, n_rows - r0);
+  for (int i = threadIdx.x; i < nr * n_grp; i += blockDim.x) {
+    const LayerGroup G = lg[(long long)r0 * n_grp + i];
+    const double inv_t = 1.0 / G.T;
+    RowGroupF32 q;
+    q.p_self = G.p_self;
+    q.p_air = G.p_air;
+    q.col_q = G.q_ratio * G.col;
+    q.dinv = inv_t - 1.0 / T_REF;
+    q.minus_c2_inv_t = -C2 * inv_t;
+    q.half_c2_inv_t = 0.5 * C2 * inv_t;
+    q.inv_dop = 1.0 / G.dop;
+    q.log_t296 = (float)log(T_REF * inv_t);
+    q.active = G.col != 0.0;                                    // forward.py:253-255
+    s_rg[i] = q;
+  }
+  __syncthreads();
   const int j = blockIdx.x * blockDim.x + threadIdx.x;
-  const int row = blockIdx.y;
-  if (j >= n_lines || row >= n_rows) return;
+  if (j >= n_lines) return;
   LineF32 r;
   r.nuc = CUDART_NAN; r.j0 = 0; r.b = 0.f; r.a = 0.f; r.y = 0.f; r.amp = 0.f; r.amp_far = 0.f;
-  if (j < *n_kept) {
-    const LineIn L = lines[j];
-    const ScaledLine s = scale_line(L, lg[(long long)row * n_grp + L.gid], err, row * (n_grp + 1) + L.gid);
-    if (s.active) {
-      const double sc = SQRT_LN2 / s.alpha;
-      double jd = rint((s.nuc - nu_min) / step);
+  if (j >= *n_kept) {
+    for (int k = 0; k < nr; ++k) out[(long long)(r0 + k) * n_lines + j] = r;
+    return;
+  }
+  const LineIn L = lines[j];
+  const double stim296 = -expm1(-C2 * L.nu0 / T_REF);
+  const double sref_stim = L.sref / stim296;
+  const double c2_elow = -C2 * L.elow;
+  const double inv_nd = 1.0 / (L.nu0 * DOPPLER);
+  const double inv_step = 1.0 / step;
+  const float n_air = (float)L.n_air;
+  for (int k = 0; k < nr; ++k) {
+    const int row = r0 + k;
+    const RowGroupF32& G = s_rg[k * n_grp + L.gid];
+    LineF32 o = r;
+    if (G.active) {
+      const double nuc = L.nu0 + L.shift * G.p_air;             // forward.py:263
+      double S = sref_stim * G.col_q * exp(c2_elow * G.dinv) * -expm1(G.minus_c2_inv_t * L.nu0);
+      S /= nuc * tanh(nuc * G.half_c2_inv_t);                  // / R(nuc, T), forward.py:277
+      if (!isfinite(S) || S < 0.0) flag_error(err, row * (n_grp + 1) + L.gid);   // forward.py:280-283
+      const double gamma = (double)expf(n_air * G.log_t296) * (L.g_air * G.p_air + L.g_self * G.p_self);
+      const double sc = SQRT_LN2 * inv_nd * G.inv_dop;           // sqrt(ln 2) / alpha_D, forward.py:292
+      double jd = rint((nuc - nu_min) * inv_step);
       jd = fmin(fmax(jd, -2.0e9), 2.0e9);     // host guarantees |j0| < 2^31 for kept lines
       const int j0 = (int)jd;
-      const double rem = s.nuc - grid_nu(nu_min, step, j0);
-      const double y = SQRT_LN2 * s.gamma / s.alpha;
-      const double amp = VOIGT_K / s.alpha * s.S;
-      r.nuc = s.nuc;
-      r.j0 = j0;
-      r.b = (float)(rem * sc);
-      r.a = (float)(step * sc);
-      r.y = (float)y;
-      r.amp = (float)amp;
-      r.amp_far = (float)(amp * y * INV_SQRT_PI);
+      const double rem = nuc - grid_nu(nu_min, step, j0);
+      const double y = sc * gamma;
+      const double amp = VOIGT_K * inv_nd * G.inv_dop * S;
+      o.nuc = nuc;
+      o.j0 = j0;
+      o.b = (float)(rem * sc);
+      o.a = (float)(step * sc);
+      o.y = (float)y;
+      o.amp = (float)amp;
+      o.amp_far = (float)(amp * y * INV_SQRT_PI);
     }
+    out[(long long)row * n_lines + j] = o;
   }
-  out[(long long)row * n_lines + j] = r;
 }
 
 }  // namespace lbl
@@ -408,9 +462,11 @@ extern "C" int lbl_line_prep_f32(const LineIn* lines, const int* n_kept, int n_l
                                  void* stream) {
   if (n_lines < 1 || n_rows < 1 || n_rows > 65535 || n_grp < 1 || !lines || !lg || !out || !(step > 0))
     return lbl_set_error(LBL_EINVAL, "lbl_line_prep_f32: bad arguments");
-  dim3 grid(grid1(n_lines, 128), n_rows);
-  line_prep_f32_kernel<<<grid, 128, 0, (cudaStream_t)stream>>>(lines, n_kept, n_lines, lg, n_rows, n_grp,
-                                                               nu_min, step, out, err);
+  dim3 grid(grid1(n_lines, PREP_THREADS), (unsigned)((n_rows + PREP_ROWS - 1) / PREP_ROWS));
+  const size_t smem = sizeof(RowGroupF32) * PREP_ROWS * (size_t)n_grp;
+  if (smem > 48 * 1024) return lbl_set_error(LBL_EINVAL, "lbl_line_prep_f32: too many line groups");
+  line_prep_f32_kernel<<<grid, PREP_THREADS, smem, (cudaStream_t)stream>>>(lines, n_kept, n_lines, lg, n_rows,
+                                                                           n_grp, nu_min, step, out, err);
   return lbl_check_launch("lbl_line_prep_f32");
 }
 

@@ -45,7 +45,6 @@ constexpr int ML_KF = 8;                       // nodes for level-1 lines far fr
 constexpr float ML_FAR1 = 5.f;                 // "far": more than (1 + ML_FAR1) half-widths from the centre
 constexpr float ML_MIN_H1 = 32.f;              // smallest chunk half-width (points) using level 1
 constexpr float ML_MIN_H2 = 16.f;              // smallest sub-chunk half-width using level 2
-constexpr int ML_NB = 2048;                    // near items buffered per batch
 
 // Chebyshev node offsets (fractions of the half-width) and DCT weights, row-major [k][j]
 static __constant__ float c_node16[ML_K] = {LBL_CHEB16_NODES};
@@ -309,34 +308,166 @@ tau_far_kernel(const LineF32* __restrict__ prep, int n_lines, const int2* __rest
   }
 }
 
+// ---------------------------------------------------------------------------
+// Levels 2 and 3 (tau_ml_kernel). Each round stages up to 256 candidate lines; the
+// inner ones (not level-1 lines of tau_far_kernel) go to shared memory as
+// structure-of-arrays records, with a 2-bit class per warp (none, level 3, level 2
+// with 16 nodes, level 2 with 8 nodes). Then each warp works alone on its own
+// 256-point sub-chunk, with no CTA barrier until the next round:
+//  * level 2, one lane per line: the lane evaluates its line at every node of the
+//    sub-chunk from registers (node offsets are constant operands); the lanes' node
+//    sums are reduced once per round (transposed warp reduction) and added to the
+//    warp's float64 node sums;
+//  * level 3: each lane evaluates the line at its own 8 points, by the clamped
+//    five-term form, or by the two-term form when the line is far from every point of
+//    the sub-chunk (|z|^2 >= FAR_Z2 there);
+//  * near zones: the near points of the warp's level-3 lines inside its sub-chunk form
+//    an item space (middles, where the float64 core may apply, then tails); lanes take
+//    consecutive items, find their line by a shuffle search over a group of 32 lines
+//    and add (accurate value - clamped loop value) into the warp's part of s_core.
+// The epilogue folds the level-1 series and both level-2 interpolants into one
+// 16-term Chebyshev series per sub-chunk, so each point evaluates one series.
+constexpr int ML_NBW = 256;                    // near items buffered per warp (bit-reproducible mode)
+constexpr unsigned FULL_MASK = 0xffffffffu;
+
+// Sum over the 32 lanes of f[16], transposed: afterwards lanes 2j and 2j+1 hold the
+// total of node j (j = (lane >> 1) & 15); 16 shuffles for the 16 sums.
+__device__ __forceinline__ float reduce16_transposed(const float (&f)[ML_K], int lane) {
+  float g[8], h[4], u[2];
+  const bool b4 = lane & 16, b3 = lane & 8, b2 = lane & 4, b1 = lane & 2;
+#pragma unroll
+  for (int k = 0; k < 8; ++k) g[k] = (b4 ? f[k + 8] : f[k]) + __shfl_xor_sync(FULL_MASK, b4 ? f[k] : f[k + 8], 16);
+#pragma unroll
+  for (int k = 0; k < 4; ++k) h[k] = (b3 ? g[k + 4] : g[k]) + __shfl_xor_sync(FULL_MASK, b3 ? g[k] : g[k + 4], 8);
+#pragma unroll
+  for (int k = 0; k < 2; ++k) u[k] = (b2 ? h[k + 2] : h[k]) + __shfl_xor_sync(FULL_MASK, b2 ? h[k] : h[k + 2], 4);
+  float v = (b1 ? u[1] : u[0]) + __shfl_xor_sync(FULL_MASK, b1 ? u[0] : u[1], 2);
+  return v + __shfl_xor_sync(FULL_MASK, v, 1);
+}
+
+// The same for f[8]: afterwards lanes 4j .. 4j+3 hold the total of node j = (lane >> 2) & 7.
+__device__ __forceinline__ float reduce8_transposed(const float (&f)[ML_KF], int lane) {
+  float g[4], h[2];
+  const bool b4 = lane & 16, b3 = lane & 8, b2 = lane & 4;
+#pragma unroll
+  for (int k = 0; k < 4; ++k) g[k] = (b4 ? f[k + 4] : f[k]) + __shfl_xor_sync(FULL_MASK, b4 ? f[k] : f[k + 4], 16);
+#pragma unroll
+  for (int k = 0; k < 2; ++k) h[k] = (b3 ? g[k + 2] : g[k]) + __shfl_xor_sync(FULL_MASK, b3 ? g[k] : g[k + 2], 8);
+  float v = (b2 ? h[1] : h[0]) + __shfl_xor_sync(FULL_MASK, b2 ? h[0] : h[1], 4);
+  v += __shfl_xor_sync(FULL_MASK, v, 2);
+  return v + __shfl_xor_sync(FULL_MASK, v, 1);
+}
+
+// amp_far * (1 + B_1 r + ... + B_8 r^8) of one line by Horner's rule (see asym5_line_coeffs).
+__device__ __forceinline__ float asym5_poly(float r, float amp_far, const float4& p, const float4& q) {
+  float v = fmaf(q.w, r, q.z);
+  v = fmaf(v, r, q.y);
+  v = fmaf(v, r, q.x);
+  v = fmaf(v, r, p.w);
+  v = fmaf(v, r, p.z);
+  v = fmaf(v, r, p.y);
+  v = fmaf(v, r, p.x);
+  return fmaf(v, r, amp_far);
+}
+
+// Level 2, one lane per line: lane i of each 32-line step takes line list[stride * i]
+// and adds its values at the K nodes offset (node_k * H2) from the sub-chunk centre C2w
+// into f. Nodes k and K-1-k are mirror images, so each pair shares one offset. Three
+// warp-uniform paths: two-term far-wing form when every lane's line has |z|^2 >=
+// FAR_Z2 at every node, five-term form when |z|^2 >= MID_Z2 everywhere, else the full
+// algorithm per node.
+template <int K>
+__device__ __forceinline__ void level2_lines(float (&f)[K], const unsigned char* list, int stride, int n,
+                                             const float4* __restrict__ s_g, const float4* __restrict__ s_h,
+                                             const float4* __restrict__ s_p, const float4* __restrict__ s_q,
+                                             float C2w, float H2, int lane) {
+  const float* nodes = K == ML_K ? c_node16 : c_node8;
+  for (int i0 = 0; i0 < n; i0 += 32) {
+    const int i = i0 + lane;
+    const bool act = i < n;
+    int l = 0;
+    float4 g = make_float4(C2w, 0.f, -1.0e4f, 0.f), h = make_float4(1.f, 1.f, 0.f, 0.f);   // idle lane: adds 0
+    if (act) {
+      l = list[stride * i];
+      g = s_g[l];
+      h = s_h[l];
+    }
+    const float xc = fmaf(C2w - g.x, g.y, -g.z);          // x at the sub-chunk centre
+    const float ha = H2 * g.y;                            // sub-chunk half-width in x units
+    const float xm = fmaf(-nodes[0], ha, fabsf(xc));      // |x| at the node nearest the line
+    const float zm = fmaf(xm, xm, h.y);
+    int path = 0;
+    if (act && !(h.x >= 0.f && zm >= FAR_Z2)) path = (h.x >= 0.f && xm > 0.f && zm >= MID_Z2) ? 1 : 2;
+    const int wpath = __reduce_max_sync(FULL_MASK, path);
+    if (wpath == 0) {
+      const float ny2 = -2.0f * h.y;
+#pragma unroll
+      for (int k = 0; k < K / 2; ++k) {
+        far_wing_add(f[k], fmaf(nodes[k], ha, xc), h.y, ny2, g.w);
+        far_wing_add(f[K - 1 - k], fmaf(-nodes[k], ha, xc), h.y, ny2, g.w);
+      }
+    } else if (wpath == 1) {
+      float4 p = make_float4(0.f, 0.f, 0.f, 0.f), q = p;
+      if (act) {
+        p = s_p[l];
+        q = s_q[l];
+      }
+#pragma unroll
+      for (int k = 0; k < K / 2; ++k) {
+        const float xa = fmaf(nodes[k], ha, xc), xb = fmaf(-nodes[k], ha, xc);
+        const float ra = rcp_approx(fmaf(xa, xa, h.y)), rb = rcp_approx(fmaf(xb, xb, h.y));
+        f[k] = fmaf(ra, asym5_poly(ra, g.w, p, q), f[k]);
+        f[K - 1 - k] = fmaf(rb, asym5_poly(rb, g.w, p, q), f[K - 1 - k]);
+      }
+    } else {
+#pragma unroll 1
+      for (int k = 0; k < K / 2; ++k) {
+        f[k] += far_node_general(fmaf(nodes[k], ha, xc), h.x, h.y, h.z, g.w);
+        f[K - 1 - k] += far_node_general(fmaf(-nodes[k], ha, xc), h.x, h.y, h.z, g.w);
+      }
+    }
+  }
+}
+
+// (accurate value - clamped loop value) of a level-3 line at chunk point p; x is
+// formed exactly as in the level-3 loop, so the clamped constant h.w cancels.
+__device__ __forceinline__ float near_correction(int p, const float4& g, const float4& h) {
+  const float x0 = fmaf((float)(p & ~(ML_P - 1)) - g.x, g.y, -g.z);
+  const float x = fmaf((float)(p & (ML_P - 1)), g.y, x0);
+  const float z2 = fmaf(x, x, h.y);
+  if (z2 >= MID_Z2) return 0.f;
+  float v;
+  if (z2 >= CORE_Z2 && h.x >= 0.f) v = h.z * re_w_cf32(x, h.x, z2);
+  else v = (float)((double)h.z * weideman_re_f32((double)x, (double)h.x));
+  return v - h.w;
+}
+
+#ifndef LBL_ML_MIN_BLOCKS
+#define LBL_ML_MIN_BLOCKS 4                    // resident CTAs per SM the register budget aims at
+#endif
+
 template <bool DET>
-__global__ void __launch_bounds__(ML_THREADS, 4)
+__global__ void __launch_bounds__(ML_THREADS, LBL_ML_MIN_BLOCKS)
 tau_ml_kernel(const LineF32* __restrict__ prep, int n_lines, const int2* __restrict__ ranges,
               const int2* __restrict__ inner_ranges, const double* __restrict__ t_layer, double nu_min,
               double step, long long n_nu, int tile_samples, int chunks_per_tile, double cutoff, int n_grp,
               float* __restrict__ od, int* err, unsigned long long* evals, unsigned long long* work,
               int tile_first, long long out_first, long long out_stride) {
   constexpr int P = ML_P;
-  __shared__ MlLine s2[ML_THREADS];                 // inner lines of the round
-  __shared__ unsigned char s_l2[ML_THREADS / 32][ML_THREADS];   // per-warp level-2 slots
-  __shared__ unsigned char s_l3[ML_THREADS / 32][ML_THREADS];   // per-warp level-3 slots
-  __shared__ unsigned char s_nl[ML_THREADS / 32][ML_THREADS];   // per-warp slots with near points in it
-  __shared__ int s_cnt[3][ML_THREADS / 32];
-  __shared__ int s_seg_start[ML_THREADS + 1];       // near-item prefix per inner slot (default: middles)
-  __shared__ short s_seg_lo[ML_THREADS];            // first near point per inner slot (default: of the middle)
-  // default mode: the near zone of a slot is split into its middle (|z|^2 < CORE_Z2, the
-  // float64 core) and its two tails (the float continued fraction), each kind in an item
-  // space of its own, so that a warp's consecutive items take the same branch
-  __shared__ int s_segc_start[ML_THREADS + 1];      // tail-item prefix per inner slot
-  __shared__ short s_segc_lo[ML_THREADS];           // first point of the left tail
-  __shared__ short s_segc_nl[ML_THREADS];           // points in the left tail
-  __shared__ short s_segc_rlo[ML_THREADS];          // first point of the right tail
-  __shared__ unsigned char s_seg_mask[ML_THREADS];  // warps treating the inner line directly (level 3)
-  __shared__ float s_core[ML_CHUNK];               // near-zone corrections (each point owned by one thread)
-  __shared__ float s_nbuf[ML_NB];                   // near-item values of one batch
+  constexpr int NW = ML_THREADS / 32;
+  __shared__ float4 s_g[ML_THREADS];                // jf, a, b, amp_far of the round's inner lines
+  __shared__ float4 s_h[ML_THREADS];                // y, y^2, amp, clamped-loop value inside the near zone
+  __shared__ float4 s_p[ML_THREADS];                // amp_far * (B_1 .. B_4)
+  __shared__ float4 s_q[ML_THREADS];                // amp_far * (B_5 .. B_8)
+  __shared__ short4 s_nr[ML_THREADS];               // near range (lo, n) and its middle (lo, n), chunk points
+  __shared__ unsigned short s_cls[ML_THREADS];      // 2-bit class per warp: 0 -, 1 level 3, 2/3 level 2 (16/8)
+  __shared__ unsigned char s_l2[NW][ML_THREADS];    // per-warp level-2 slots (16 nodes from the front, 8 from the back)
+  __shared__ unsigned char s_l3[NW][ML_THREADS];    // per-warp level-3 slots
+  __shared__ int s_cnt[NW];
+  __shared__ float s_core[ML_CHUNK];                // near-zone corrections (each warp owns its points)
+  __shared__ double s_n2[NW][ML_K + ML_KF];         // level-2 node sums per warp
   __shared__ float s_c1[ML_K + ML_KF];              // level-1 coefficients from tau_far_kernel
-  __shared__ float s_c2[ML_THREADS / 32][ML_K];
-  __shared__ float s_c2f[ML_THREADS / 32][ML_KF];
+  __shared__ float s_nbuf[DET ? NW : 1][DET ? ML_NBW : 1];   // near-item values (bit-reproducible mode)
 
   const int row = blockIdx.y;
   const int tile = tile_first + (int)(blockIdx.x / chunks_per_tile), chunk = blockIdx.x % chunks_per_tile;
@@ -366,22 +497,18 @@ tau_ml_kernel(const LineF32* __restrict__ prep, int n_lines, const int2* __restr
   const int n_w = max(0, min(ML_WARP_PTS, n_c - w0));
   const float H2 = 0.5f * (float)(n_w - 1), C2w = (float)w0 + H2;
   const bool use_l2 = H2 >= ML_MIN_H2;
-  // level-2 Chebyshev nodes owned by this lane: (lane & 15), and (lane & 7) of the 8-node set
-  const float xn2 = H2 * c_node16[lane & 15];
-  const float xn2f = H2 * c_node8[lane & 7];
   const float pf = (float)(w0 + lane * P);                   // this lane's first point
 
-  for (int i = tid; i < ML_CHUNK; i += blockDim.x) s_core[i] = 0.f;
+  for (int i = lane; i < ML_WARP_PTS; i += 32) s_core[w0 + i] = 0.f;
+  if (lane < ML_K + ML_KF) s_n2[warp][lane] = 0.0;
   // read before the first barrier; this CTA writes the slice only after the last one
   if (use_l1 && tid < ML_K + ML_KF) s_c1[tid] = od[(long long)row * out_stride + (c0 - out_first) + tid];
 
   // level-3 sums hold only the lines within ~2 sub-chunk widths (tens of terms), so
-  // plain float accumulation suffices; the 16-node level-2 sums are Kahan-compensated
-  // across rounds, the 8-node ones (far lines, smaller terms) are plain float.
+  // plain float accumulation suffices
   float acc[P];
 #pragma unroll
   for (int m = 0; m < P; ++m) acc[m] = 0.f;
-  float sum2 = 0.f, comp2 = 0.f, sum2f = 0.f;
   unsigned long long n_pass = 0, n_nodes = 0, n_l3 = 0, n_near_items = 0;
 
   // register prefetch of the next round's line records
@@ -398,283 +525,262 @@ tau_ml_kernel(const LineF32* __restrict__ prep, int n_lines, const int2* __restr
     const float d1 = fabsf(jf - C1) - H1;
     const bool lev1 = pass && use_l1 && (d1 > H1 + 1.f);   // tau_far_kernel's line
     const bool inner = pass && !lev1;
-    // near range (points with possibly |z|^2 < MID_Z2) of an inner line, clipped to the chunk
-    const float y2 = L.y * L.y;
-    float hw = -1.0f;                               // near half-width in points (inner lines only)
-    if (inner && !(y2 >= MID_Z2 && L.y >= 0.f)) hw = sqrtf(fmaxf(MID_Z2 - y2, 0.f)) / L.a + 1.0f;
-    int near_lo = 0, near_n = 0;
-    unsigned l3mask = 0;
+    // class of the line for every warp's sub-chunk
+    unsigned cls = 0u;
+    bool any3 = false;
     if (inner) {
-      for (int w = 0; w < n_warps; ++w) {             // same test as the per-warp split below
+      for (int w = 0; w < n_warps; ++w) {
         const int nw = min(ML_WARP_PTS, n_c - w * ML_WARP_PTS);
         if (nw <= 0) break;
         const float h2 = 0.5f * (float)(nw - 1);
-        const bool l2 = h2 >= ML_MIN_H2 && fabsf(jf - ((float)(w * ML_WARP_PTS) + h2)) - h2 > h2 + 1.f;
-        if (!l2) l3mask |= 1u << w;
+        const float d = fabsf(jf - ((float)(w * ML_WARP_PTS) + h2)) - h2;
+        unsigned c = 1u;
+        if (h2 >= ML_MIN_H2 && d > h2 + 1.f) c = d > ML_FAR1 * h2 ? 3u : 2u;
+        any3 |= c == 1u;
+        cls |= c << (2 * w);
       }
     }
-    if (inner && hw >= 0.f && l3mask) {
+    // near range (points with possibly |z|^2 < MID_Z2) of an inner line, clipped to the
+    // chunk, and its middle, where |z|^2 may be below CORE_Z2 (one point of margin each;
+    // every item still picks its formula from its own |z|^2)
+    const float y2 = L.y * L.y;
+    int near_lo = 0, near_n = 0, mid_lo = 0, mid_n = 0;
+    if (inner && any3 && !(y2 >= MID_Z2 && L.y >= 0.f)) {
+      const float hw = sqrtf(fmaxf(MID_Z2 - y2, 0.f)) / L.a + 1.0f;
       const float q = jf + L.b / L.a;                       // centre in points
       const float lo_f = fmaxf(ceilf(q - hw), 0.f);
       const float hi_f = fminf(floorf(q + hw), (float)(n_c - 1));
       if (lo_f <= hi_f) {
         near_lo = (int)lo_f;
         near_n = (int)hi_f - near_lo + 1;
-      }
-    }
-    // default mode: the middle [mid_lo, mid_lo + mid_n) of the near range, where |z|^2 may be
-    // below CORE_Z2 (one point of margin; each item still picks its formula from its own |z|^2)
-    int mid_lo = near_lo, mid_n = 0;
-    if constexpr (!DET) {
-      if (near_n > 0 && y2 < CORE_Z2 && L.y >= 0.f) {
-        const float hw36 = sqrtf(CORE_Z2 - y2) / L.a + 1.0f;
-        const float q = jf + L.b / L.a;
-        const float a0 = fmaxf(ceilf(q - hw36), (float)near_lo);           // clamped before the
-        const float a1 = fminf(floorf(q + hw36), (float)(near_lo + near_n - 1));   // int conversion
-        if (a0 <= a1) {
-          mid_lo = (int)a0;
-          mid_n = (int)a1 - mid_lo + 1;
+        if (y2 < CORE_Z2 && L.y >= 0.f) {
+          const float hw36 = sqrtf(CORE_Z2 - y2) / L.a + 1.0f;
+          const float a0 = fmaxf(ceilf(q - hw36), (float)near_lo);           // clamped before the
+          const float a1 = fminf(floorf(q + hw36), (float)(near_lo + near_n - 1));   // int conversion
+          if (a0 <= a1) {
+            mid_lo = (int)a0;
+            mid_n = (int)a1 - mid_lo + 1;
+          }
         }
       }
     }
-    const int tail_n = near_n - mid_n;
-    // inclusive warp scans: DET the whole near range; default the middles and the tails
-    int near_scan = DET ? near_n : mid_n, tail_scan = tail_n;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-      const int t = __shfl_up_sync(0xffffffffu, near_scan, o);
-      const int u = __shfl_up_sync(0xffffffffu, tail_scan, o);
-      if (lane >= o) {
-        near_scan += t;
-        tail_scan += u;
-      }
-    }
-    const unsigned b2 = __ballot_sync(0xffffffffu, inner);
-    if (lane == 0) s_cnt[0][warp] = __popc(b2);
-    if (lane == 31) {
-      s_cnt[1][warp] = near_scan;
-      s_cnt[2][warp] = tail_scan;
-    }
+    const unsigned b2 = __ballot_sync(FULL_MASK, inner);
+    if (lane == 0) s_cnt[warp] = __popc(b2);
     __syncthreads();
-    int off2 = 0, off3 = 0, offc = 0, n2 = 0, n_near = 0, n_tail = 0;
+    int off2 = 0, n2 = 0;
     for (int w = 0; w < n_warps; ++w) {
-      const int a2 = s_cnt[0][w], a3 = s_cnt[1][w], a4 = s_cnt[2][w];
+      const int a2 = s_cnt[w];
       off2 += (w < warp) ? a2 : 0;
-      off3 += (w < warp) ? a3 : 0;
-      offc += (w < warp) ? a4 : 0;
       n2 += a2;
-      n_near += a3;
-      n_tail += a4;
     }
     if (inner) {
-      MlLine r;
-      r.g = make_float4(jf, L.a, L.b, L.amp_far);
-      asym5_line_coeffs(y2, L.amp_far, r.p, r.q);
-      const float rc = clamped_r(0.f, y2);                      // = rcp(MID_Z2) when y2 < MID_Z2
-      r.h = make_float4(L.y, y2, L.amp, rc * asym5_scaled(rc, r));
       const int slot = off2 + __popc(b2 & ((1u << lane) - 1u));
-      s2[slot] = r;
-      s_seg_mask[slot] = (unsigned char)l3mask;
-      if constexpr (DET) {
-        s_seg_start[slot] = off3 + near_scan - near_n;       // exclusive prefix in slot order
-        s_seg_lo[slot] = (short)near_lo;
-      } else {
-        s_seg_start[slot] = off3 + near_scan - mid_n;
-        s_seg_lo[slot] = (short)mid_lo;
-        s_segc_start[slot] = offc + tail_scan - tail_n;
-        s_segc_lo[slot] = (short)near_lo;
-        s_segc_nl[slot] = (short)(mid_n > 0 ? mid_lo - near_lo : tail_n);
-        s_segc_rlo[slot] = (short)(mid_lo + mid_n);
-      }
-    }
-    if (tid == 0) {
-      s_seg_start[n2] = n_near;
-      if constexpr (!DET) s_segc_start[n2] = n_tail;
+      float4 p, q;
+      asym5_line_coeffs(y2, L.amp_far, p, q);
+      const float rc = clamped_r(0.f, y2);                      // = rcp(MID_Z2) when y2 < MID_Z2
+      s_g[slot] = make_float4(jf, L.a, L.b, L.amp_far);
+      s_h[slot] = make_float4(L.y, y2, L.amp, rc * asym5_poly(rc, L.amp_far, p, q));
+      s_p[slot] = p;
+      s_q[slot] = q;
+      s_nr[slot] = make_short4((short)near_lo, (short)near_n, (short)mid_lo, (short)mid_n);
+      s_cls[slot] = (unsigned short)cls;
     }
     __syncthreads();
     n_pass += (unsigned long long)n2;
 
-    // ---- per-warp split of the inner lines into level 2 (16 nodes; 8 beyond six
-    // sub-chunk half-widths, listed from the back of s_l2) and level 3
-    int n2w = 0, n2fw = 0, n3w = 0, nnw = 0;
+    // ---- this warp's lists: level 2 (16 nodes from the front, 8 from the back), level 3
+    int n2w = 0, n2fw = 0, n3w = 0;
     for (int k = 0; k < n2; k += 32) {
       const int l = k + lane;
-      bool is2 = false, is2f = false, is3 = false, nz = false;
-      if (l < n2) {
-        const float d = fabsf(s2[l].g.x - C2w) - H2;
-        const bool lev2 = use_l2 && d > H2 + 1.f;
-        is2f = lev2 && d > ML_FAR1 * H2;
-        is2 = lev2 && !is2f;
-        is3 = !lev2 && n_w > 0;
-        if constexpr (DET) {   // near points of slot l inside this warp's sub-chunk (level 3 here)
-          const int st = s_seg_start[l], len = s_seg_start[l + 1] - st, lo = s_seg_lo[l];
-          nz = len > 0 && ((s_seg_mask[l] >> warp) & 1u) && lo < w0 + n_w && lo + len > w0;
-        }
-      }
-      const unsigned q2 = __ballot_sync(0xffffffffu, is2), q3 = __ballot_sync(0xffffffffu, is3);
-      const unsigned q2f = __ballot_sync(0xffffffffu, is2f);
+      const unsigned c = l < n2 ? ((unsigned)s_cls[l] >> (2 * warp)) & 3u : 0u;
+      const unsigned q3 = __ballot_sync(FULL_MASK, c == 1u), q2 = __ballot_sync(FULL_MASK, c == 2u);
+      const unsigned q2f = __ballot_sync(FULL_MASK, c == 3u);
       const unsigned lt = (1u << lane) - 1u;
-      if (is2) s_l2[warp][n2w + __popc(q2 & lt)] = (unsigned char)l;
-      if (is2f) s_l2[warp][ML_THREADS - 1 - (n2fw + __popc(q2f & lt))] = (unsigned char)l;
-      if (is3) s_l3[warp][n3w + __popc(q3 & lt)] = (unsigned char)l;
+      if (c == 2u) s_l2[warp][n2w + __popc(q2 & lt)] = (unsigned char)l;
+      if (c == 3u) s_l2[warp][ML_THREADS - 1 - (n2fw + __popc(q2f & lt))] = (unsigned char)l;
+      if (c == 1u) s_l3[warp][n3w + __popc(q3 & lt)] = (unsigned char)l;
       n2w += __popc(q2);
       n2fw += __popc(q2f);
       n3w += __popc(q3);
-      if constexpr (DET) {
-        const unsigned qn = __ballot_sync(0xffffffffu, nz);
-        if (nz) s_nl[warp][nnw + __popc(qn & lt)] = (unsigned char)l;
-        nnw += __popc(qn);
-      }
     }
     __syncwarp();
 
-    // ---- level 2: half-warps take one line each, lane (& 15) = node
-    {
-      float a2 = 0.f;
-      for (int i = lane >> 4; i < n2w; i += 2) {
-        const MlLine R = s2[s_l2[warp][i]];
-        const float e = C2w - R.g.x;                          // exact: half-integer minus integer
-        const float x = fmaf(xn2 + e, R.g.y, -R.g.z);
-        a2 += line_value(x, R);
-      }
-      kahan_add(sum2, comp2, a2);
-      // far level-2 lines: quarter-warps take one line each, lane (& 7) = node
-      for (int i = lane >> 3; i < n2fw; i += 4) {
-        const MlLine R = s2[s_l2[warp][ML_THREADS - 1 - i]];
-        const float x = fmaf(xn2f + (C2w - R.g.x), R.g.y, -R.g.z);
-        sum2f += line_value(x, R);
-      }
-      if (lane == 0) n_nodes += (unsigned long long)n2w * ML_K + (unsigned long long)n2fw * ML_KF;
-    }
-
-    // ---- level 3, far part: every point of the warp, |z|^2 clamped (branch-free)
-    for (int i = 0; i < n3w; ++i) {
-      const MlLine R = s2[s_l3[warp][i]];
-      const float x0 = fmaf(pf - R.g.x, R.g.y, -R.g.z);
+    // ---- level 2, one lane per line; node sums reduced once per round
+    if (n2w > 0) {
+      float f[ML_K];
 #pragma unroll
-      for (int m = 0; m < P; ++m) {
-        const float r = clamped_r(fmaf((float)m, R.g.y, x0), R.h.y);
-        acc[m] = fmaf(r, asym5_scaled(r, R), acc[m]);
+      for (int k = 0; k < ML_K; ++k) f[k] = 0.f;
+      level2_lines<ML_K>(f, s_l2[warp], 1, n2w, s_g, s_h, s_p, s_q, C2w, H2, lane);
+      const float v = reduce16_transposed(f, lane);
+      if (!(lane & 1)) s_n2[warp][(lane >> 1) & 15] += (double)v;
+    }
+    if (n2fw > 0) {
+      float f[ML_KF];
+#pragma unroll
+      for (int k = 0; k < ML_KF; ++k) f[k] = 0.f;
+      level2_lines<ML_KF>(f, &s_l2[warp][ML_THREADS - 1], -1, n2fw, s_g, s_h, s_p, s_q, C2w, H2, lane);
+      const float v = reduce8_transposed(f, lane);
+      if (!(lane & 3)) s_n2[warp][ML_K + ((lane >> 2) & 7)] += (double)v;
+    }
+    if (lane == 0) n_nodes += (unsigned long long)n2w * ML_K + (unsigned long long)n2fw * ML_KF;
+
+    // ---- level 3: every point of the warp
+    const float xw_lo = (float)w0, xw_hi = (float)(w0 + n_w - 1);
+    for (int i = 0; i < n3w; ++i) {
+      const int l = s_l3[warp][i];
+      const float4 g = s_g[l], h = s_h[l];
+      const float x0 = fmaf(pf - g.x, g.y, -g.z);
+      // |x| at the sub-chunk point nearest to the line centre (0 if it lies inside)
+      const float xmin = fmaxf(fmaxf(fmaf(xw_lo - g.x, g.y, -g.z), -fmaf(xw_hi - g.x, g.y, -g.z)), 0.f);
+      if (h.x >= 0.f && fmaf(xmin, xmin, h.y) >= FAR_Z2) {        // far from every point: two terms
+        const float ny2 = -2.0f * h.y;
+#pragma unroll
+        for (int m = 0; m < P; ++m) far_wing_add(acc[m], fmaf((float)m, g.y, x0), h.y, ny2, g.w);
+      } else {                                                    // |z|^2 clamped to >= MID_Z2
+        const float4 p = s_p[l], q = s_q[l];
+#pragma unroll
+        for (int m = 0; m < P; ++m) {
+          const float r = clamped_r(fmaf((float)m, g.y, x0), h.y);
+          acc[m] = fmaf(r, asym5_poly(r, g.w, p, q), acc[m]);
+        }
       }
     }
     if (lane == 0) n_l3 += (unsigned long long)n3w * n_w;
-    // ---- level 3, near part, spread over the CTA: near item i is point
-    // s_seg_lo[l] + (i - s_seg_start[l]) of inner line l. It gets (accurate value -
-    // clamped loop value) if the line is level 3 for the warp owning the point and
-    // |z|^2 < MID_Z2 there; x is formed exactly as in the loop, so the clamped value
-    // cancels. Consecutive threads take consecutive points of a line. Where near
-    // zones of several lines overlap, the shared-memory atomics add in scheduling
-    // order (results reproducible to rounding, ~1e-9 relative).
-    if constexpr (!DET) {
-      auto near_item = [&](int l, int p) {
-        if (!((s_seg_mask[l] >> (p >> 8)) & 1u)) return;   // level 2 for the owning warp
-        const MlLine R = s2[l];
-        const float x0 = fmaf((float)(p & ~(P - 1)) - R.g.x, R.g.y, -R.g.z);
-        const float x = fmaf((float)(p & (P - 1)), R.g.y, x0);
-        const float z2 = fmaf(x, x, R.h.y);
-        if (z2 >= MID_Z2) return;
-        float v;
-        if (z2 >= CORE_Z2 && R.h.x >= 0.f) v = R.h.z * re_w_cf32(x, R.h.x, z2);
-        else v = (float)((double)R.h.z * weideman_re_f32((double)x, (double)R.h.x));
-        atomicAdd(&s_core[p], v - R.h.w);
+
+    // ---- near zones of the warp's level-3 lines inside its points, 32 lines at a time
+    for (int j0 = 0; j0 < n3w; j0 += 32) {
+      const int j = j0 + lane;
+      int slot = 0, lo = 0, mlo = 0, mhi = 0, mn = 0, tn = 0, ln = 0;
+      if (j < n3w) {
+        slot = s_l3[warp][j];
+        const short4 nr = s_nr[slot];
+        const int a0 = max((int)nr.x, w0), a1 = min((int)nr.x + (int)nr.y, w0 + n_w);
+        if (a1 > a0) {
+          lo = a0;
+          mlo = max((int)nr.z, a0);
+          mhi = min((int)nr.z + (int)nr.w, a1);
+          mn = max(0, mhi - mlo);
+          if (mn == 0) mlo = mhi = a1;                  // no middle here: all of it is the left tail
+          tn = (a1 - a0) - mn;
+          ln = mlo - a0;                                // left tail [a0, mlo), right tail [mhi, a1)
+        }
+      }
+      int mo = mn, to = tn;                             // inclusive scans, then exclusive offsets
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const int u = __shfl_up_sync(FULL_MASK, mo, o), w = __shfl_up_sync(FULL_MASK, to, o);
+        if (lane >= o) {
+          mo += u;
+          to += w;
+        }
+      }
+      const int M = __shfl_sync(FULL_MASK, mo, 31), T = __shfl_sync(FULL_MASK, to, 31);
+      mo -= mn;
+      to -= tn;
+      // item t of a space lies in the run of the last lane whose offset is <= t
+      auto owner = [&](int off, int t) {
+        int o = 0;
+#pragma unroll
+        for (int s = 16; s >= 1; s >>= 1)
+          if (__shfl_sync(FULL_MASK, off, o + s) <= t) o += s;
+        return o;
       };
-      // the middles (float64 core), then the tails (continued fraction)
-      for (int i = tid; i < n_near; i += blockDim.x) {
-        int l = 0, hi = n2;                               // largest l with s_seg_start[l] <= i
-        while (hi - l > 1) {
-          const int mid = (l + hi) >> 1;
-          if (s_seg_start[mid] <= i) l = mid; else hi = mid;
-        }
-        near_item(l, s_seg_lo[l] + (i - s_seg_start[l]));
-      }
-      for (int i = tid; i < n_tail; i += blockDim.x) {
-        int l = 0, hi = n2;                               // largest l with s_segc_start[l] <= i
-        while (hi - l > 1) {
-          const int mid = (l + hi) >> 1;
-          if (s_segc_start[mid] <= i) l = mid; else hi = mid;
-        }
-        const int k = i - s_segc_start[l], nl = s_segc_nl[l];
-        near_item(l, k < nl ? s_segc_lo[l] + k : s_segc_rlo[l] + (k - nl));
-      }
-    } else {
-      // Bit-reproducible variant, in two phases so that the sums do not depend on thread
-      // scheduling. Phase 1 spreads the near items over the CTA: item i is point
-      // s_seg_lo[l] + (i - s_seg_start[l]) of inner line l; its value is (accurate value -
-      // clamped loop value) if the line is level 3 for the warp owning the point and
-      // |z|^2 < MID_Z2 there (x is formed exactly as in the loop, so the clamped value
-      // cancels), else 0. Phase 2: every thread adds the values of its own points in slot
-      // order. Items go through a buffer of ML_NB at a time.
-      for (int nb0 = 0; nb0 < n_near; nb0 += ML_NB) {
-        const int nb1 = min(n_near, nb0 + ML_NB);
-        for (int i = nb0 + tid; i < nb1; i += blockDim.x) {
-          int l = 0, hi = n2;                               // largest l with s_seg_start[l] <= i
-          while (hi - l > 1) {
-            const int mid = (l + hi) >> 1;
-            if (s_seg_start[mid] <= i) l = mid; else hi = mid;
-          }
-          const int p = s_seg_lo[l] + (i - s_seg_start[l]);
-          float v = 0.f;
-          if ((s_seg_mask[l] >> (p >> 8)) & 1u) {            // level 3 for the owning warp
-            const MlLine R = s2[l];
-            const float x0 = fmaf((float)(p & ~(P - 1)) - R.g.x, R.g.y, -R.g.z);
-            const float x = fmaf((float)(p & (P - 1)), R.g.y, x0);
-            const float z2 = fmaf(x, x, R.h.y);
-            if (z2 < MID_Z2) {
-              if (z2 >= CORE_Z2 && R.h.x >= 0.f) v = R.h.z * re_w_cf32(x, R.h.x, z2);
-              else v = (float)((double)R.h.z * weideman_re_f32((double)x, (double)R.h.x));
-              v -= R.h.w;
+      // point of item t of the middles (mid) or tails space, and the item's line slot
+      auto locate = [&](bool mid, int t, int& p, int& sl) {
+        const int o = owner(mid ? mo : to, t);
+        const int k = t - __shfl_sync(FULL_MASK, mid ? mo : to, o);
+        const int m_lo = __shfl_sync(FULL_MASK, mlo, o), t_lo = __shfl_sync(FULL_MASK, lo, o);
+        const int t_ln = __shfl_sync(FULL_MASK, ln, o), t_hi = __shfl_sync(FULL_MASK, mhi, o);
+        sl = __shfl_sync(FULL_MASK, slot, o);
+        p = mid ? m_lo + k : (k < t_ln ? t_lo + k : t_hi + (k - t_ln));
+      };
+      if constexpr (!DET) {
+        // values added by shared-memory atomics: overlapping near zones of two lines in one
+        // 32-item step meet at a point in an order the hardware picks (~1e-9 relative)
+        for (int pass_mid = 1; pass_mid >= 0; --pass_mid) {
+          const bool mid = pass_mid;
+          const int total = mid ? M : T;
+          for (int it0 = 0; it0 < total; it0 += 32) {
+            const int t = min(it0 + lane, total - 1);
+            int p, sl;
+            locate(mid, t, p, sl);
+            if (it0 + lane < total) {
+              const float v = near_correction(p, s_g[sl], s_h[sl]);
+              if (v != 0.f) atomicAdd(&s_core[p], v);
             }
           }
-          s_nbuf[i - nb0] = v;
         }
-        __syncthreads();
-        const int q0 = w0 + lane * P;                       // this thread's points [q0, q0 + P)
-        for (int j = 0; j < nnw; ++j) {                     // slots with near points in this warp, in order
-          const int l = s_nl[warp][j];
-          const int st = s_seg_start[l], en = s_seg_start[l + 1];
-          if (en <= nb0 || st >= nb1) continue;
-          const int lo = s_seg_lo[l];
-          const int pa = max(q0, lo + (max(st, nb0) - st)), pb = min(q0 + P, lo + (min(en, nb1) - st));
-          for (int p = pa; p < pb; ++p) s_core[p] += s_nbuf[st + (p - lo) - nb0];
+      } else {
+        // bit-reproducible: values go through a buffer; then the lines add theirs in
+        // list order, middles before tails, each line's points spread over the lanes
+        for (int pass_mid = 1; pass_mid >= 0; --pass_mid) {
+          const bool mid = pass_mid;
+          const int total = mid ? M : T;
+          for (int b0 = 0; b0 < total; b0 += ML_NBW) {
+            const int b1 = min(total, b0 + ML_NBW);
+            for (int it0 = b0; it0 < b1; it0 += 32) {
+              const int t = min(it0 + lane, b1 - 1);
+              int p, sl;
+              locate(mid, t, p, sl);
+              if (it0 + lane < b1) s_nbuf[warp][t - b0] = near_correction(p, s_g[sl], s_h[sl]);
+            }
+            __syncwarp();
+            for (int jl = 0; jl < 32; ++jl) {
+              const int st = __shfl_sync(FULL_MASK, mid ? mo : to, jl), n = __shfl_sync(FULL_MASK, mid ? mn : tn, jl);
+              const int m_lo = __shfl_sync(FULL_MASK, mlo, jl), t_lo = __shfl_sync(FULL_MASK, lo, jl);
+              const int t_ln = __shfl_sync(FULL_MASK, ln, jl), t_hi = __shfl_sync(FULL_MASK, mhi, jl);
+              const int ia = max(st, b0), ib = min(st + n, b1);
+              for (int it = ia + lane; it < ib; it += 32) {
+                const int k = it - st;
+                const int p = mid ? m_lo + k : (k < t_ln ? t_lo + k : t_hi + (k - t_ln));
+                s_core[p] += s_nbuf[warp][it - b0];
+              }
+              __syncwarp();
+            }
+          }
         }
-        if (nb1 < n_near) __syncthreads();                  // the buffer is refilled
       }
+      if (lane == 0) n_near_items += (unsigned long long)(M + T);
     }
-    if (tid == 0) n_near_items += (unsigned long long)(DET ? n_near : n_near + n_tail);
     // No barrier here: the next round writes the staging arrays only after its first
     // barrier, which every warp reaches after finishing this round.
   }
-  __syncthreads();
+  __syncthreads();                                  // s_c1 visible even when no round ran
 
-  // ---- level-2 node values of this warp: lanes j and j+16 hold halves of node j
-  {
-    float f2 = sum2 - comp2;
-    f2 += __shfl_xor_sync(0xffffffffu, f2, 16);
-    double c = 0.0;
-    for (int j = 0; j < ML_K; ++j) {
-      const float fj = __shfl_sync(0xffffffffu, f2, j);
-      c += (double)fj * c_dct16[(lane & 15) * ML_K + j];
+  // ---- one Chebyshev series per sub-chunk: level-2 node sums + the 8-node interpolant
+  // + the level-1 series, at the 16 nodes, transformed back to coefficients
+  const float inv_h1 = use_l1 ? 1.0f / H1 : 0.f, inv_h2 = use_l2 ? 1.0f / H2 : 0.f;
+  float cw[ML_K];
+#pragma unroll
+  for (int k = 0; k < ML_K; ++k) cw[k] = 0.f;
+  if (use_l2) {
+    double c8 = 0.0;
+    if (lane < ML_KF) {
+      for (int j = 0; j < ML_KF; ++j) c8 += s_n2[warp][ML_K + j] * c_dct8[lane * ML_KF + j];
+      c8 *= 2.0 / ML_KF;
     }
-    if (lane < ML_K) s_c2[warp][lane] = use_l2 ? (float)(c * (2.0 / ML_K)) : 0.f;
-    // 8-node set: lanes j, j+8, j+16, j+24 hold quarters of node j
-    float g2 = sum2f;
-    g2 += __shfl_xor_sync(0xffffffffu, g2, 16);
-    g2 += __shfl_xor_sync(0xffffffffu, g2, 8);
-    double cf = 0.0;
-    for (int j = 0; j < ML_KF; ++j) {
-      const float gj = __shfl_sync(0xffffffffu, g2, j);
-      cf += (double)gj * c_dct8[(lane & 7) * ML_KF + j];
+    float c8f[ML_KF];
+#pragma unroll
+    for (int k = 0; k < ML_KF; ++k) c8f[k] = (float)__shfl_sync(FULL_MASK, c8, k);
+    const int jn = lane & 15;
+    const float tj = c_node16[jn];
+    double fj = s_n2[warp][jn] + (double)clenshaw16<ML_KF>(c8f, tj);
+    if (use_l1) {
+      const float t1 = fmaf(H2, tj, C2w - C1) * inv_h1;
+      fj += (double)(clenshaw16(s_c1, t1) + clenshaw16<ML_KF>(s_c1 + ML_K, t1));
     }
-    if (lane < ML_KF) s_c2f[warp][lane] = use_l2 ? (float)(cf * (2.0 / ML_KF)) : 0.f;
+    double ck = 0.0;
+#pragma unroll
+    for (int j = 0; j < ML_K; ++j) ck += __shfl_sync(FULL_MASK, fj, j) * c_dct16[jn * ML_K + j];
+    ck *= 2.0 / ML_K;
+#pragma unroll
+    for (int k = 0; k < ML_K; ++k) cw[k] = (float)__shfl_sync(FULL_MASK, ck, k);
   }
-  __syncthreads();
+  __syncwarp();
 
   const double T = t_layer[row];
+  const float half_c2_t = (float)(0.5 * C2 / T);
   float* out = od + (long long)row * out_stride;   // points [out_first, out_first + out_stride) of the grid
-  float c2[ML_K];
-#pragma unroll
-  for (int k = 0; k < ML_K; ++k) c2[k] = s_c2[warp][k];
-  const float inv_h1 = use_l1 ? 1.0f / H1 : 0.f, inv_h2 = use_l2 ? 1.0f / H2 : 0.f;
   bool bad = false;
 #pragma unroll
   for (int m = 0; m < P; ++m) {
@@ -682,16 +788,14 @@ tau_ml_kernel(const LineF32* __restrict__ prep, int n_lines, const int2* __restr
     if (pl < n_c) {
       const long long p = c0 + pl;
       float v = s_core[pl];
-      if (use_l1) {
+      if (use_l2) {
+        v += clenshaw16(cw, ((float)pl - C2w) * inv_h2);
+      } else if (use_l1) {
         const float t1 = ((float)pl - C1) * inv_h1;
         v += clenshaw16(s_c1, t1) + clenshaw16<ML_KF>(s_c1 + ML_K, t1);
       }
-      if (use_l2) {
-        const float t2 = ((float)pl - C2w) * inv_h2;
-        v += clenshaw16(c2, t2) + clenshaw16<ML_KF>(s_c2f[warp], t2);
-      }
-      const double nu = grid_nu(nu_min, step, p);
-      const float o = (float)(((double)acc[m] + (double)v) * radiation_term_grid(nu, T));
+      const float nu = (float)grid_nu(nu_min, step, p);
+      const float o = (acc[m] + v) * (nu * tanhf(nu * half_c2_t));   // R(nu, T) = nu tanh(c2 nu / 2T)
       bad |= !isfinite(o);
       out[p - out_first] = o;
     }

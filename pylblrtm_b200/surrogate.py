@@ -443,11 +443,45 @@ class MLP:
 # ---------------------------------------------------------------------------
 # Ensemble, gate and fallback
 
+def gate_threshold(est: np.ndarray, err: np.ndarray, target: float = 1e-3, quantile: float = 0.999,
+                   margin: float = 0.5) -> float:
+    """Largest gate t on the error estimate such that the profiles it accepts
+    (est <= t) keep their ``quantile`` of the true error at or below ``target``, with
+    room to spare: among the accepted, at most ``margin * (1 - quantile)`` of them may
+    exceed ``target``. ``est`` and ``err`` are per-profile arrays of a calibration
+    split (estimate and true max-channel error). Returns 0 when nothing qualifies."""
+    est = np.asarray(est, dtype=np.float64)
+    err = np.asarray(err, dtype=np.float64)
+    order = np.argsort(est, kind="stable")
+    e_sorted, bad = est[order], np.cumsum(err[order] > target)
+    k = np.arange(1, est.size + 1)
+    ok = bad <= margin * (1.0 - quantile) * k
+    # a threshold must accept every profile with the same estimate: stop where est changes
+    last_of_value = np.r_[e_sorted[1:] != e_sorted[:-1], True]
+    cand = np.flatnonzero(ok & last_of_value)
+    return float(e_sorted[cand[-1]]) if cand.size else 0.0
+
+
+def channel_weights(spread: np.ndarray, err: np.ndarray, q: float = 0.99, floor: float = 1e-12) -> np.ndarray:
+    """Per-channel factors that put each channel's ensemble spread on the scale of its
+    true error: the ratio of their ``q`` quantiles over a calibration split
+    ([n_profiles, n_channels] each), normalised to a median of 1."""
+    s = np.quantile(np.asarray(spread, dtype=np.float64), q, axis=0)
+    e = np.quantile(np.asarray(err, dtype=np.float64), q, axis=0)
+    w = e / np.maximum(s, floor)
+    w = np.where(np.isfinite(w) & (w > 0), w, 1.0)
+    return (w / np.median(w)).astype(np.float32)
+
+
 class GatedSurrogate:
-    """4-member ensemble with a spread gate and float32-engine fallback."""
+    """4-member ensemble with a spread gate and float32-engine fallback.
+
+    A profile is flagged when ``scale * max_c(ch_scale[c] * std_c) > gate``, std_c the
+    members' spread in channel c; :func:`calibrate_gate` fits ``ch_scale`` and ``gate``
+    on a calibration split so that accepted profiles meet an error target."""
 
     def __init__(self, members: Sequence[MLP], gate: float = 1e-3, scale: float = 1.0,
-                 deterministic: bool = False):
+                 deterministic: bool = False, ch_scale: Optional[np.ndarray] = None):
         if not members:
             raise ValueError("at least one member")
         self.members = list(members)
@@ -455,9 +489,19 @@ class GatedSurrogate:
         self.deterministic = bool(deterministic)      # of the engine fallback
         self.torch = members[0].torch
         self.launches = 0
+        self.ch_scale = None
+        if ch_scale is not None:
+            w = np.ascontiguousarray(ch_scale, dtype=np.float32).reshape(-1)
+            if w.size != members[0].n_out:
+                raise ValueError(f"ch_scale needs {members[0].n_out} values, got {w.size}")
+            self.ch_scale = self.torch.as_tensor(w, device=members[0].dev)
 
-    def ensemble(self, raw):
-        """(mean [B, n_out], est [B], flag [B] bool) on the device."""
+    def predictions(self, raw):
+        """Every member's channel predictions [n_members, B, n_out] (device)."""
+        pred, B = self._members(raw)
+        return pred[:, :B, :self.members[0].n_out]
+
+    def _members(self, raw):
         torch = self.torch
         net0 = self.members[0]
         B = raw.shape[0]
@@ -474,11 +518,19 @@ class GatedSurrogate:
                 ws.raw[B:].zero_()
             net._forward(ws, stream, False, out=pred[m])
             self.launches += net.launches
+        return pred, B
+
+    def ensemble(self, raw):
+        """(mean [B, n_out], est [B], flag [B] bool) on the device."""
+        torch = self.torch
+        net0 = self.members[0]
+        pred, B = self._members(raw)
+        Bp, n_pad = pred.shape[1], pred.shape[2]
         mean = torch.empty((B, net0.n_out), dtype=torch.float32, device=net0.dev)
         est = torch.empty((B,), dtype=torch.float32, device=net0.dev)
         flag = torch.empty((B,), dtype=torch.int32, device=net0.dev)
         _lib.call("lbl_ensemble_gate", pred.data_ptr(), len(self.members), Bp * n_pad, B, n_pad, net0.n_out,
-                  self.scale, self.gate, mean.data_ptr(), est.data_ptr(), flag.data_ptr(),
+                  _lib.ptr(self.ch_scale), self.scale, self.gate, mean.data_ptr(), est.data_ptr(), flag.data_ptr(),
                   torch.cuda.current_stream().cuda_stream)
         self.launches += 1
         return mean, est, flag.bool()
@@ -508,6 +560,32 @@ class GatedSurrogate:
         if timings is not None:
             timings.update({"surrogate_s": t1 - t0, "fallback_s": t2 - t1, "n_flagged": int(idx.size)})
         return mean, est, flag
+
+
+def calibrate_gate(gs: "GatedSurrogate", raw, reference: np.ndarray, target: float = 1e-3,
+                   quantile: float = 0.999, margin: float = 0.5) -> dict:
+    """Fit the gate of ``gs`` on a calibration split: ``raw`` features [n, 61] and the
+    engine's channel transmittances ``reference`` [n, n_out] of the same profiles (not
+    used in training). Sets ``gs.ch_scale`` (:func:`channel_weights` of the members'
+    spread against the ensemble mean's error), ``gs.gate`` (:func:`gate_threshold` of
+    the weighted estimate) and ``gs.scale = 1``; returns the fitted values and the
+    split's accepted fraction and accepted-error quantile."""
+    torch = gs.torch
+    pred = gs.predictions(torch.as_tensor(raw, device=gs.members[0].dev))
+    mean = pred.mean(0)
+    spread = pred.std(0, unbiased=False).cpu().numpy()
+    err_c = np.abs(mean.cpu().numpy() - np.asarray(reference, dtype=np.float32))
+    w = channel_weights(spread, err_c)
+    est = (spread * w[None, :]).max(1)
+    err = err_c.max(1)
+    t = gate_threshold(est, err, target, quantile, margin)
+    gs.ch_scale = torch.as_tensor(w, device=gs.members[0].dev)
+    gs.gate, gs.scale = float(t), 1.0
+    acc = est <= t
+    return {"gate": float(t), "profiles": int(est.size), "accepted": float(acc.mean()),
+            "accepted_err_quantile": float(np.quantile(err[acc], quantile)) if acc.any() else None,
+            "spread_vs_error_corr": float(np.corrcoef(est, err)[0, 1]) if est.size > 1 else None,
+            "target": target, "quantile": quantile, "margin": margin}
 
 
 # ---------------------------------------------------------------------------

@@ -7,13 +7,18 @@ Steps (all on one GPU):
      transmittances (650-1150 cm^-1, 0.25 cm^-1 channels, grid step 0.001) with the
      float32 line-by-line engine: the training targets;
   2. train a 4-member ensemble (61 -> 1024 x 4 -> 2000, BF16, Adam, batch 4096);
-  3. draw ``--eval`` fresh profiles plus a fraction ``--ood`` shifted by +25 K, compute
+  3. calibrate the gate on ``--calibrate`` further in-distribution profiles with their
+     engine spectra (per-channel spread weights and a threshold such that accepted
+     profiles keep the 99.9th percentile of their maximum channel error <= ``--gate``;
+     ``--calibrate 0`` keeps the raw spread compared with ``--gate``);
+  4. draw ``--eval`` fresh profiles plus a fraction ``--ood`` shifted by +25 K, compute
      their engine spectra (the reference values for the surrogate's errors, and the engine's
      own spectra/s),
      run the ensemble (surrogate-only spectra/s), and the gated path that recomputes
      flagged profiles with the engine (blended spectra/s);
-  4. report per-profile maximum channel errors (quantiles, fraction <= 1e-3) for the
-     ensemble mean and for the gated output, split in/out of distribution.
+  5. report per-profile maximum channel errors (quantiles, fraction <= 1e-3) for the
+     ensemble mean, the profiles the gate accepts and the gated output, split in/out of
+     distribution.
 
 The line list is the three-gas synthetic list (200,000 lines over 600-2500 cm^-1)
 restricted to the window plus the cutoff; ``--strength-scale`` multiplies every line
@@ -49,7 +54,7 @@ def line_list(n_lines: int, problem: surrogate.SurrogateProblem, strength_scale:
 def run(n_train: int = 100_000, n_eval: int = 65_536, ood: float = 0.05, steps: int = 20_000,
         members: int = 4, batch: int = 4096, hidden: int = 1024, depth: int = 4, lr: float = 1e-3,
         strength_scale: float = 1e-4, n_lines: int = 200_000, gate: float = 1e-3, seed: int = 0,
-        profiles_per_launch: int = 256, infer_batch: int = 0, log=print) -> dict:
+        profiles_per_launch: int = 256, infer_batch: int = 0, n_calibrate: int = 8192, log=print) -> dict:
     """The study; ``infer_batch`` > 0 also times surrogate-only inference on that many
     fresh profiles (features only, no engine reference)."""
     import torch
@@ -86,7 +91,16 @@ def run(n_train: int = 100_000, n_eval: int = 65_536, ood: float = 0.05, steps: 
                        "final_mse": [float(np.mean(n.train_losses[-50:])) for n in nets]}
     log(f"training: {members} x {steps} steps in {t_train:.1f} s")
 
-    # 3. evaluation profiles and their engine spectra
+    # 3. gate calibration on a split of its own
+    gs = surrogate.GatedSurrogate(nets, gate=gate)
+    if n_calibrate:
+        cal = surrogate.sample_profiles(n_calibrate, seed=seed + 5)
+        y_cal = surrogate.engine_channels(sd, cal, problem, profiles_per_launch=profiles_per_launch)
+        rep["calibration"] = surrogate.calibrate_gate(gs, cal.features(), y_cal, target=gate)
+        log(f"gate calibrated on {n_calibrate} profiles: threshold {gs.gate:.3e}, "
+            f"accepted {rep['calibration']['accepted']:.4f}")
+
+    # 4. evaluation profiles and their engine spectra
     n_ood = int(round(ood * n_eval))
     ev_in = surrogate.sample_profiles(n_eval, seed=seed + 2)
     ev_ood = surrogate.sample_profiles(n_ood, seed=seed + 3, t_offset=25.0) if n_ood else None
@@ -100,7 +114,6 @@ def run(n_train: int = 100_000, n_eval: int = 65_536, ood: float = 0.05, steps: 
     t_eng = time.perf_counter() - t0
     log(f"engine on {len(ev)} evaluation profiles: {t_eng:.1f} s")
 
-    gs = surrogate.GatedSurrogate(nets, gate=gate)
     raw = torch.as_tensor(ev.features(), device=nets[0].dev)
     gs.ensemble(raw[:1024])                                       # warm-up (workspaces)
     torch.cuda.synchronize()
@@ -144,13 +157,15 @@ def run(n_train: int = 100_000, n_eval: int = 65_536, ood: float = 0.05, steps: 
             "profiles": infer_batch, "seconds": t_big, "spectra_per_s": infer_batch / t_big,
             "tflops": rep["throughput"]["gemm_flops_per_spectrum"] * infer_batch / t_big / 1e12,
             "launches": gs.launches}
-    rep["gate"] = {"gate": gate, "flagged_in": float(flag_h[~is_ood].mean()),
+    rep["gate"] = {"gate": gs.gate, "target": gate, "calibrated": bool(n_calibrate),
+                   "flagged_in": float(flag_h[~is_ood].mean()),
                    "flagged_ood": float(flag_h[is_ood].mean()) if n_ood else None,
                    "n_flagged": int(flag_h.sum()), "n_eval": len(ev)}
     rep["errors"] = {
         "surrogate_in": _quantiles(err_sur[~is_ood]),
         "surrogate_ood": _quantiles(err_sur[is_ood]),
         "accepted": _quantiles(err_sur[acc]),
+        "accepted_in": _quantiles(err_sur[acc & ~is_ood]),
         "gated_all": _quantiles(err_gated),
         "channel_abs_err_in": _quantiles(np.abs(mean_h - ref)[~is_ood].ravel()),
         "spread_vs_error_corr": float(np.corrcoef(est_h, err_sur)[0, 1]),
@@ -201,6 +216,7 @@ def main(argv=None) -> None:
     ap.add_argument("--gate", type=float, default=1e-3)
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--infer-batch", type=int, default=0)
+    ap.add_argument("--calibrate", type=int, default=8192, help="calibration profiles for the gate (0: none)")
     ap.add_argument("--profiles-per-launch", type=int, default=256)
     ap.add_argument("--infer-only", action="store_true",
                     help="only time surrogate inference on --infer-batch profiles (random weights)")
@@ -211,7 +227,8 @@ def main(argv=None) -> None:
         print(json.dumps(rep))
         return
     rep = run(a.train, a.eval, a.ood, a.steps, a.members, a.batch, a.hidden, a.depth, a.lr, a.strength_scale,
-              a.lines, a.gate, a.seed, profiles_per_launch=a.profiles_per_launch, infer_batch=a.infer_batch)
+              a.lines, a.gate, a.seed, profiles_per_launch=a.profiles_per_launch, infer_batch=a.infer_batch,
+              n_calibrate=a.calibrate)
     text = json.dumps(rep, indent=1)
     print(text)
     if a.out:

@@ -236,7 +236,7 @@ def test_ensemble_gate_matches_numpy(cuda):
     mean = torch.empty((B, n_ch), device="cuda")
     est = torch.empty(B, device="cuda")
     flag = torch.empty(B, dtype=torch.int32, device="cuda")
-    _lib.call("lbl_ensemble_gate", pred.data_ptr(), n_mem, B * ld, B, ld, n_ch, 2.0, 1e-3, mean.data_ptr(),
+    _lib.call("lbl_ensemble_gate", pred.data_ptr(), n_mem, B * ld, B, ld, n_ch, 0, 2.0, 1e-3, mean.data_ptr(),
               est.data_ptr(), flag.data_ptr(), 0)
     torch.cuda.synchronize()
     p = pred[:, :, :n_ch].double().cpu().numpy()
@@ -244,6 +244,14 @@ def test_ensemble_gate_matches_numpy(cuda):
     np.testing.assert_allclose(est.cpu().numpy(), p.std(0).max(1), rtol=1e-3, atol=1e-7)
     np.testing.assert_array_equal(flag.cpu().numpy(), (2.0 * est.cpu().numpy() > 1e-3).astype(np.int32))
     assert flag[:150].sum() == 0 and flag[150:].sum() == 150
+    # per-channel weights (a calibrated gate): est = max_c w_c std_c
+    w = torch.rand(n_ch, generator=g) * 3.0
+    _lib.call("lbl_ensemble_gate", pred.data_ptr(), n_mem, B * ld, B, ld, n_ch, w.cuda().data_ptr(), 1.0, 0.5,
+              mean.data_ptr(), est.data_ptr(), flag.data_ptr(), 0)
+    torch.cuda.synchronize()
+    ref = (p.std(0) * w.double().numpy()[None, :]).max(1)
+    np.testing.assert_allclose(est.cpu().numpy(), ref, rtol=1e-3, atol=1e-7)
+    np.testing.assert_array_equal(flag.cpu().numpy(), (est.cpu().numpy() > 0.5).astype(np.int32))
 
 
 def test_gated_surrogate_against_engine(cuda):
@@ -291,3 +299,18 @@ def test_gated_surrogate_against_engine(cuda):
     torch.cuda.synchronize()
     t_eng = time.perf_counter() - t0
     assert t_eng > 5 * t_sur, (t_eng, t_sur)
+    # calibration on a split of its own: weights and threshold such that the accepted
+    # calibration profiles meet a target; on fresh profiles the accepted error quantile
+    # stays near it (the calibration split and the test set are different draws)
+    cal = surrogate.sample_profiles(2048, seed=4)
+    ref_cal = surrogate.engine_channels(sd, cal, problem, deterministic=True)
+    target = float(np.quantile(err_in, 0.7))
+    fit = surrogate.calibrate_gate(gate, cal.features(), ref_cal, target=target, quantile=0.95, margin=0.5)
+    assert gate.ch_scale is not None and gate.ch_scale.shape == (problem.n_channels,)
+    assert 0.0 < fit["accepted"] < 1.0 and fit["accepted_err_quantile"] <= target
+    mean2, est2, flag2 = gate.ensemble(torch.from_numpy(test_in.features()).cuda())
+    acc = ~flag2.cpu().numpy()
+    err2 = np.abs(mean2.cpu().numpy() - ref_in).max(1)
+    assert acc.any() and np.quantile(err2[acc], 0.95) <= 1.5 * target
+    flag_ood2 = gate.ensemble(torch.from_numpy(test_ood.features()).cuda())[2].cpu().numpy()
+    assert flag_ood2.mean() > flag2.cpu().numpy().mean()
