@@ -22,6 +22,7 @@ from __future__ import annotations
 
 import ctypes
 import math
+import threading
 import warnings
 from dataclasses import dataclass, field
 from typing import Dict, List, Optional, Sequence, Tuple
@@ -329,14 +330,15 @@ class Job:
         self.p_max = layers.p_max_atm() if self.n_lay > 0 else 1.0
         self.nu_first, self.nu_last = grid.nu_at(0), grid.nu_at(grid.n_nu - 1)
         self.h2d_bytes = 0
-        # the line arrays go to the device while the host selects the groups (copies from
-        # page-locked arrays are asynchronous; the first device stage orders after them)
+        # the line arrays go to the device while the host selects the groups
         L = sd.lines
-        self.lines_in = tuple(self._up(L[k], np.float64, non_blocking=True)
-                              for k in ("nu0", "Sref", "g_air", "g_self", "Elow", "n_air", "shift"))
+        staged = self._stage_lines(L)
         st = {}
-        self.groups, gid = select_groups(sd, layers.gases, self.nu_first, self.nu_last, self.cutoff,
-                                         self.p_max, warn_level + 1, stats=st)
+        try:
+            self.groups, gid = select_groups(sd, layers.gases, self.nu_first, self.nu_last, self.cutoff,
+                                             self.p_max, warn_level + 1, stats=st)
+        finally:
+            self.lines_in = self._finish_lines(staged)
         self.n_lines = int(gid.size)
         self.mask_lo, self.mask_hi = band_edges(self.nu_first, self.nu_last, self.cutoff, line_window)
         band_lines = int(st["band_lines"])
@@ -377,6 +379,38 @@ class Job:
         self.grp = tuple(views[len(lay):len(lay) + 6])
         self.gid = views[-1]
         self.pad = float(st["max_abs_shift"]) * self.p_max * (1 + 1e-9) + 1e-9
+
+    LINE_KEYS = ("nu0", "Sref", "g_air", "g_self", "Elow", "n_air", "shift")
+
+    def _stage_lines(self, L):
+        """Start moving the seven float64 line columns to the device. Page-locked columns
+        are copied asynchronously right away; pageable ones (ordinary NumPy arrays) are
+        packed into one page-locked buffer by a worker thread while the caller's thread
+        selects the groups, and :meth:`_finish_lines` then issues one asynchronous copy."""
+        torch = self.torch
+        arrs = [np.ascontiguousarray(L[k], dtype=np.float64) for k in self.LINE_KEYS]
+        n = arrs[0].size
+        if n == 0 or any(a.size != n for a in arrs) or all(torch.from_numpy(a).is_pinned() for a in arrs):
+            return tuple(self._up(a, np.float64, non_blocking=True) for a in arrs)
+        host = torch.empty((len(arrs), n), dtype=torch.float64, pin_memory=True)
+        hb = host.numpy()
+
+        def pack():
+            for i, a in enumerate(arrs):
+                hb[i] = a                    # NumPy copies without holding the GIL
+
+        worker = threading.Thread(target=pack, name="lbl-pack")
+        worker.start()
+        return host, worker
+
+    def _finish_lines(self, staged):
+        if len(staged) == len(self.LINE_KEYS):      # already on its way (page-locked columns)
+            return staged
+        host, worker = staged
+        worker.join()
+        dev = host.to(self.dev, non_blocking=True)   # the caching host allocator keeps host alive
+        self.h2d_bytes += host.numel() * host.element_size()
+        return tuple(dev[i] for i in range(dev.shape[0]))
 
     def _up(self, a, dtype, non_blocking: bool = False):
         t = _upload(self.torch, a, dtype, self.dev, non_blocking)
