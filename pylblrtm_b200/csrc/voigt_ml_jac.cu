@@ -36,7 +36,7 @@ constexpr int MJ_CHUNK = MJ_THREADS * MJ_P;       // 1024 points
 constexpr int MJ_K = 16;
 constexpr float MJ_MIN_H1 = 32.f;
 constexpr float MJ_MIN_H2 = 16.f;
-constexpr int MJ_NB = 1024;                        // near items buffered per batch (dynamic shared memory)
+constexpr int MJ_NBW = 128;                        // near items buffered per warp (bit-reproducible mode)
 
 // Chebyshev node offsets (fractions of the half-width) and DCT weights, row-major [k][j]
 static __constant__ float c_jnode16[MJ_K] = {LBL_CHEB16_NODES};
@@ -376,17 +376,12 @@ jac_ml_kernel(const LineF32* __restrict__ prep, const LineJac* __restrict__ jpre
   __shared__ JLine s2[MJ_THREADS];
   __shared__ unsigned char s_l2[MJ_THREADS / 32][MJ_THREADS];
   __shared__ unsigned char s_l3[MJ_THREADS / 32][MJ_THREADS];
-  __shared__ unsigned char s_nl[MJ_THREADS / 32][MJ_THREADS];   // per-warp slots with near points in it
-  __shared__ int s_cnt[2][MJ_THREADS / 32];
-  __shared__ int s_seg_start[MJ_THREADS + 1];
-  __shared__ short s_seg_lo[MJ_THREADS];
-  __shared__ unsigned char s_seg_mask[MJ_THREADS];
-  __shared__ float s_core[3][MJ_CHUNK];              // near corrections (each point owned by one thread)
-  extern __shared__ float s_nbuf_dyn[];              // near-item values of one batch: [3][MJ_NB]
-  float (*s_nbuf)[MJ_NB] = reinterpret_cast<float (*)[MJ_NB]>(s_nbuf_dyn);
+  __shared__ int s_cnt[MJ_THREADS / 32];
+  __shared__ short4 s_nr[MJ_THREADS];                // near range (lo, n) and its middle (lo, n), chunk points
+  __shared__ float s_core[3][MJ_CHUNK];              // near corrections (each warp owns its points)
+  extern __shared__ float s_nbuf_dyn[];              // bit-reproducible mode: [warp][3][MJ_NBW] near-item values
   __shared__ float s_c1[MJ_NCOEF];                  // level-1 coefficients from jac_far_kernel
-  __shared__ float s_c2[MJ_THREADS / 32][3][MJ_K];
-  __shared__ float s_c2f[MJ_THREADS / 32][3][MJ_KF];
+  __shared__ float s_c2[MJ_THREADS / 32][3][MJ_K];   // merged series of levels 1 and 2 per warp
   __shared__ double s_vjp[2][MJ_THREADS / 32];
 
   const int row = blockIdx.y;
@@ -442,44 +437,45 @@ jac_ml_kernel(const LineF32* __restrict__ prep, const LineJac* __restrict__ jpre
     const bool lev1 = pass && use_l1 && (fabsf(jf - C1) - H1 > H1 + 1.f);   // jac_far_kernel's line
     const bool inner = pass && !lev1;
     const float y2 = L.y * L.y;
-    const float hw = (y2 >= MID_Z2 && L.y >= 0.f) ? -1.0f : sqrtf(fmaxf(MID_Z2 - y2, 0.f)) / L.a + 1.0f;
-    int near_lo = 0, near_n = 0;
-    unsigned l3mask = 0;
+    bool any3 = false;
     if (inner) {
       for (int w = 0; w < n_warps; ++w) {              // same test as the per-warp split below
         const int nw = min(MJ_WARP_PTS, n_c - w * MJ_WARP_PTS);
         if (nw <= 0) break;
         const float h2 = 0.5f * (float)(nw - 1);
-        const bool l2 = h2 >= MJ_MIN_H2 && fabsf(jf - ((float)(w * MJ_WARP_PTS) + h2)) - h2 > h2 + 1.f;
-        if (!l2) l3mask |= 1u << w;
+        any3 |= !(h2 >= MJ_MIN_H2 && fabsf(jf - ((float)(w * MJ_WARP_PTS) + h2)) - h2 > h2 + 1.f);
       }
     }
-    if (inner && hw >= 0.f && l3mask) {
+    // near range (points with possibly |z|^2 < MID_Z2) clipped to the chunk, and its middle
+    // (|z|^2 possibly < CORE_Z2), one point of margin each
+    int near_lo = 0, near_n = 0, mid_lo = 0, mid_n = 0;
+    if (inner && any3 && !(y2 >= MID_Z2 && L.y >= 0.f)) {
+      const float hw = sqrtf(fmaxf(MID_Z2 - y2, 0.f)) / L.a + 1.0f;
       const float q = jf + L.b / L.a;
       const float lo_f = fmaxf(ceilf(q - hw), 0.f);
       const float hi_f = fminf(floorf(q + hw), (float)(n_c - 1));
       if (lo_f <= hi_f) {
         near_lo = (int)lo_f;
         near_n = (int)hi_f - near_lo + 1;
+        if (y2 < CORE_Z2 && L.y >= 0.f) {
+          const float hw36 = sqrtf(CORE_Z2 - y2) / L.a + 1.0f;
+          const float a0 = fmaxf(ceilf(q - hw36), (float)near_lo);
+          const float a1 = fminf(floorf(q + hw36), (float)(near_lo + near_n - 1));
+          if (a0 <= a1) {
+            mid_lo = (int)a0;
+            mid_n = (int)a1 - mid_lo + 1;
+          }
+        }
       }
     }
-    int near_scan = near_n;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-      const int t = __shfl_up_sync(0xffffffffu, near_scan, o);
-      if (lane >= o) near_scan += t;
-    }
     const unsigned b2 = __ballot_sync(0xffffffffu, inner);
-    if (lane == 0) s_cnt[0][warp] = __popc(b2);
-    if (lane == 31) s_cnt[1][warp] = near_scan;
+    if (lane == 0) s_cnt[warp] = __popc(b2);
     __syncthreads();
-    int off2 = 0, off3 = 0, n2 = 0, n_near = 0;
+    int off2 = 0, n2 = 0;
     for (int w = 0; w < n_warps; ++w) {
-      const int a2 = s_cnt[0][w], a3 = s_cnt[1][w];
+      const int a2 = s_cnt[w];
       off2 += (w < warp) ? a2 : 0;
-      off3 += (w < warp) ? a3 : 0;
       n2 += a2;
-      n_near += a3;
     }
     if (inner) {
       JLine r;
@@ -488,29 +484,22 @@ jac_ml_kernel(const LineF32* __restrict__ prep, const LineJac* __restrict__ jpre
       r.k = make_float4(J.jT_y, J.jv_u, J.jv_y, J.jv_x);
       const int slot = off2 + __popc(b2 & ((1u << lane) - 1u));
       s2[slot] = r;
-      s_seg_start[slot] = off3 + near_scan - near_n;
-      s_seg_lo[slot] = (short)near_lo;
-      s_seg_mask[slot] = (unsigned char)l3mask;
+      s_nr[slot] = make_short4((short)near_lo, (short)near_n, (short)mid_lo, (short)mid_n);
     }
-    if (tid == 0) s_seg_start[n2] = n_near;
     __syncthreads();
 
     // per-warp split of the inner lines into level 2 (16 nodes; 8 beyond six sub-chunk
     // half-widths, listed from the back of s_l2) and level 3
-    int n2w = 0, n2fw = 0, n3w = 0, nnw = 0;
+    int n2w = 0, n2fw = 0, n3w = 0;
     for (int k = 0; k < n2; k += 32) {
       const int l = k + lane;
-      bool is2 = false, is2f = false, is3 = false, nz = false;
+      bool is2 = false, is2f = false, is3 = false;
       if (l < n2) {
         const float d = fabsf(s2[l].g.x - C2w) - H2;
         const bool lev2 = use_l2 && d > H2 + 1.f;
         is2f = lev2 && d > MJ_FAR1 * H2;
         is2 = lev2 && !is2f;
         is3 = !lev2 && n_w > 0;
-        if constexpr (DET) {   // near points of slot l inside this warp's sub-chunk (level 3 here)
-          const int st = s_seg_start[l], len = s_seg_start[l + 1] - st, lo = s_seg_lo[l];
-          nz = len > 0 && ((s_seg_mask[l] >> warp) & 1u) && lo < w0 + n_w && lo + len > w0;
-        }
       }
       const unsigned q2 = __ballot_sync(0xffffffffu, is2), q3 = __ballot_sync(0xffffffffu, is3);
       const unsigned q2f = __ballot_sync(0xffffffffu, is2f);
@@ -521,11 +510,6 @@ jac_ml_kernel(const LineF32* __restrict__ prep, const LineJac* __restrict__ jpre
       n2w += __popc(q2);
       n2fw += __popc(q2f);
       n3w += __popc(q3);
-      if constexpr (DET) {
-        const unsigned qn = __ballot_sync(0xffffffffu, nz);
-        if (nz) s_nl[warp][nnw + __popc(qn & lt)] = (unsigned char)l;
-        nnw += __popc(qn);
-      }
     }
     __syncwarp();
     // level 2: half-warps take one line each, lane (& 15) = node
@@ -577,85 +561,123 @@ jac_ml_kernel(const LineF32* __restrict__ prep, const LineJac* __restrict__ jpre
         }
       }
     }
-    // level 3, near correction (accurate - clamped) spread over the CTA; x is formed
-    // exactly as in the loop above, so the clamped values cancel. Where near zones
-    // overlap, the shared-memory atomics add in scheduling order (reproducible to
-    // rounding, ~1e-9 relative).
-    if constexpr (!DET) {
-      for (int i = tid; i < n_near; i += blockDim.x) {
-        int l = 0, hi = n2;                               // largest l with s_seg_start[l] <= i
-        while (hi - l > 1) {
-          const int mid = (l + hi) >> 1;
-          if (s_seg_start[mid] <= i) l = mid; else hi = mid;
+    // level 3, near correction (accurate - clamped) of the warp's level-3 lines at the near
+    // points inside its sub-chunk, 32 lines at a time: the middles (float64 core), then the
+    // tails, as item spaces; lanes take consecutive items and find their line by a shuffle
+    // search. x is formed exactly as in the loop above, so the clamped values cancel.
+    for (int j0 = 0; j0 < n3w; j0 += 32) {
+      const int j = j0 + lane;
+      int slot = 0, lo = 0, mlo = 0, mhi = 0, mn = 0, tn = 0, ln = 0;
+      if (j < n3w) {
+        slot = s_l3[warp][j];
+        const short4 nr = s_nr[slot];
+        const int a0 = max((int)nr.x, w0), a1 = min((int)nr.x + (int)nr.y, w0 + n_w);
+        if (a1 > a0) {
+          lo = a0;
+          mlo = max((int)nr.z, a0);
+          mhi = min((int)nr.z + (int)nr.w, a1);
+          mn = max(0, mhi - mlo);
+          if (mn == 0) mlo = mhi = a1;                  // no middle here: all of it is the left tail
+          tn = (a1 - a0) - mn;
+          ln = mlo - a0;                                // left tail [a0, mlo), right tail [mhi, a1)
         }
-        const int p = s_seg_lo[l] + (i - s_seg_start[l]);
-        if (!((s_seg_mask[l] >> (p / MJ_WARP_PTS)) & 1u)) continue;
-        const JLine R = s2[l];
+      }
+      int mo = mn, to = tn;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const int u = __shfl_up_sync(0xffffffffu, mo, o), w = __shfl_up_sync(0xffffffffu, to, o);
+        if (lane >= o) {
+          mo += u;
+          to += w;
+        }
+      }
+      const int M = __shfl_sync(0xffffffffu, mo, 31), T = __shfl_sync(0xffffffffu, to, 31);
+      mo -= mn;
+      to -= tn;
+      auto locate = [&](bool mid, int t, int& p, int& sl) {
+        const int off = mid ? mo : to;
+        int o = 0;
+#pragma unroll
+        for (int st = 16; st >= 1; st >>= 1)
+          if (__shfl_sync(0xffffffffu, off, o + st) <= t) o += st;
+        const int k = t - __shfl_sync(0xffffffffu, off, o);
+        const int m_lo = __shfl_sync(0xffffffffu, mlo, o), t_lo = __shfl_sync(0xffffffffu, lo, o);
+        const int t_ln = __shfl_sync(0xffffffffu, ln, o), t_hi = __shfl_sync(0xffffffffu, mhi, o);
+        sl = __shfl_sync(0xffffffffu, slot, o);
+        p = mid ? m_lo + k : (k < t_ln ? t_lo + k : t_hi + (k - t_ln));
+      };
+      auto correction = [&](int p, int sl, float (&d)[3]) {
+        d[0] = d[1] = d[2] = 0.f;
+        const JLine R = s2[sl];
         const float x0 = fmaf((float)(p & ~(P - 1)) - R.g.x, R.g.y, -R.g.z);
         const float x = fmaf((float)(p & (P - 1)), R.g.y, x0);
         const float z2 = fmaf(x, x, R.h.y);
-        if (z2 >= MID_Z2) continue;
+        if (z2 >= MID_Z2) return;
         const U3 good = near3(x, R.h.x, z2);
         const U3 clamped = series5(x, R.h.x, rcp_approx(fmaxf(z2, MID_Z2)));
         float a[3] = {0.f, 0.f, 0.f}, b[3] = {0.f, 0.f, 0.f};
         add3(a, good, x, R);
         add3(b, clamped, x, R);
-        atomicAdd(&s_core[0][p], a[0] - b[0]);
-        atomicAdd(&s_core[1][p], a[1] - b[1]);
-        atomicAdd(&s_core[2][p], a[2] - b[2]);
-      }
-    } else {
-      // bit-reproducible variant: near correction (accurate - clamped) in two phases so that the sums do
-      // not depend on thread scheduling: the items are spread over the CTA into a buffer
-      // (x formed exactly as in the loop above, so the clamped values cancel; 0 where the
-      // line is not level 3 for the owning warp or |z|^2 >= MID_Z2), then every thread
-      // adds the values of its own points in slot order. MJ_NB items per batch.
-      for (int nb0 = 0; nb0 < n_near; nb0 += MJ_NB) {
-        const int nb1 = min(n_near, nb0 + MJ_NB);
-        for (int i = nb0 + tid; i < nb1; i += blockDim.x) {
-          int l = 0, hi = n2;                               // largest l with s_seg_start[l] <= i
-          while (hi - l > 1) {
-            const int mid = (l + hi) >> 1;
-            if (s_seg_start[mid] <= i) l = mid; else hi = mid;
-          }
-          const int p = s_seg_lo[l] + (i - s_seg_start[l]);
-          float d[3] = {0.f, 0.f, 0.f};
-          if ((s_seg_mask[l] >> (p / MJ_WARP_PTS)) & 1u) {
-            const JLine R = s2[l];
-            const float x0 = fmaf((float)(p & ~(P - 1)) - R.g.x, R.g.y, -R.g.z);
-            const float x = fmaf((float)(p & (P - 1)), R.g.y, x0);
-            const float z2 = fmaf(x, x, R.h.y);
-            if (z2 < MID_Z2) {
-              const U3 good = near3(x, R.h.x, z2);
-              const U3 clamped = series5(x, R.h.x, rcp_approx(fmaxf(z2, MID_Z2)));
-              float a[3] = {0.f, 0.f, 0.f}, b[3] = {0.f, 0.f, 0.f};
-              add3(a, good, x, R);
-              add3(b, clamped, x, R);
-              d[0] = a[0] - b[0];
-              d[1] = a[1] - b[1];
-              d[2] = a[2] - b[2];
+        d[0] = a[0] - b[0];
+        d[1] = a[1] - b[1];
+        d[2] = a[2] - b[2];
+      };
+      for (int pass_mid = 1; pass_mid >= 0; --pass_mid) {
+        const bool mid = pass_mid;
+        const int total = mid ? M : T;
+        if constexpr (!DET) {
+          // shared-memory atomics: overlapping near zones of two lines in one 32-item step
+          // meet at a point in an order the hardware picks (~1e-9 relative)
+          for (int it0 = 0; it0 < total; it0 += 32) {
+            const int t = min(it0 + lane, total - 1);
+            int p, sl;
+            locate(mid, t, p, sl);
+            if (it0 + lane < total) {
+              float d[3];
+              correction(p, sl, d);
+              if (d[0] != 0.f || d[1] != 0.f || d[2] != 0.f) {
+                atomicAdd(&s_core[0][p], d[0]);
+                atomicAdd(&s_core[1][p], d[1]);
+                atomicAdd(&s_core[2][p], d[2]);
+              }
             }
           }
-          s_nbuf[0][i - nb0] = d[0];
-          s_nbuf[1][i - nb0] = d[1];
-          s_nbuf[2][i - nb0] = d[2];
-        }
-        __syncthreads();
-        const int q0 = w0 + lane * P;                       // this thread's points [q0, q0 + P)
-        for (int j = 0; j < nnw; ++j) {                     // slots with near points in this warp, in order
-          const int l = s_nl[warp][j];
-          const int st = s_seg_start[l], en = s_seg_start[l + 1];
-          if (en <= nb0 || st >= nb1) continue;
-          const int lo = s_seg_lo[l];
-          const int pa = max(q0, lo + (max(st, nb0) - st)), pb = min(q0 + P, lo + (min(en, nb1) - st));
-          for (int p = pa; p < pb; ++p) {
-            const int k = st + (p - lo) - nb0;
-            s_core[0][p] += s_nbuf[0][k];
-            s_core[1][p] += s_nbuf[1][k];
-            s_core[2][p] += s_nbuf[2][k];
+        } else {
+          // bit-reproducible: values into the warp's buffer, then added line by line in list
+          // order, each line's points spread over the lanes
+          float* buf = s_nbuf_dyn + warp * 3 * MJ_NBW;
+          for (int b0 = 0; b0 < total; b0 += MJ_NBW) {
+            const int b1 = min(total, b0 + MJ_NBW);
+            for (int it0 = b0; it0 < b1; it0 += 32) {
+              const int t = min(it0 + lane, b1 - 1);
+              int p, sl;
+              locate(mid, t, p, sl);
+              if (it0 + lane < b1) {
+                float d[3];
+                correction(p, sl, d);
+                buf[t - b0] = d[0];
+                buf[MJ_NBW + t - b0] = d[1];
+                buf[2 * MJ_NBW + t - b0] = d[2];
+              }
+            }
+            __syncwarp();
+            for (int jl = 0; jl < 32; ++jl) {
+              const int st = __shfl_sync(0xffffffffu, mid ? mo : to, jl);
+              const int n = __shfl_sync(0xffffffffu, mid ? mn : tn, jl);
+              const int m_lo = __shfl_sync(0xffffffffu, mlo, jl), t_lo = __shfl_sync(0xffffffffu, lo, jl);
+              const int t_ln = __shfl_sync(0xffffffffu, ln, jl), t_hi = __shfl_sync(0xffffffffu, mhi, jl);
+              const int ia = max(st, b0), ib = min(st + n, b1);
+              for (int it = ia + lane; it < ib; it += 32) {
+                const int k = it - st;
+                const int p = mid ? m_lo + k : (k < t_ln ? t_lo + k : t_hi + (k - t_ln));
+                s_core[0][p] += buf[it - b0];
+                s_core[1][p] += buf[MJ_NBW + it - b0];
+                s_core[2][p] += buf[2 * MJ_NBW + it - b0];
+              }
+              __syncwarp();
+            }
           }
         }
-        if (nb1 < n_near) __syncthreads();                  // the buffer is refilled
       }
     }
     // No barrier here: the next round writes the staging arrays only after its first
@@ -663,67 +685,68 @@ jac_ml_kernel(const LineF32* __restrict__ prep, const LineJac* __restrict__ jpre
   }
   __syncthreads();
 
-  // level-2 node values of this warp: lanes j and j+16 hold halves of node j
+  // One Chebyshev series per sum and sub-chunk: the level-2 node sums (lanes j and j+16
+  // hold halves of node j), the 8-node interpolant and the level-1 series evaluated at the
+  // 16 nodes, transformed back to coefficients; each point then evaluates one series per sum.
+  const float inv_h1 = use_l1 ? 1.0f / H1 : 0.f, inv_h2 = use_l2 ? 1.0f / H2 : 0.f;
+  if (use_l2) {
+    const int jn = lane & 15;
+    const float tj = c_jnode16[jn];
+    const float t1 = fmaf(H2, tj, C2w - C1) * inv_h1;
 #pragma unroll
-  for (int q = 0; q < 3; ++q) {
-    float f2 = sum2[q] - comp2[q];
-    f2 += __shfl_xor_sync(0xffffffffu, f2, 16);
-    double c = 0.0;
-    for (int j = 0; j < MJ_K; ++j) {
-      const float fj = __shfl_sync(0xffffffffu, f2, j);
-      c += (double)fj * c_jdct16[(lane & 15) * MJ_K + j];
+    for (int q = 0; q < 3; ++q) {
+      float f2 = sum2[q] - comp2[q];
+      f2 += __shfl_xor_sync(0xffffffffu, f2, 16);
+      float g2 = sum2f[q];                                    // lanes j, j+8, j+16, j+24: quarters of node j
+      g2 += __shfl_xor_sync(0xffffffffu, g2, 16);
+      g2 += __shfl_xor_sync(0xffffffffu, g2, 8);
+      double cf = 0.0;
+      for (int j = 0; j < MJ_KF; ++j) cf += (double)__shfl_sync(0xffffffffu, g2, j) * c_jdct8[(lane & 7) * MJ_KF + j];
+      float c8f[MJ_KF];
+#pragma unroll
+      for (int k = 0; k < MJ_KF; ++k) c8f[k] = (float)(__shfl_sync(0xffffffffu, cf, k) * (2.0 / MJ_KF));
+      double fj = (double)f2 + (double)clenshaw_k<MJ_KF>(c8f, tj);
+      if (use_l1)
+        fj += (double)(clenshaw_k(s_c1 + q * MJ_K, t1) + clenshaw_k<MJ_KF>(s_c1 + 3 * MJ_K + q * MJ_KF, t1));
+      double ck = 0.0;
+      for (int j = 0; j < MJ_K; ++j) ck += __shfl_sync(0xffffffffu, fj, j) * c_jdct16[jn * MJ_K + j];
+      if (lane < MJ_K) s_c2[warp][q][lane] = (float)(ck * (2.0 / MJ_K));
     }
-    if (lane < MJ_K) s_c2[warp][q][lane] = use_l2 ? (float)(c * (2.0 / MJ_K)) : 0.f;
-    // 8-node set: lanes j, j+8, j+16, j+24 hold quarters of node j
-    float g2 = sum2f[q];
-    g2 += __shfl_xor_sync(0xffffffffu, g2, 16);
-    g2 += __shfl_xor_sync(0xffffffffu, g2, 8);
-    double cf = 0.0;
-    for (int j = 0; j < MJ_KF; ++j) {
-      const float gj = __shfl_sync(0xffffffffu, g2, j);
-      cf += (double)gj * c_jdct8[(lane & 7) * MJ_KF + j];
-    }
-    if (lane < MJ_KF) s_c2f[warp][q][lane] = use_l2 ? (float)(cf * (2.0 / MJ_KF)) : 0.f;
   }
-  __syncthreads();
+  __syncwarp();
 
   const double T = t_layer[row];
-  const float inv_h1 = use_l1 ? 1.0f / H1 : 0.f, inv_h2 = use_l2 ? 1.0f / H2 : 0.f;
+  const float half_c2_t = (float)(0.5 * C2 / T), inv_t = (float)(1.0 / T);
   const double* g = g_tau ? g_tau + (long long)(row / n_lay) * n_nu : nullptr;
   double pt = 0.0, pv = 0.0;
 #pragma unroll
   for (int m = 0; m < P; ++m) {
     const int pl = w0 + lane * P + m;
     if (pl >= n_c) continue;
-    double v[3];
+    float v[3];
+    const float t1 = ((float)pl - C1) * inv_h1, t2 = ((float)pl - C2w) * inv_h2;
 #pragma unroll
     for (int q = 0; q < 3; ++q) {
       float s = s_core[q][pl];
-      if (use_l1) {
-        const float t1 = ((float)pl - C1) * inv_h1;
-        s += clenshaw_k(s_c1 + q * MJ_K, t1) + clenshaw_k<MJ_KF>(s_c1 + 3 * MJ_K + q * MJ_KF, t1);
-      }
-      if (use_l2) {
-        const float t2 = ((float)pl - C2w) * inv_h2;
-        s += clenshaw_k(s_c2[warp][q], t2) + clenshaw_k<MJ_KF>(s_c2f[warp][q], t2);
-      }
-      v[q] = (double)acc[q][m] + (double)s;
+      if (use_l2) s += clenshaw_k(s_c2[warp][q], t2);
+      else if (use_l1) s += clenshaw_k(s_c1 + q * MJ_K, t1) + clenshaw_k<MJ_KF>(s_c1 + 3 * MJ_K + q * MJ_KF, t1);
+      v[q] = acc[q][m] + s;
     }
     const long long p = c0 + pl;
-    const double nu = grid_nu(nu_min, step, p);
-    const double hv = 0.5 * C2 * nu / T;
-    const double R = nu * tanh(hv);
-    const double ch = cosh(hv);
-    const double R_T = -nu * (hv / T) / (ch * ch);          // dR/dT
-    const double jt = R_T * v[0] + R * v[1], jv = R * v[2];
+    const float nu = (float)grid_nu(nu_min, step, p);
+    const float hv = nu * half_c2_t;                          // c2 nu / 2T
+    const float R = nu * tanhf(hv);                           // R(nu, T)
+    const float ch = coshf(hv);
+    const float R_T = -nu * (hv * inv_t) / (ch * ch);         // dR/dT
+    const float jt = R_T * v[0] + R * v[1], jv = R * v[2];
     if (g) {                      // vector-Jacobian product with d loss / d tau
-      pt += g[p] * jt;
-      pv += g[p] * jv;
+      pt += g[p] * (double)jt;
+      pv += g[p] * (double)jv;
     } else {
       const long long o = (long long)row * n_nu + p;
-      od[o] = (float)(v[0] * R);
-      d_t[o] = (float)jt;
-      d_v[o] = (float)jv;
+      od[o] = v[0] * R;
+      d_t[o] = jt;
+      d_v[o] = jv;
     }
   }
   if (g) {
@@ -803,7 +826,7 @@ extern "C" int lbl_jacobian_ml_f32(const LineF32* prep, const LineJac* jprep, in
   jac_far_kernel<<<grid, MJF_THREADS, 0, st>>>(prep, jprep, n_lines, (const int2*)ranges, (const int2*)near, nu_min,
                                                step, n_nu, tile_samples, (int)chunks, cp, cutoff, l1_work);
   if (flags & LBL_DETERMINISTIC) {
-    constexpr int dyn_bytes = 3 * MJ_NB * (int)sizeof(float);   // near-item buffer
+    constexpr int dyn_bytes = (MJ_THREADS / 32) * 3 * MJ_NBW * (int)sizeof(float);   // near-item buffers
     int dev = 0;
     cudaGetDevice(&dev);
     static int attr_set[64] = {0};
