@@ -342,17 +342,17 @@ def plain_and_accuracy(torch, job, sd, prof, grid, evals, fp32_value):
 def surrogate_timing():
     """Gated surrogate on the 20-layer, 650-1150 cm^-1, 2,000-channel workload at its
     stated size: the 4-member 61 -> 1024x4 -> 2000 ensemble trained for 20,000 steps per
-    member on 100,000 engine spectra, the gate calibrated on 8,192 further profiles,
+    member on 100,000 engine spectra, the gate calibrated on 16,384 further profiles,
     65,536 fresh + 5 % OOD (+25 K) profiles evaluated against the engine, and
     surrogate-only inference timed on the gated workload's 68,813 profiles.
     """
     from pylblrtm_b200 import surrogate_study
     rep = surrogate_study.run(n_train=100_000, n_eval=65_536, ood=0.05, steps=20_000, infer_batch=68813,
-                              n_calibrate=8192, log=lambda *_: None)
+                              n_calibrate=16384, log=lambda *_: None)
     th, err = rep["throughput"], rep["errors"]
     return {"workload": "20-layer profiles, 650-1150 cm^-1 at 0.001, 2000 channels of 0.25 cm^-1, "
                         f"{rep['problem']['lines']} lines x {rep['problem']['strength_scale']:g} strength; "
-                        "100000 training spectra, 20000 steps/member, gate calibrated on 8192 profiles",
+                        "100000 training spectra, 20000 steps/member, gate calibrated on 16384 profiles",
             "blended_ceiling": "1 / (OOD share + flagged share): about 20x with 5 % OOD",
             "gate": rep["gate"], "calibration": rep.get("calibration"),
             "max_channel_err_accepted": err["accepted"],

@@ -566,23 +566,34 @@ def calibrate_gate(gs: "GatedSurrogate", raw, reference: np.ndarray, target: flo
                    quantile: float = 0.999, margin: float = 0.5) -> dict:
     """Fit the gate of ``gs`` on a calibration split: ``raw`` features [n, 61] and the
     engine's channel transmittances ``reference`` [n, n_out] of the same profiles (not
-    used in training). Sets ``gs.ch_scale`` (:func:`channel_weights` of the members'
-    spread against the ensemble mean's error), ``gs.gate`` (:func:`gate_threshold` of
-    the weighted estimate) and ``gs.scale = 1``; returns the fitted values and the
-    split's accepted fraction and accepted-error quantile."""
+    used in training). Tries three per-channel weightings of the members' spread --
+    uniform, :func:`channel_weights` of the spread against the ensemble mean's error,
+    and its square root -- sets for each the largest threshold that meets the target
+    (:func:`gate_threshold`) and keeps the weighting that accepts the most profiles:
+    ``gs.ch_scale`` (None for uniform), ``gs.gate`` and ``gs.scale = 1``. Returns the
+    fitted values and the split's accepted fraction and accepted-error quantile."""
     torch = gs.torch
     pred = gs.predictions(torch.as_tensor(raw, device=gs.members[0].dev))
     mean = pred.mean(0)
     spread = pred.std(0, unbiased=False).cpu().numpy()
     err_c = np.abs(mean.cpu().numpy() - np.asarray(reference, dtype=np.float32))
-    w = channel_weights(spread, err_c)
-    est = (spread * w[None, :]).max(1)
     err = err_c.max(1)
-    t = gate_threshold(est, err, target, quantile, margin)
-    gs.ch_scale = torch.as_tensor(w, device=gs.members[0].dev)
+    fitted = channel_weights(spread, err_c)
+    # candidate weightings; the one whose threshold accepts the most calibration profiles wins
+    cands = {"uniform": np.ones_like(fitted), "fitted": fitted, "sqrt_fitted": np.sqrt(fitted).astype(np.float32)}
+    trials = {}
+    for name, w in cands.items():
+        est = (spread * w[None, :]).max(1)
+        t = gate_threshold(est, err, target, quantile, margin)
+        trials[name] = (float(np.mean(est <= t)), t, est)
+    best = max(trials, key=lambda k: trials[k][0])
+    acc_frac, t, est = trials[best]
+    w = cands[best]
+    gs.ch_scale = None if best == "uniform" else torch.as_tensor(w, device=gs.members[0].dev)
     gs.gate, gs.scale = float(t), 1.0
     acc = est <= t
-    return {"gate": float(t), "profiles": int(est.size), "accepted": float(acc.mean()),
+    return {"gate": float(t), "weights": best, "profiles": int(est.size), "accepted": acc_frac,
+            "accepted_by_weighting": {k: v[0] for k, v in trials.items()},
             "accepted_err_quantile": float(np.quantile(err[acc], quantile)) if acc.any() else None,
             "spread_vs_error_corr": float(np.corrcoef(est, err)[0, 1]) if est.size > 1 else None,
             "target": target, "quantile": quantile, "margin": margin}

@@ -306,7 +306,10 @@ def test_gated_surrogate_against_engine(cuda):
     ref_cal = surrogate.engine_channels(sd, cal, problem, deterministic=True)
     target = float(np.quantile(err_in, 0.7))
     fit = surrogate.calibrate_gate(gate, cal.features(), ref_cal, target=target, quantile=0.95, margin=0.5)
-    assert gate.ch_scale is not None and gate.ch_scale.shape == (problem.n_channels,)
+    assert fit["weights"] in ("uniform", "fitted", "sqrt_fitted")
+    assert fit["accepted"] == max(fit["accepted_by_weighting"].values())
+    assert (gate.ch_scale is None) == (fit["weights"] == "uniform")
+    assert gate.ch_scale is None or gate.ch_scale.shape == (problem.n_channels,)
     assert 0.0 < fit["accepted"] < 1.0 and fit["accepted_err_quantile"] <= target
     mean2, est2, flag2 = gate.ensemble(torch.from_numpy(test_in.features()).cuda())
     acc = ~flag2.cpu().numpy()
