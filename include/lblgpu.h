@@ -171,14 +171,15 @@ int lbl_ml_inner_ranges(const LineIn* lines, const int* n_kept, double nu_min, d
                         int tile_samples, double pad, int n_tiles, int* inner, void* stream);
 
 /* Same contract as lbl_tau_tiles_f32, multi-level float32 summation (the
- * default float32 engine): per CTA chunk (<= 2048 points of one reference
- * tile), lines farther than a chunk half-width contribute through 16 Chebyshev
- * nodes over the chunk (8 beyond six half-widths; a line-per-thread kernel that
- * runs first and hands the chunk's coefficients over through od), the remaining lines farther than a
+ * default float32 engine): per chunk (<= 2048 points of one reference tile),
+ * lines farther than a chunk half-width contribute through 16 Chebyshev nodes over
+ * the chunk (8 beyond six half-widths; a line-per-thread kernel that runs first and
+ * leaves the chunk's coefficients in l1_work), the remaining lines farther than a
  * 256-point sub-chunk half-width through 16 nodes over that sub-chunk, the rest
- * directly. inner (nullable; from lbl_ml_inner_ranges with the ranges' lines
- * and pad) limits the second kernel to the lines that can be inner; NULL scans
- * every candidate of the tile (same results, slower). evals
+ * directly; one warp per sub-chunk does levels 2 and 3. inner (nullable; from
+ * lbl_ml_inner_ranges with the ranges' lines and pad) limits the second kernel to the
+ * lines that can be inner; NULL scans every candidate of the tile (same results,
+ * slower). l1_work: lbl_ml_work_floats floats of device memory (required). evals
  * counts reference-rule evaluations; work (nullable, 3 x u64) receives the
  * evaluations actually performed: [0] Chebyshev-node evaluations, [1] level-3
  * loop evaluations, [2] near-zone points. flags: LBL_DETERMINISTIC adds the
@@ -189,10 +190,15 @@ int lbl_ml_inner_ranges(const LineIn* lines, const int* n_kept, double nu_min, d
  * them: 0 and ceil(n_nu / tile_samples)); od is then [n_rows, n_local] with the
  * tiles' n_local points, grid values staying nu_min + i*step of the full grid (a
  * wavenumber shard gives bit-identical results). Replaces pylblrtm/forward.py:295-315. */
-int lbl_tau_tiles_ml_f32(const LineF32* prep, int n_lines, const int* ranges, const int* inner,
+int lbl_tau_tiles_ml_f32(const LineF32* prep, int n_lines, const int* ranges, const int* inner, float* l1_work,
                          const double* t_layer, int n_rows, double nu_min, double step, long long n_nu,
                          int tile_samples, double cutoff, int n_grp, float* od, int* err, unsigned long long* evals,
                          unsigned long long* work, int tile_first, int tile_count, int flags, void* stream);
+
+/* Floats of the l1_work buffer of lbl_tau_tiles_ml_f32 for tile_count reference tiles
+ * (16 + 8 level-1 coefficients per chunk and row); -1 for bad arguments. No reference
+ * counterpart: a workspace of the summation. */
+long long lbl_ml_work_floats(int n_rows, int tile_samples, int tile_count);
 
 /* Layer Jacobians by the multi-level float32 summation (no reference
  * counterpart; the retrieval adjoint): writes od (as lbl_tau_tiles_ml_f32),

@@ -46,7 +46,9 @@ SIGNATURES = {
     "lbl_tau_tiles_f64": (_I, [_P, _I, _P, _P, _I, _D, _D, _L, _I, _D, _I, _P, _P, _P, _P]),
     "lbl_tau_tiles_f32": (_I, [_P, _I, _P, _P, _I, _D, _D, _L, _I, _D, _I, _P, _P, _P, _P]),
     "lbl_ml_inner_ranges": (_I, [_P, _P, _D, _D, _L, _I, _D, _I, _P, _P]),
-    "lbl_tau_tiles_ml_f32": (_I, [_P, _I, _P, _P, _P, _I, _D, _D, _L, _I, _D, _I, _P, _P, _P, _P, _I, _I, _I, _P]),
+    "lbl_tau_tiles_ml_f32": (_I, [_P, _I, _P, _P, _P, _P, _I, _D, _D, _L, _I, _D, _I, _P, _P, _P, _P, _I, _I, _I,
+                                  _P]),
+    "lbl_ml_work_floats": (_L, [_I, _I, _I]),
     "lbl_line_prep_jac": (_I, [_P, _I, _P, _I, _I, _P, _P, _P, _P, _I, _P, _P, _P]),
     "lbl_jacobian_ml_f32": (_I, [_P, _P, _I, _P, _P, _P, _P, _I, _I, _D, _D, _L, _I, _D, _P, _P, _P, _P, _P, _P,
                                  _P, _I, _P]),

@@ -278,7 +278,10 @@ __global__ void line_prep_f64_kernel(const LineIn* __restrict__ lines, const int
 // the Lorentz width's (296/T)^n_air is a float exponential (the record holds y in
 // float anyway). Same records and error word as before; the float64 engine's prep
 // (line_prep_f64_kernel) keeps the reference's operation order.
-constexpr int PREP_ROWS = 8;
+#ifndef LBL_PREP_ROWS
+#define LBL_PREP_ROWS 8
+#endif
+constexpr int PREP_ROWS = LBL_PREP_ROWS;                       // rows (profile-layers) per thread
 constexpr int PREP_THREADS = 128;
 
 struct RowGroupF32 {
@@ -325,6 +328,7 @@ line_prep_f32_kernel(const LineIn* __restrict__ lines, const int* __restrict__ n
   const double inv_nd = 1.0 / (L.nu0 * DOPPLER);
   const double inv_step = 1.0 / step;
   const float n_air = (float)L.n_air;
+#pragma unroll 2
   for (int k = 0; k < nr; ++k) {
     const int row = r0 + k;
     const RowGroupF32& G = s_rg[k * n_grp + L.gid];
@@ -332,7 +336,10 @@ line_prep_f32_kernel(const LineIn* __restrict__ lines, const int* __restrict__ n
     if (G.active) {
       const double nuc = L.nu0 + L.shift * G.p_air;             // forward.py:263
       double S = sref_stim * G.col_q * exp(c2_elow * G.dinv) * -expm1(G.minus_c2_inv_t * L.nu0);
-      S /= nuc * tanh(nuc * G.half_c2_inv_t);                  // / R(nuc, T), forward.py:277
+      // / R(nuc, T) = nuc tanh(v), v = c2 nuc / 2T (forward.py:277): with e = expm1(-2v),
+      // tanh(v) = -e / (2 + e), so S / R = S (2 + e) / (-nuc e): one expm1, no tanh
+      const double e = expm1(G.minus_c2_inv_t * nuc);
+      S = S * (2.0 + e) / (-nuc * e);
       if (!isfinite(S) || S < 0.0) flag_error(err, row * (n_grp + 1) + L.gid);   // forward.py:280-283
       const double gamma = (double)expf(n_air * G.log_t296) * (L.g_air * G.p_air + L.g_self * G.p_self);
       const double sc = SQRT_LN2 * inv_nd * G.inv_dop;           // sqrt(ln 2) / alpha_D, forward.py:292

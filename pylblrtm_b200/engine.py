@@ -620,8 +620,10 @@ class Job:
                   grid.n_nu, grid.tile_samples, self.cutoff, n_grp, od.data_ptr(), err.data_ptr(),
                   _lib.ptr(evals))
         if precision == "fp32":
-            _lib.call("lbl_tau_tiles_ml_f32", common[0], common[1], common[2], inner.data_ptr(), *common[3:],
-                      0 if evals is None else evals.data_ptr() + 8, t_first, t_count,
+            l1_work = torch.empty((_lib.load().lbl_ml_work_floats(n_rows, grid.tile_samples, t_count),),
+                                  dtype=torch.float32, device=dev)
+            _lib.call("lbl_tau_tiles_ml_f32", common[0], common[1], common[2], inner.data_ptr(), l1_work.data_ptr(),
+                      *common[3:], 0 if evals is None else evals.data_ptr() + 8, t_first, t_count,
                       _lib.LBL_DETERMINISTIC if deterministic else 0, stream)
             self.launches += 2
         else:

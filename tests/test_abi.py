@@ -84,6 +84,11 @@ def test_host_queries_and_argument_errors():
     assert lib.lbl_jacobian_ml_work_floats(2, 10000, 5000) == 2 * 2 * 5 * 72
     assert lib.lbl_jacobian_ml_work_floats(1, 100, 50) == 2 * 72
     assert lib.lbl_jacobian_ml_work_floats(0, 100, 50) == -1
+    # forward level-1 workspace: 24 coefficients per (row, chunk); chunks of <= 2048 points
+    assert lib.lbl_ml_work_floats(60, 2000, 950) == 60 * 950 * 24
+    assert lib.lbl_ml_work_floats(2, 5000, 3) == 2 * 3 * 3 * 24
+    assert lib.lbl_ml_work_floats(1, 300, 1) == 24
+    assert lib.lbl_ml_work_floats(0, 2000, 1) == -1
     for name in ("lbl_ml_inner_ranges", "lbl_jac_near_ranges"):
         with pytest.raises(RuntimeError, match="bad arguments"):
             _lib.call(name, 0, 0, 700.0, 0.0, 10, 2000, 0.0, 1, 0, 0)
