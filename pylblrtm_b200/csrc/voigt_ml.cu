@@ -368,15 +368,16 @@ __device__ __forceinline__ float asym5_poly(float r, float amp_far, const float4
   return fmaf(v, r, amp_far);
 }
 
-// Level 2, one lane per line: lane i of each 32-line step takes line list[i] and adds
-// its values at the K nodes offset (node_k * H2) from the sub-chunk centre C2w
+// Level 2, one lane per line: lane i of each 32-line step takes line list[stride * i]
+// and adds its values at the K nodes offset (node_k * H2) from the sub-chunk centre C2w
 // into f. Nodes k and K-1-k are mirror images, so each pair shares one offset. Three
 // warp-uniform paths: two-term far-wing form when every lane's line has |z|^2 >=
 // FAR_Z2 at every node, five-term form when |z|^2 >= MID_Z2 everywhere, else the full
 // algorithm per node.
 template <int K>
-__device__ __forceinline__ void level2_lines(float (&f)[K], const unsigned char* list, int n,
+__device__ __forceinline__ void level2_lines(float (&f)[K], const unsigned char* list, int stride, int n,
                                              const float4* __restrict__ s_g, const float4* __restrict__ s_h,
+                                             const float4* __restrict__ s_p, const float4* __restrict__ s_q,
                                              float C2w, float H2, int lane) {
   const float* nodes = K == ML_K ? c_node16 : c_node8;
   for (int i0 = 0; i0 < n; i0 += 32) {
@@ -385,7 +386,7 @@ __device__ __forceinline__ void level2_lines(float (&f)[K], const unsigned char*
     int l = 0;
     float4 g = make_float4(C2w, 0.f, -1.0e4f, 0.f), h = make_float4(1.f, 1.f, 0.f, 0.f);   // idle lane: adds 0
     if (act) {
-      l = list[i];
+      l = list[stride * i];
       g = s_g[l];
       h = s_h[l];
     }
@@ -404,8 +405,11 @@ __device__ __forceinline__ void level2_lines(float (&f)[K], const unsigned char*
         far_wing_add(f[K - 1 - k], fmaf(-nodes[k], ha, xc), h.y, ny2, g.w);
       }
     } else if (wpath == 1) {
-      float4 p, q;
-      asym5_line_coeffs(h.y, g.w, p, q);                   // zero for an idle lane (amp_far = 0)
+      float4 p = make_float4(0.f, 0.f, 0.f, 0.f), q = p;
+      if (act) {
+        p = s_p[l];
+        q = s_q[l];
+      }
 #pragma unroll
       for (int k = 0; k < K / 2; ++k) {
         const float xa = fmaf(nodes[k], ha, xc), xb = fmaf(-nodes[k], ha, xc);
@@ -436,69 +440,63 @@ __device__ __forceinline__ float near_correction(int p, const float4& g, const f
   return v - h.w;
 }
 
-constexpr int MLW_BATCH = 128;                  // candidate lines a warp scans per batch
-
-// One CTA = one warp = one 256-point sub-chunk of a chunk (grid.x = chunks x sub-chunks).
-// The warp scans its tile's inner-line range itself, 128 candidates per batch: each lane
-// tests one line (window, level 1 of the chunk, class for this sub-chunk), the passing
-// ones are written to shared memory by scan position and listed per class with ballots;
-// then level 2, level 3 and the near zones of the batch. Nothing waits for another warp,
-// so a sub-chunk with more lines near it delays no other, and a finished warp's slot is
-// refilled by the next CTA. Level-1 coefficients come from tau_far_kernel through l1_work.
 template <bool DET>
-__global__ void __launch_bounds__(32, 32)
+__global__ void __launch_bounds__(ML_THREADS, 4)
 tau_ml_kernel(const LineF32* __restrict__ prep, int n_lines, const int2* __restrict__ ranges,
               const int2* __restrict__ inner_ranges, const float* __restrict__ l1_work,
-              const double* __restrict__ t_layer, double nu_min, double step, long long n_nu, int tile_samples,
-              int chunks_per_tile, int chunk_pts, double cutoff, int n_grp, float* __restrict__ od, int* err,
-              unsigned long long* evals, unsigned long long* work, int tile_first, long long out_first,
-              long long out_stride) {
+              const double* __restrict__ t_layer, double nu_min,
+              double step, long long n_nu, int tile_samples, int chunks_per_tile, double cutoff, int n_grp,
+              float* __restrict__ od, int* err, unsigned long long* evals, unsigned long long* work,
+              int tile_first, long long out_first, long long out_stride) {
   constexpr int P = ML_P;
-  __shared__ float4 s_g[MLW_BATCH];                // jf, a, b, amp_far of the batch's lines (by scan position)
-  __shared__ float4 s_h[MLW_BATCH];                // y, y^2, amp, clamped-loop value inside the near zone
-  __shared__ short4 s_nr[MLW_BATCH];               // near range (lo, n) and its middle (lo, n) in this sub-chunk
-  __shared__ unsigned char s_l2[MLW_BATCH], s_l2f[MLW_BATCH], s_l3[MLW_BATCH];   // positions per class
-  __shared__ float s_core[ML_WARP_PTS];            // near-zone corrections of the sub-chunk's points
-  __shared__ double s_n2[ML_K + ML_KF];            // level-2 node sums
-  __shared__ float s_c1[ML_K + ML_KF];             // level-1 coefficients of the chunk
-  __shared__ float s_nbuf[DET ? ML_NBW : 1];       // near-item values (bit-reproducible mode)
+  constexpr int NW = ML_THREADS / 32;
+  __shared__ float4 s_g[ML_THREADS];                // jf, a, b, amp_far of the round's inner lines
+  __shared__ float4 s_h[ML_THREADS];                // y, y^2, amp, clamped-loop value inside the near zone
+  __shared__ float4 s_p[ML_THREADS];                // amp_far * (B_1 .. B_4)
+  __shared__ float4 s_q[ML_THREADS];                // amp_far * (B_5 .. B_8)
+  __shared__ short4 s_nr[ML_THREADS];               // near range (lo, n) and its middle (lo, n), chunk points
+  __shared__ unsigned short s_cls[ML_THREADS];      // 2-bit class per warp: 0 -, 1 level 3, 2/3 level 2 (16/8)
+  __shared__ unsigned char s_l2[NW][ML_THREADS];    // per-warp level-2 slots (16 nodes from the front, 8 from the back)
+  __shared__ unsigned char s_l3[NW][ML_THREADS];    // per-warp level-3 slots
+  __shared__ int s_cnt[NW];
+  __shared__ float s_core[ML_CHUNK];                // near-zone corrections (each warp owns its points)
+  __shared__ double s_n2[NW][ML_K + ML_KF];         // level-2 node sums per warp
+  __shared__ float s_c1[ML_K + ML_KF];              // level-1 coefficients from tau_far_kernel
+  __shared__ float s_nbuf[DET ? NW : 1][DET ? ML_NBW : 1];   // near-item values (bit-reproducible mode)
 
-  const int lane = threadIdx.x;
-  const int subs = chunk_pts / ML_WARP_PTS;
-  const int chunk_id = blockIdx.x / subs, sub = blockIdx.x % subs;
   const int row = blockIdx.y;
-  const int tile = tile_first + chunk_id / chunks_per_tile, chunk = chunk_id % chunks_per_tile;
+  const int tile = tile_first + (int)(blockIdx.x / chunks_per_tile), chunk = blockIdx.x % chunks_per_tile;
   const long long t0 = (long long)tile * tile_samples;
   const long long t1 = min(t0 + (long long)tile_samples, n_nu);
-  const long long c0 = t0 + (long long)chunk * chunk_pts;
+  const long long c0 = t0 + (long long)chunk * (blockDim.x * P);
   if (c0 >= t1) return;
-  const int n_c = (int)(min(c0 + (long long)chunk_pts, t1) - c0);
-  const int w0 = sub * ML_WARP_PTS;
-  const int n_w = min(ML_WARP_PTS, n_c - w0);
-  if (n_w <= 0) return;
+  const int n_c = (int)(min(c0 + (long long)(blockDim.x * P), t1) - c0);
   const int c0i = (int)c0;
   const double wlo = __dsub_rn(grid_nu(nu_min, step, t0), cutoff);
   const double whi = __dadd_rn(grid_nu(nu_min, step, t1 - 1), cutoff);
   const LineF32* lp = prep + (long long)row * n_lines;
-  // chunk geometry (points relative to c0), as in tau_far_kernel
+
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, n_warps = blockDim.x >> 5;
+  // chunk geometry (points relative to c0)
   const float H1 = 0.5f * (float)(n_c - 1), C1 = H1;
   const bool use_l1 = H1 >= ML_MIN_H1;
+  // With level 1 (done by tau_far_kernel) only lines inside the tile's inner range
+  // can be inner lines of this chunk; without it every line of the window is.
   int2 rng = ranges[tile];
   if (use_l1 && inner_ranges) {
     const int2 q = inner_ranges[tile];
     rng = make_int2(max(rng.x, q.x), min(rng.y, q.y));
   }
-  // this sub-chunk
+  // this warp's sub-chunk
+  const int w0 = warp * ML_WARP_PTS;
+  const int n_w = max(0, min(ML_WARP_PTS, n_c - w0));
   const float H2 = 0.5f * (float)(n_w - 1), C2w = (float)w0 + H2;
   const bool use_l2 = H2 >= ML_MIN_H2;
   const float pf = (float)(w0 + lane * P);                   // this lane's first point
 
-  for (int i = lane; i < ML_WARP_PTS; i += 32) s_core[i] = 0.f;
-  if (lane < ML_K + ML_KF) {
-    s_n2[lane] = 0.0;
-    if (use_l1) s_c1[lane] = l1_work[((long long)row * (gridDim.x / subs) + chunk_id) * (ML_K + ML_KF) + lane];
-  }
-  __syncwarp();
+  for (int i = lane; i < ML_WARP_PTS; i += 32) s_core[w0 + i] = 0.f;
+  if (lane < ML_K + ML_KF) s_n2[warp][lane] = 0.0;
+  if (use_l1 && tid < ML_K + ML_KF) s_c1[tid] = l1_work[((long long)row * gridDim.x + blockIdx.x) * (ML_K + ML_KF) + tid];
 
   // level-3 sums hold only the lines within ~2 sub-chunk widths (tens of terms), so
   // plain float accumulation suffices
@@ -507,92 +505,123 @@ tau_ml_kernel(const LineF32* __restrict__ prep, int n_lines, const int2* __restr
   for (int m = 0; m < P; ++m) acc[m] = 0.f;
   unsigned long long n_pass = 0, n_nodes = 0, n_l3 = 0, n_near_items = 0;
 
-  for (int b0 = rng.x; b0 < rng.y; b0 += MLW_BATCH) {
-    // ---- scan: class of each candidate for this sub-chunk, lists by ballot
-    int n2w = 0, n2fw = 0, n3w = 0;
-#pragma unroll 1
-    for (int s = 0; s < MLW_BATCH; s += 32) {
-      const int li = b0 + s + lane;
-      LineF32 L;
-      bool pass = false;
-      if (li < rng.y) {
-        L = lp[li];
-        pass = (L.nuc >= wlo) && (L.nuc <= whi);
+  // register prefetch of the next round's line records
+  LineF32 nxt;
+  int li = rng.x + tid;
+  if (li < rng.y) nxt = lp[li];
+
+  for (int base = rng.x; base < rng.y; base += blockDim.x) {
+    const LineF32 L = nxt;
+    const bool have = base + tid < rng.y;
+    if (base + blockDim.x + tid < rng.y) nxt = lp[base + blockDim.x + tid];
+    const bool pass = have && (L.nuc >= wlo) && (L.nuc <= whi);
+    const float jf = (float)(L.j0 - c0i);           // |j0 - c0| < 1.5e9 (grid index span check)
+    const float d1 = fabsf(jf - C1) - H1;
+    const bool lev1 = pass && use_l1 && (d1 > H1 + 1.f);   // tau_far_kernel's line
+    const bool inner = pass && !lev1;
+    // class of the line for every warp's sub-chunk
+    unsigned cls = 0u;
+    bool any3 = false;
+    if (inner) {
+      for (int w = 0; w < n_warps; ++w) {
+        const int nw = min(ML_WARP_PTS, n_c - w * ML_WARP_PTS);
+        if (nw <= 0) break;
+        const float h2 = 0.5f * (float)(nw - 1);
+        const float d = fabsf(jf - ((float)(w * ML_WARP_PTS) + h2)) - h2;
+        unsigned c = 1u;
+        if (h2 >= ML_MIN_H2 && d > h2 + 1.f) c = d > ML_FAR1 * h2 ? 3u : 2u;
+        any3 |= c == 1u;
+        cls |= c << (2 * w);
       }
-      const float jf = (float)(L.j0 - c0i);           // |j0 - c0| < 1.5e9 (grid index span check)
-      const bool lev1 = pass && use_l1 && (fabsf(jf - C1) - H1 > H1 + 1.f);   // tau_far_kernel's line
-      const bool inner = pass && !lev1;
-      const float d = fabsf(jf - C2w) - H2;
-      const bool lev2 = inner && use_l2 && d > H2 + 1.f;
-      const bool is2f = lev2 && d > ML_FAR1 * H2, is2 = lev2 && !is2f, is3 = inner && !lev2;
-      if (inner) {
-        const float y2 = L.y * L.y;
-        float4 p, q;
-        asym5_line_coeffs(y2, L.amp_far, p, q);
-        const float rc = clamped_r(0.f, y2);                    // = rcp(MID_Z2) when y2 < MID_Z2
-        s_g[s + lane] = make_float4(jf, L.a, L.b, L.amp_far);
-        s_h[s + lane] = make_float4(L.y, y2, L.amp, rc * asym5_poly(rc, L.amp_far, p, q));
-        // near range (points with possibly |z|^2 < MID_Z2) of a level-3 line, clipped to the
-        // sub-chunk, and its middle (|z|^2 possibly < CORE_Z2), one point of margin each
-        int near_lo = 0, near_n = 0, mid_lo = 0, mid_n = 0;
-        if (is3 && !(y2 >= MID_Z2 && L.y >= 0.f)) {
-          const float hw = sqrtf(fmaxf(MID_Z2 - y2, 0.f)) / L.a + 1.0f;
-          const float qc = jf + L.b / L.a;                     // centre in points
-          const float lo_f = fmaxf(ceilf(qc - hw), (float)w0);
-          const float hi_f = fminf(floorf(qc + hw), (float)(w0 + n_w - 1));
-          if (lo_f <= hi_f) {
-            near_lo = (int)lo_f;
-            near_n = (int)hi_f - near_lo + 1;
-            if (y2 < CORE_Z2 && L.y >= 0.f) {
-              const float hw36 = sqrtf(CORE_Z2 - y2) / L.a + 1.0f;
-              const float a0 = fmaxf(ceilf(qc - hw36), (float)near_lo);
-              const float a1 = fminf(floorf(qc + hw36), (float)(near_lo + near_n - 1));
-              if (a0 <= a1) {
-                mid_lo = (int)a0;
-                mid_n = (int)a1 - mid_lo + 1;
-              }
-            }
+    }
+    // near range (points with possibly |z|^2 < MID_Z2) of an inner line, clipped to the
+    // chunk, and its middle, where |z|^2 may be below CORE_Z2 (one point of margin each;
+    // every item still picks its formula from its own |z|^2)
+    const float y2 = L.y * L.y;
+    int near_lo = 0, near_n = 0, mid_lo = 0, mid_n = 0;
+    if (inner && any3 && !(y2 >= MID_Z2 && L.y >= 0.f)) {
+      const float hw = sqrtf(fmaxf(MID_Z2 - y2, 0.f)) / L.a + 1.0f;
+      const float q = jf + L.b / L.a;                       // centre in points
+      const float lo_f = fmaxf(ceilf(q - hw), 0.f);
+      const float hi_f = fminf(floorf(q + hw), (float)(n_c - 1));
+      if (lo_f <= hi_f) {
+        near_lo = (int)lo_f;
+        near_n = (int)hi_f - near_lo + 1;
+        if (y2 < CORE_Z2 && L.y >= 0.f) {
+          const float hw36 = sqrtf(CORE_Z2 - y2) / L.a + 1.0f;
+          const float a0 = fmaxf(ceilf(q - hw36), (float)near_lo);           // clamped before the
+          const float a1 = fminf(floorf(q + hw36), (float)(near_lo + near_n - 1));   // int conversion
+          if (a0 <= a1) {
+            mid_lo = (int)a0;
+            mid_n = (int)a1 - mid_lo + 1;
           }
         }
-        s_nr[s + lane] = make_short4((short)near_lo, (short)near_n, (short)mid_lo, (short)mid_n);
       }
-      const unsigned q2 = __ballot_sync(FULL_MASK, is2), q2f = __ballot_sync(FULL_MASK, is2f);
-      const unsigned q3 = __ballot_sync(FULL_MASK, is3);
+    }
+    const unsigned b2 = __ballot_sync(FULL_MASK, inner);
+    if (lane == 0) s_cnt[warp] = __popc(b2);
+    __syncthreads();
+    int off2 = 0, n2 = 0;
+    for (int w = 0; w < n_warps; ++w) {
+      const int a2 = s_cnt[w];
+      off2 += (w < warp) ? a2 : 0;
+      n2 += a2;
+    }
+    if (inner) {
+      const int slot = off2 + __popc(b2 & ((1u << lane) - 1u));
+      float4 p, q;
+      asym5_line_coeffs(y2, L.amp_far, p, q);
+      const float rc = clamped_r(0.f, y2);                      // = rcp(MID_Z2) when y2 < MID_Z2
+      s_g[slot] = make_float4(jf, L.a, L.b, L.amp_far);
+      s_h[slot] = make_float4(L.y, y2, L.amp, rc * asym5_poly(rc, L.amp_far, p, q));
+      s_p[slot] = p;
+      s_q[slot] = q;
+      s_nr[slot] = make_short4((short)near_lo, (short)near_n, (short)mid_lo, (short)mid_n);
+      s_cls[slot] = (unsigned short)cls;
+    }
+    __syncthreads();
+    n_pass += (unsigned long long)n2;
+
+    // ---- this warp's lists: level 2 (16 nodes from the front, 8 from the back), level 3
+    int n2w = 0, n2fw = 0, n3w = 0;
+    for (int k = 0; k < n2; k += 32) {
+      const int l = k + lane;
+      const unsigned c = l < n2 ? ((unsigned)s_cls[l] >> (2 * warp)) & 3u : 0u;
+      const unsigned q3 = __ballot_sync(FULL_MASK, c == 1u), q2 = __ballot_sync(FULL_MASK, c == 2u);
+      const unsigned q2f = __ballot_sync(FULL_MASK, c == 3u);
       const unsigned lt = (1u << lane) - 1u;
-      if (is2) s_l2[n2w + __popc(q2 & lt)] = (unsigned char)(s + lane);
-      if (is2f) s_l2f[n2fw + __popc(q2f & lt)] = (unsigned char)(s + lane);
-      if (is3) s_l3[n3w + __popc(q3 & lt)] = (unsigned char)(s + lane);
+      if (c == 2u) s_l2[warp][n2w + __popc(q2 & lt)] = (unsigned char)l;
+      if (c == 3u) s_l2[warp][ML_THREADS - 1 - (n2fw + __popc(q2f & lt))] = (unsigned char)l;
+      if (c == 1u) s_l3[warp][n3w + __popc(q3 & lt)] = (unsigned char)l;
       n2w += __popc(q2);
       n2fw += __popc(q2f);
       n3w += __popc(q3);
-      if (b0 + s + 32 >= rng.y) break;
     }
     __syncwarp();
-    n_pass += (unsigned long long)(n2w + n2fw + n3w);
 
-    // ---- level 2, one lane per line; node sums reduced once per batch
+    // ---- level 2, one lane per line; node sums reduced once per round
     if (n2w > 0) {
       float f[ML_K];
 #pragma unroll
       for (int k = 0; k < ML_K; ++k) f[k] = 0.f;
-      level2_lines<ML_K>(f, s_l2, n2w, s_g, s_h, C2w, H2, lane);
+      level2_lines<ML_K>(f, s_l2[warp], 1, n2w, s_g, s_h, s_p, s_q, C2w, H2, lane);
       const float v = reduce16_transposed(f, lane);
-      if (!(lane & 1)) s_n2[(lane >> 1) & 15] += (double)v;
+      if (!(lane & 1)) s_n2[warp][(lane >> 1) & 15] += (double)v;
     }
     if (n2fw > 0) {
       float f[ML_KF];
 #pragma unroll
       for (int k = 0; k < ML_KF; ++k) f[k] = 0.f;
-      level2_lines<ML_KF>(f, s_l2f, n2fw, s_g, s_h, C2w, H2, lane);
+      level2_lines<ML_KF>(f, &s_l2[warp][ML_THREADS - 1], -1, n2fw, s_g, s_h, s_p, s_q, C2w, H2, lane);
       const float v = reduce8_transposed(f, lane);
-      if (!(lane & 3)) s_n2[ML_K + ((lane >> 2) & 7)] += (double)v;
+      if (!(lane & 3)) s_n2[warp][ML_K + ((lane >> 2) & 7)] += (double)v;
     }
-    n_nodes += (unsigned long long)n2w * ML_K + (unsigned long long)n2fw * ML_KF;
+    if (lane == 0) n_nodes += (unsigned long long)n2w * ML_K + (unsigned long long)n2fw * ML_KF;
 
-    // ---- level 3: every point of the sub-chunk
+    // ---- level 3: every point of the warp
     const float xw_lo = (float)w0, xw_hi = (float)(w0 + n_w - 1);
     for (int i = 0; i < n3w; ++i) {
-      const int l = s_l3[i];
+      const int l = s_l3[warp][i];
       const float4 g = s_g[l], h = s_h[l];
       const float x0 = fmaf(pf - g.x, g.y, -g.z);
       // |x| at the sub-chunk point nearest to the line centre (0 if it lies inside)
@@ -602,8 +631,7 @@ tau_ml_kernel(const LineF32* __restrict__ prep, int n_lines, const int2* __restr
 #pragma unroll
         for (int m = 0; m < P; ++m) far_wing_add(acc[m], fmaf((float)m, g.y, x0), h.y, ny2, g.w);
       } else {                                                    // |z|^2 clamped to >= MID_Z2
-        float4 p, q;
-        asym5_line_coeffs(h.y, g.w, p, q);
+        const float4 p = s_p[l], q = s_q[l];
 #pragma unroll
         for (int m = 0; m < P; ++m) {
           const float r = clamped_r(fmaf((float)m, g.y, x0), h.y);
@@ -611,22 +639,22 @@ tau_ml_kernel(const LineF32* __restrict__ prep, int n_lines, const int2* __restr
         }
       }
     }
-    n_l3 += (unsigned long long)n3w * n_w;
+    if (lane == 0) n_l3 += (unsigned long long)n3w * n_w;
 
-    // ---- near zones of the batch's level-3 lines, 32 lines at a time
+    // ---- near zones of the warp's level-3 lines inside its points, 32 lines at a time
     for (int j0 = 0; j0 < n3w; j0 += 32) {
       const int j = j0 + lane;
       int slot = 0, lo = 0, mlo = 0, mhi = 0, mn = 0, tn = 0, ln = 0;
       if (j < n3w) {
-        slot = s_l3[j];
+        slot = s_l3[warp][j];
         const short4 nr = s_nr[slot];
-        if (nr.y > 0) {
-          const int a0 = nr.x, a1 = nr.x + nr.y;
+        const int a0 = max((int)nr.x, w0), a1 = min((int)nr.x + (int)nr.y, w0 + n_w);
+        if (a1 > a0) {
           lo = a0;
-          mlo = nr.z;
-          mhi = nr.z + nr.w;
-          mn = nr.w;
-          if (mn == 0) mlo = mhi = a1;                  // no middle: all of it is the left tail
+          mlo = max((int)nr.z, a0);
+          mhi = min((int)nr.z + (int)nr.w, a1);
+          mn = max(0, mhi - mlo);
+          if (mn == 0) mlo = mhi = a1;                  // no middle here: all of it is the left tail
           tn = (a1 - a0) - mn;
           ln = mlo - a0;                                // left tail [a0, mlo), right tail [mhi, a1)
         }
@@ -643,70 +671,78 @@ tau_ml_kernel(const LineF32* __restrict__ prep, int n_lines, const int2* __restr
       const int M = __shfl_sync(FULL_MASK, mo, 31), T = __shfl_sync(FULL_MASK, to, 31);
       mo -= mn;
       to -= tn;
-      // point and line of item t of the middles (mid) or tails space: the last lane whose
-      // offset is <= t owns it
-      auto locate = [&](bool mid, int t, int& p, int& sl) {
-        const int off = mid ? mo : to;
+      // item t of a space lies in the run of the last lane whose offset is <= t
+      auto owner = [&](int off, int t) {
         int o = 0;
 #pragma unroll
-        for (int st = 16; st >= 1; st >>= 1)
-          if (__shfl_sync(FULL_MASK, off, o + st) <= t) o += st;
-        const int k = t - __shfl_sync(FULL_MASK, off, o);
+        for (int s = 16; s >= 1; s >>= 1)
+          if (__shfl_sync(FULL_MASK, off, o + s) <= t) o += s;
+        return o;
+      };
+      // point of item t of the middles (mid) or tails space, and the item's line slot
+      auto locate = [&](bool mid, int t, int& p, int& sl) {
+        const int o = owner(mid ? mo : to, t);
+        const int k = t - __shfl_sync(FULL_MASK, mid ? mo : to, o);
         const int m_lo = __shfl_sync(FULL_MASK, mlo, o), t_lo = __shfl_sync(FULL_MASK, lo, o);
         const int t_ln = __shfl_sync(FULL_MASK, ln, o), t_hi = __shfl_sync(FULL_MASK, mhi, o);
         sl = __shfl_sync(FULL_MASK, slot, o);
         p = mid ? m_lo + k : (k < t_ln ? t_lo + k : t_hi + (k - t_ln));
       };
-      for (int pass_mid = 1; pass_mid >= 0; --pass_mid) {
-        const bool mid = pass_mid;
-        const int total = mid ? M : T;
-        if constexpr (!DET) {
-          // values added by shared-memory atomics: two lines' items at one point in one
-          // 32-item step meet in an order the hardware picks (~1e-9 relative)
+      if constexpr (!DET) {
+        // values added by shared-memory atomics: overlapping near zones of two lines in one
+        // 32-item step meet at a point in an order the hardware picks (~1e-9 relative)
+        for (int pass_mid = 1; pass_mid >= 0; --pass_mid) {
+          const bool mid = pass_mid;
+          const int total = mid ? M : T;
           for (int it0 = 0; it0 < total; it0 += 32) {
             const int t = min(it0 + lane, total - 1);
             int p, sl;
             locate(mid, t, p, sl);
             if (it0 + lane < total) {
               const float v = near_correction(p, s_g[sl], s_h[sl]);
-              if (v != 0.f) atomicAdd(&s_core[p - w0], v);
+              if (v != 0.f) atomicAdd(&s_core[p], v);
             }
           }
-        } else {
-          // bit-reproducible: values go through the buffer; then the lines add theirs in
-          // list order, middles before tails, each line's points spread over the lanes
-          for (int bb = 0; bb < total; bb += ML_NBW) {
-            const int be = min(total, bb + ML_NBW);
-            for (int it0 = bb; it0 < be; it0 += 32) {
-              const int t = min(it0 + lane, be - 1);
+        }
+      } else {
+        // bit-reproducible: values go through a buffer; then the lines add theirs in
+        // list order, middles before tails, each line's points spread over the lanes
+        for (int pass_mid = 1; pass_mid >= 0; --pass_mid) {
+          const bool mid = pass_mid;
+          const int total = mid ? M : T;
+          for (int b0 = 0; b0 < total; b0 += ML_NBW) {
+            const int b1 = min(total, b0 + ML_NBW);
+            for (int it0 = b0; it0 < b1; it0 += 32) {
+              const int t = min(it0 + lane, b1 - 1);
               int p, sl;
               locate(mid, t, p, sl);
-              if (it0 + lane < be) s_nbuf[t - bb] = near_correction(p, s_g[sl], s_h[sl]);
+              if (it0 + lane < b1) s_nbuf[warp][t - b0] = near_correction(p, s_g[sl], s_h[sl]);
             }
             __syncwarp();
             for (int jl = 0; jl < 32; ++jl) {
               const int st = __shfl_sync(FULL_MASK, mid ? mo : to, jl), n = __shfl_sync(FULL_MASK, mid ? mn : tn, jl);
               const int m_lo = __shfl_sync(FULL_MASK, mlo, jl), t_lo = __shfl_sync(FULL_MASK, lo, jl);
               const int t_ln = __shfl_sync(FULL_MASK, ln, jl), t_hi = __shfl_sync(FULL_MASK, mhi, jl);
-              const int ia = max(st, bb), ib = min(st + n, be);
+              const int ia = max(st, b0), ib = min(st + n, b1);
               for (int it = ia + lane; it < ib; it += 32) {
                 const int k = it - st;
                 const int p = mid ? m_lo + k : (k < t_ln ? t_lo + k : t_hi + (k - t_ln));
-                s_core[p - w0] += s_nbuf[it - bb];
+                s_core[p] += s_nbuf[warp][it - b0];
               }
               __syncwarp();
             }
           }
         }
       }
-      n_near_items += (unsigned long long)(M + T);
+      if (lane == 0) n_near_items += (unsigned long long)(M + T);
     }
-    __syncwarp();                                    // the next batch rewrites the staging arrays
+    // No barrier here: the next round writes the staging arrays only after its first
+    // barrier, which every warp reaches after finishing this round.
   }
-  __syncwarp();
+  __syncthreads();                                  // s_c1 visible even when no round ran
 
-  // ---- one Chebyshev series for the sub-chunk: level-2 node sums + the 8-node
-  // interpolant + the level-1 series, at the 16 nodes, transformed back to coefficients
+  // ---- one Chebyshev series per sub-chunk: level-2 node sums + the 8-node interpolant
+  // + the level-1 series, at the 16 nodes, transformed back to coefficients
   const float inv_h1 = use_l1 ? 1.0f / H1 : 0.f, inv_h2 = use_l2 ? 1.0f / H2 : 0.f;
   float cw[ML_K];
 #pragma unroll
@@ -714,7 +750,7 @@ tau_ml_kernel(const LineF32* __restrict__ prep, int n_lines, const int2* __restr
   if (use_l2) {
     double c8 = 0.0;
     if (lane < ML_KF) {
-      for (int j = 0; j < ML_KF; ++j) c8 += s_n2[ML_K + j] * c_dct8[lane * ML_KF + j];
+      for (int j = 0; j < ML_KF; ++j) c8 += s_n2[warp][ML_K + j] * c_dct8[lane * ML_KF + j];
       c8 *= 2.0 / ML_KF;
     }
     float c8f[ML_KF];
@@ -722,7 +758,7 @@ tau_ml_kernel(const LineF32* __restrict__ prep, int n_lines, const int2* __restr
     for (int k = 0; k < ML_KF; ++k) c8f[k] = (float)__shfl_sync(FULL_MASK, c8, k);
     const int jn = lane & 15;
     const float tj = c_node16[jn];
-    double fj = s_n2[jn] + (double)clenshaw16<ML_KF>(c8f, tj);
+    double fj = s_n2[warp][jn] + (double)clenshaw16<ML_KF>(c8f, tj);
     if (use_l1) {
       const float t1 = fmaf(H2, tj, C2w - C1) * inv_h1;
       fj += (double)(clenshaw16(s_c1, t1) + clenshaw16<ML_KF>(s_c1 + ML_K, t1));
@@ -734,6 +770,7 @@ tau_ml_kernel(const LineF32* __restrict__ prep, int n_lines, const int2* __restr
 #pragma unroll
     for (int k = 0; k < ML_K; ++k) cw[k] = (float)__shfl_sync(FULL_MASK, ck, k);
   }
+  __syncwarp();
 
   const double T = t_layer[row];
   const float half_c2_t = (float)(0.5 * C2 / T);
@@ -742,9 +779,9 @@ tau_ml_kernel(const LineF32* __restrict__ prep, int n_lines, const int2* __restr
 #pragma unroll
   for (int m = 0; m < P; ++m) {
     const int pl = w0 + lane * P + m;
-    if (pl < w0 + n_w) {
+    if (pl < n_c) {
       const long long p = c0 + pl;
-      float v = s_core[pl - w0];
+      float v = s_core[pl];
       if (use_l2) {
         v += clenshaw16(cw, ((float)pl - C2w) * inv_h2);
       } else if (use_l1) {
@@ -758,14 +795,11 @@ tau_ml_kernel(const LineF32* __restrict__ prep, int n_lines, const int2* __restr
     }
   }
   if (bad) flag_error(err, row * (n_grp + 1) + n_grp);
-  n_pass = __shfl_sync(FULL_MASK, n_pass, 0);
-  if (lane == 0) {
-    if (evals && n_pass) atomicAdd(evals, n_pass * (unsigned long long)n_w);
-    if (work) {   // work[0]: node evaluations, work[1]: level-3 loop evaluations, work[2]: near items
-      if (n_nodes) atomicAdd(&work[0], n_nodes);
-      if (n_l3) atomicAdd(&work[1], n_l3);
-      if (n_near_items) atomicAdd(&work[2], n_near_items);
-    }
+  if (tid == 0 && evals && n_pass) atomicAdd(evals, n_pass * (unsigned long long)n_c);
+  if (work) {   // work[0]: node evaluations, work[1]: level-3 loop evaluations, work[2]: near items
+    if (n_nodes) atomicAdd(&work[0], n_nodes);
+    if (n_l3) atomicAdd(&work[1], n_l3);
+    if (n_near_items) atomicAdd(&work[2], n_near_items);
   }
 }
 
@@ -788,12 +822,11 @@ extern "C" int lbl_ml_inner_ranges(const LineIn* lines, const int* n_kept, doubl
   return lbl_tile_ranges(lines, n_kept, nu_min, step, n_nu, tile_samples, reach, pad, n_tiles, inner, stream);
 }
 
-static int ml_geometry(int tile_samples, int* threads, int* cp, long long* chunks) {
+static void ml_geometry(int tile_samples, int* threads, int* cp, long long* chunks) {
   const int per_tile = tile_samples < ML_CHUNK ? tile_samples : ML_CHUNK;
   *threads = 32 * ((per_tile + ML_WARP_PTS - 1) / ML_WARP_PTS);
   *cp = *threads * ML_P;
   *chunks = (tile_samples + *cp - 1) / *cp;
-  return 0;
 }
 
 extern "C" long long lbl_ml_work_floats(int n_rows, int tile_samples, int tile_count) {
@@ -822,20 +855,19 @@ extern "C" int lbl_tau_tiles_ml_f32(const LineF32* prep, int n_lines, const int*
   long long chunks;
   ml_geometry(tile_samples, &threads, &cp, &chunks);
   const long long n_tiles = tile_count;
-  const int subs = threads / 32;
-  if (n_tiles * chunks * subs > 0x7fffffffLL) return lbl_set_error(LBL_EINVAL, "lbl_tau_tiles_ml_f32: grid too large");
+  if (n_tiles * chunks > 0x7fffffffLL) return lbl_set_error(LBL_EINVAL, "lbl_tau_tiles_ml_f32: grid too large");
+  dim3 grid((unsigned)(n_tiles * chunks), (unsigned)n_rows);
   cudaStream_t st = (cudaStream_t)stream;
-  dim3 grid_far((unsigned)(n_tiles * chunks), (unsigned)n_rows);
-  tau_far_kernel<<<grid_far, MF_THREADS, 0, st>>>(prep, n_lines, (const int2*)ranges, nu_min, step, n_nu, tile_samples,
-                                                   (int)chunks, cp, cutoff, l1_work, evals, work, tile_first);
-  dim3 grid((unsigned)(n_tiles * chunks * subs), (unsigned)n_rows);
+  tau_far_kernel<<<grid, MF_THREADS, 0, st>>>(prep, n_lines, (const int2*)ranges, nu_min, step, n_nu, tile_samples,
+                                               (int)chunks, cp, cutoff, l1_work, evals, work, tile_first);
   if (flags & LBL_DETERMINISTIC)
-    tau_ml_kernel<true><<<grid, 32, 0, st>>>(prep, n_lines, (const int2*)ranges, (const int2*)inner, l1_work, t_layer,
-                                             nu_min, step, n_nu, tile_samples, (int)chunks, cp, cutoff, n_grp, od, err,
-                                             evals, work, tile_first, out_first, out_end - out_first);
+    tau_ml_kernel<true><<<grid, threads, 0, st>>>(prep, n_lines, (const int2*)ranges, (const int2*)inner, l1_work,
+                                                  t_layer, nu_min, step, n_nu, tile_samples, (int)chunks, cutoff, n_grp,
+                                                  od, err, evals, work, tile_first, out_first, out_end - out_first);
   else
-    tau_ml_kernel<false><<<grid, 32, 0, st>>>(prep, n_lines, (const int2*)ranges, (const int2*)inner, l1_work, t_layer,
-                                              nu_min, step, n_nu, tile_samples, (int)chunks, cp, cutoff, n_grp, od, err,
-                                              evals, work, tile_first, out_first, out_end - out_first);
+    tau_ml_kernel<false><<<grid, threads, 0, st>>>(prep, n_lines, (const int2*)ranges, (const int2*)inner, l1_work,
+                                                   t_layer, nu_min, step, n_nu, tile_samples, (int)chunks, cutoff,
+                                                   n_grp, od, err, evals, work, tile_first, out_first,
+                                                   out_end - out_first);
   return lbl_check_launch("lbl_tau_tiles_ml_f32");
 }
