@@ -440,37 +440,48 @@ __device__ __forceinline__ float near_correction(int p, const float4& g, const f
   return v - h.w;
 }
 
+#ifndef LBL_ML_CTA_SUBS
+#define LBL_ML_CTA_SUBS 8
+#endif
+constexpr int ML_CTA_SUBS = LBL_ML_CTA_SUBS;    // 256-point sub-chunks (warps) per CTA of tau_ml_kernel
+
 template <bool DET>
-__global__ void __launch_bounds__(ML_THREADS, 4)
+__global__ void __launch_bounds__(32 * ML_CTA_SUBS, 4 * 8 / ML_CTA_SUBS)
 tau_ml_kernel(const LineF32* __restrict__ prep, int n_lines, const int2* __restrict__ ranges,
               const int2* __restrict__ inner_ranges, const float* __restrict__ l1_work,
               const double* __restrict__ t_layer, double nu_min,
-              double step, long long n_nu, int tile_samples, int chunks_per_tile, double cutoff, int n_grp,
-              float* __restrict__ od, int* err, unsigned long long* evals, unsigned long long* work,
+              double step, long long n_nu, int tile_samples, int chunks_per_tile, int chunk_pts, double cutoff,
+              int n_grp, float* __restrict__ od, int* err, unsigned long long* evals, unsigned long long* work,
               int tile_first, long long out_first, long long out_stride) {
   constexpr int P = ML_P;
-  constexpr int NW = ML_THREADS / 32;
-  __shared__ float4 s_g[ML_THREADS];                // jf, a, b, amp_far of the round's inner lines
-  __shared__ float4 s_h[ML_THREADS];                // y, y^2, amp, clamped-loop value inside the near zone
-  __shared__ float4 s_p[ML_THREADS];                // amp_far * (B_1 .. B_4)
-  __shared__ float4 s_q[ML_THREADS];                // amp_far * (B_5 .. B_8)
-  __shared__ short4 s_nr[ML_THREADS];               // near range (lo, n) and its middle (lo, n), chunk points
-  __shared__ unsigned short s_cls[ML_THREADS];      // 2-bit class per warp: 0 -, 1 level 3, 2/3 level 2 (16/8)
-  __shared__ unsigned char s_l2[NW][ML_THREADS];    // per-warp level-2 slots (16 nodes from the front, 8 from the back)
-  __shared__ unsigned char s_l3[NW][ML_THREADS];    // per-warp level-3 slots
+  constexpr int NW = ML_CTA_SUBS;
+  constexpr int ST = 32 * NW;                       // lines staged per round (one per thread)
+  __shared__ float4 s_g[ST];                // jf, a, b, amp_far of the round's inner lines
+  __shared__ float4 s_h[ST];                // y, y^2, amp, clamped-loop value inside the near zone
+  __shared__ float4 s_p[ST];                // amp_far * (B_1 .. B_4)
+  __shared__ float4 s_q[ST];                // amp_far * (B_5 .. B_8)
+  __shared__ short4 s_nr[ST];               // near range (lo, n) and its middle (lo, n), chunk points
+  __shared__ unsigned short s_cls[ST];      // 2-bit class per warp: 0 -, 1 level 3, 2/3 level 2 (16/8)
+  __shared__ unsigned char s_l2[NW][ST];    // per-warp level-2 slots (16 nodes from the front, 8 from the back)
+  __shared__ unsigned char s_l3[NW][ST];    // per-warp level-3 slots
   __shared__ int s_cnt[NW];
-  __shared__ float s_core[ML_CHUNK];                // near-zone corrections (each warp owns its points)
+  __shared__ float s_core[NW * ML_WARP_PTS];        // near-zone corrections (each warp owns its points)
   __shared__ double s_n2[NW][ML_K + ML_KF];         // level-2 node sums per warp
   __shared__ float s_c1[ML_K + ML_KF];              // level-1 coefficients from tau_far_kernel
   __shared__ float s_nbuf[DET ? NW : 1][DET ? ML_NBW : 1];   // near-item values (bit-reproducible mode)
 
   const int row = blockIdx.y;
-  const int tile = tile_first + (int)(blockIdx.x / chunks_per_tile), chunk = blockIdx.x % chunks_per_tile;
+  // a chunk's sub-chunks are split over `parts` CTAs of up to NW warps each
+  const int parts = (chunk_pts / ML_WARP_PTS + NW - 1) / NW;
+  const int chunk_id = blockIdx.x / parts, part = blockIdx.x % parts;
+  const int tile = tile_first + chunk_id / chunks_per_tile, chunk = chunk_id % chunks_per_tile;
   const long long t0 = (long long)tile * tile_samples;
   const long long t1 = min(t0 + (long long)tile_samples, n_nu);
-  const long long c0 = t0 + (long long)chunk * (blockDim.x * P);
+  const long long c0 = t0 + (long long)chunk * chunk_pts;
   if (c0 >= t1) return;
-  const int n_c = (int)(min(c0 + (long long)(blockDim.x * P), t1) - c0);
+  const int n_c = (int)(min(c0 + (long long)chunk_pts, t1) - c0);
+  const int first_sub = part * NW, p0 = first_sub * ML_WARP_PTS;   // this CTA's first sub-chunk and point
+  if (p0 >= n_c) return;
   const int c0i = (int)c0;
   const double wlo = __dsub_rn(grid_nu(nu_min, step, t0), cutoff);
   const double whi = __dadd_rn(grid_nu(nu_min, step, t1 - 1), cutoff);
@@ -488,15 +499,16 @@ tau_ml_kernel(const LineF32* __restrict__ prep, int n_lines, const int2* __restr
     rng = make_int2(max(rng.x, q.x), min(rng.y, q.y));
   }
   // this warp's sub-chunk
-  const int w0 = warp * ML_WARP_PTS;
+  const int w0 = (first_sub + warp) * ML_WARP_PTS;
   const int n_w = max(0, min(ML_WARP_PTS, n_c - w0));
   const float H2 = 0.5f * (float)(n_w - 1), C2w = (float)w0 + H2;
   const bool use_l2 = H2 >= ML_MIN_H2;
   const float pf = (float)(w0 + lane * P);                   // this lane's first point
 
-  for (int i = lane; i < ML_WARP_PTS; i += 32) s_core[w0 + i] = 0.f;
+  for (int i = lane; i < ML_WARP_PTS; i += 32) s_core[w0 - p0 + i] = 0.f;
   if (lane < ML_K + ML_KF) s_n2[warp][lane] = 0.0;
-  if (use_l1 && tid < ML_K + ML_KF) s_c1[tid] = l1_work[((long long)row * gridDim.x + blockIdx.x) * (ML_K + ML_KF) + tid];
+  if (use_l1 && tid < ML_K + ML_KF)
+    s_c1[tid] = l1_work[((long long)row * (gridDim.x / parts) + chunk_id) * (ML_K + ML_KF) + tid];
 
   // level-3 sums hold only the lines within ~2 sub-chunk widths (tens of terms), so
   // plain float accumulation suffices
@@ -524,10 +536,10 @@ tau_ml_kernel(const LineF32* __restrict__ prep, int n_lines, const int2* __restr
     bool any3 = false;
     if (inner) {
       for (int w = 0; w < n_warps; ++w) {
-        const int nw = min(ML_WARP_PTS, n_c - w * ML_WARP_PTS);
+        const int nw = min(ML_WARP_PTS, n_c - (first_sub + w) * ML_WARP_PTS);
         if (nw <= 0) break;
         const float h2 = 0.5f * (float)(nw - 1);
-        const float d = fabsf(jf - ((float)(w * ML_WARP_PTS) + h2)) - h2;
+        const float d = fabsf(jf - ((float)((first_sub + w) * ML_WARP_PTS) + h2)) - h2;
         unsigned c = 1u;
         if (h2 >= ML_MIN_H2 && d > h2 + 1.f) c = d > ML_FAR1 * h2 ? 3u : 2u;
         any3 |= c == 1u;
@@ -591,7 +603,7 @@ tau_ml_kernel(const LineF32* __restrict__ prep, int n_lines, const int2* __restr
       const unsigned q2f = __ballot_sync(FULL_MASK, c == 3u);
       const unsigned lt = (1u << lane) - 1u;
       if (c == 2u) s_l2[warp][n2w + __popc(q2 & lt)] = (unsigned char)l;
-      if (c == 3u) s_l2[warp][ML_THREADS - 1 - (n2fw + __popc(q2f & lt))] = (unsigned char)l;
+      if (c == 3u) s_l2[warp][ST - 1 - (n2fw + __popc(q2f & lt))] = (unsigned char)l;
       if (c == 1u) s_l3[warp][n3w + __popc(q3 & lt)] = (unsigned char)l;
       n2w += __popc(q2);
       n2fw += __popc(q2f);
@@ -612,7 +624,7 @@ tau_ml_kernel(const LineF32* __restrict__ prep, int n_lines, const int2* __restr
       float f[ML_KF];
 #pragma unroll
       for (int k = 0; k < ML_KF; ++k) f[k] = 0.f;
-      level2_lines<ML_KF>(f, &s_l2[warp][ML_THREADS - 1], -1, n2fw, s_g, s_h, s_p, s_q, C2w, H2, lane);
+      level2_lines<ML_KF>(f, &s_l2[warp][ST - 1], -1, n2fw, s_g, s_h, s_p, s_q, C2w, H2, lane);
       const float v = reduce8_transposed(f, lane);
       if (!(lane & 3)) s_n2[warp][ML_K + ((lane >> 2) & 7)] += (double)v;
     }
@@ -700,7 +712,7 @@ tau_ml_kernel(const LineF32* __restrict__ prep, int n_lines, const int2* __restr
             locate(mid, t, p, sl);
             if (it0 + lane < total) {
               const float v = near_correction(p, s_g[sl], s_h[sl]);
-              if (v != 0.f) atomicAdd(&s_core[p], v);
+              if (v != 0.f) atomicAdd(&s_core[p - p0], v);
             }
           }
         }
@@ -727,7 +739,7 @@ tau_ml_kernel(const LineF32* __restrict__ prep, int n_lines, const int2* __restr
               for (int it = ia + lane; it < ib; it += 32) {
                 const int k = it - st;
                 const int p = mid ? m_lo + k : (k < t_ln ? t_lo + k : t_hi + (k - t_ln));
-                s_core[p] += s_nbuf[warp][it - b0];
+                s_core[p - p0] += s_nbuf[warp][it - b0];
               }
               __syncwarp();
             }
@@ -781,7 +793,7 @@ tau_ml_kernel(const LineF32* __restrict__ prep, int n_lines, const int2* __restr
     const int pl = w0 + lane * P + m;
     if (pl < n_c) {
       const long long p = c0 + pl;
-      float v = s_core[pl];
+      float v = s_core[pl - p0];
       if (use_l2) {
         v += clenshaw16(cw, ((float)pl - C2w) * inv_h2);
       } else if (use_l1) {
@@ -795,7 +807,8 @@ tau_ml_kernel(const LineF32* __restrict__ prep, int n_lines, const int2* __restr
     }
   }
   if (bad) flag_error(err, row * (n_grp + 1) + n_grp);
-  if (tid == 0 && evals && n_pass) atomicAdd(evals, n_pass * (unsigned long long)n_c);
+  if (tid == 0 && evals && n_pass)
+    atomicAdd(evals, n_pass * (unsigned long long)(min(n_c, p0 + n_warps * ML_WARP_PTS) - p0));
   if (work) {   // work[0]: node evaluations, work[1]: level-3 loop evaluations, work[2]: near items
     if (n_nodes) atomicAdd(&work[0], n_nodes);
     if (n_l3) atomicAdd(&work[1], n_l3);
@@ -855,19 +868,23 @@ extern "C" int lbl_tau_tiles_ml_f32(const LineF32* prep, int n_lines, const int*
   long long chunks;
   ml_geometry(tile_samples, &threads, &cp, &chunks);
   const long long n_tiles = tile_count;
-  if (n_tiles * chunks > 0x7fffffffLL) return lbl_set_error(LBL_EINVAL, "lbl_tau_tiles_ml_f32: grid too large");
-  dim3 grid((unsigned)(n_tiles * chunks), (unsigned)n_rows);
+  const int subs = threads / 32, parts = (subs + ML_CTA_SUBS - 1) / ML_CTA_SUBS;
+  const int cta_threads = 32 * (subs < ML_CTA_SUBS ? subs : ML_CTA_SUBS);
+  if (n_tiles * chunks * parts > 0x7fffffffLL) return lbl_set_error(LBL_EINVAL, "lbl_tau_tiles_ml_f32: grid too large");
+  dim3 grid_far((unsigned)(n_tiles * chunks), (unsigned)n_rows);
   cudaStream_t st = (cudaStream_t)stream;
-  tau_far_kernel<<<grid, MF_THREADS, 0, st>>>(prep, n_lines, (const int2*)ranges, nu_min, step, n_nu, tile_samples,
-                                               (int)chunks, cp, cutoff, l1_work, evals, work, tile_first);
+  tau_far_kernel<<<grid_far, MF_THREADS, 0, st>>>(prep, n_lines, (const int2*)ranges, nu_min, step, n_nu, tile_samples,
+                                                   (int)chunks, cp, cutoff, l1_work, evals, work, tile_first);
+  dim3 grid((unsigned)(n_tiles * chunks * parts), (unsigned)n_rows);
   if (flags & LBL_DETERMINISTIC)
-    tau_ml_kernel<true><<<grid, threads, 0, st>>>(prep, n_lines, (const int2*)ranges, (const int2*)inner, l1_work,
-                                                  t_layer, nu_min, step, n_nu, tile_samples, (int)chunks, cutoff, n_grp,
-                                                  od, err, evals, work, tile_first, out_first, out_end - out_first);
+    tau_ml_kernel<true><<<grid, cta_threads, 0, st>>>(prep, n_lines, (const int2*)ranges, (const int2*)inner, l1_work,
+                                                      t_layer, nu_min, step, n_nu, tile_samples, (int)chunks, cp,
+                                                      cutoff, n_grp, od, err, evals, work, tile_first, out_first,
+                                                      out_end - out_first);
   else
-    tau_ml_kernel<false><<<grid, threads, 0, st>>>(prep, n_lines, (const int2*)ranges, (const int2*)inner, l1_work,
-                                                   t_layer, nu_min, step, n_nu, tile_samples, (int)chunks, cutoff,
-                                                   n_grp, od, err, evals, work, tile_first, out_first,
-                                                   out_end - out_first);
+    tau_ml_kernel<false><<<grid, cta_threads, 0, st>>>(prep, n_lines, (const int2*)ranges, (const int2*)inner, l1_work,
+                                                       t_layer, nu_min, step, n_nu, tile_samples, (int)chunks, cp,
+                                                       cutoff, n_grp, od, err, evals, work, tile_first, out_first,
+                                                       out_end - out_first);
   return lbl_check_launch("lbl_tau_tiles_ml_f32");
 }
