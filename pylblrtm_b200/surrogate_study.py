@@ -45,6 +45,25 @@ def _quantiles(a: np.ndarray) -> Dict[str, float]:
             "max": float(a.max()), "frac_le_1e-3": float(np.mean(a <= 1e-3))}
 
 
+def _profile_stats(gs, raw, ref, chunk: int = 8192) -> Dict[str, np.ndarray]:
+    """Per-profile statistics of the ensemble on ``raw`` features against the engine's
+    ``ref`` channels: max and mean channel spread, the spread weighted by the gate's
+    channel weights, and the ensemble mean's max channel error."""
+    import torch
+    out = {k: [] for k in ("spread_max", "spread_mean", "spread_weighted", "err_max")}
+    w = gs.ch_scale
+    for a in range(0, raw.shape[0], chunk):
+        pred = gs.predictions(torch.as_tensor(raw[a:a + chunk], device=gs.members[0].dev))
+        sp = pred.std(0, unbiased=False)
+        err = (pred.mean(0) - torch.as_tensor(ref[a:a + chunk], device=sp.device)).abs().max(1).values
+        out["spread_max"].append(sp.max(1).values.cpu().numpy())
+        out["spread_mean"].append(sp.mean(1).cpu().numpy())
+        out["spread_weighted"].append((sp * w[None, :]).max(1).values.cpu().numpy() if w is not None
+                                      else sp.max(1).values.cpu().numpy())
+        out["err_max"].append(err.cpu().numpy())
+    return {k: np.concatenate(v) for k, v in out.items()}
+
+
 def line_list(n_lines: int, problem: surrogate.SurrogateProblem, strength_scale: float):
     sd = synthetic.three_gas_lines(n_lines)
     sd = synthetic.restrict(sd, problem.nu_min - problem.cutoff, problem.nu_max + problem.cutoff)
@@ -54,7 +73,8 @@ def line_list(n_lines: int, problem: surrogate.SurrogateProblem, strength_scale:
 def run(n_train: int = 100_000, n_eval: int = 65_536, ood: float = 0.05, steps: int = 20_000,
         members: int = 4, batch: int = 4096, hidden: int = 1024, depth: int = 4, lr: float = 1e-3,
         strength_scale: float = 1e-4, n_lines: int = 200_000, gate: float = 1e-3, seed: int = 0,
-        profiles_per_launch: int = 256, infer_batch: int = 0, n_calibrate: int = 8192, log=print) -> dict:
+        profiles_per_launch: int = 256, infer_batch: int = 0, n_calibrate: int = 8192, log=print,
+        dump: str = None) -> dict:
     """The study; ``infer_batch`` > 0 also times surrogate-only inference on that many
     fresh profiles (features only, no engine reference)."""
     import torch
@@ -157,6 +177,13 @@ def run(n_train: int = 100_000, n_eval: int = 65_536, ood: float = 0.05, steps: 
             "profiles": infer_batch, "seconds": t_big, "spectra_per_s": infer_batch / t_big,
             "tflops": rep["throughput"]["gemm_flops_per_spectrum"] * infer_batch / t_big / 1e12,
             "launches": gs.launches}
+    if dump:            # per-profile data for studying error estimates (features, spreads, errors)
+        d = {"train_mean": x.mean(0), "train_cov": np.cov(x, rowvar=False), "eval_features": ev.features(),
+             "eval_ood": is_ood, **{f"eval_{k}": v for k, v in _profile_stats(gs, ev.features(), ref).items()}}
+        if n_calibrate:
+            d.update({"cal_features": cal.features(),
+                      **{f"cal_{k}": v for k, v in _profile_stats(gs, cal.features(), y_cal).items()}})
+        np.savez_compressed(dump, **d)
     rep["gate"] = {"gate": gs.gate, "target": gate, "calibrated": bool(n_calibrate),
                    "flagged_in": float(flag_h[~is_ood].mean()),
                    "flagged_ood": float(flag_h[is_ood].mean()) if n_ood else None,
@@ -217,6 +244,7 @@ def main(argv=None) -> None:
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--infer-batch", type=int, default=0)
     ap.add_argument("--calibrate", type=int, default=8192, help="calibration profiles for the gate (0: none)")
+    ap.add_argument("--dump", default=None, help="write per-profile features, spreads and errors (.npz)")
     ap.add_argument("--profiles-per-launch", type=int, default=256)
     ap.add_argument("--infer-only", action="store_true",
                     help="only time surrogate inference on --infer-batch profiles (random weights)")
@@ -228,7 +256,7 @@ def main(argv=None) -> None:
         return
     rep = run(a.train, a.eval, a.ood, a.steps, a.members, a.batch, a.hidden, a.depth, a.lr, a.strength_scale,
               a.lines, a.gate, a.seed, profiles_per_launch=a.profiles_per_launch, infer_batch=a.infer_batch,
-              n_calibrate=a.calibrate)
+              n_calibrate=a.calibrate, dump=a.dump)
     text = json.dumps(rep, indent=1)
     print(text)
     if a.out:
