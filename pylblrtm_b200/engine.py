@@ -670,7 +670,6 @@ def _jacobian_impl(job: Job, gas: str, g_tau=None, deterministic: bool = False):
     prep = torch.empty((n_rows * n_kept * _lib.SIZEOF_LINE_F32 // 8,), dtype=torch.float64, device=dev)
     _lib.call("lbl_line_prep_f32", lines.data_ptr(), job._kept.data_ptr(), n_kept, lg.data_ptr(), n_rows, n_grp,
               grid.nu_min, grid.step, prep.data_ptr(), err.data_ptr(), stream)
-    job._raise_on_error(err, n_grp)
     mask = 0
     for i, grp in enumerate(job.groups):
         if grp.gas == gas:
@@ -702,11 +701,13 @@ def _jacobian_impl(job: Job, gas: str, g_tau=None, deterministic: bool = False):
         vv = torch.zeros_like(vt)
         _lib.call("lbl_jacobian_ml_f32", *common, 0, 0, 0, g.data_ptr(), vt.data_ptr(), vv.data_ptr(), flags,
                   stream)
+        job._raise_on_error(err, n_grp)          # the line-strength check, read once at the end
         return vt, vv
     od = torch.empty((n_prof, n_lay, n_nu), dtype=torch.float32, device=dev)
     d_t = torch.empty_like(od)
     d_v = torch.empty_like(od)
     _lib.call("lbl_jacobian_ml_f32", *common, od.data_ptr(), d_t.data_ptr(), d_v.data_ptr(), 0, 0, 0, flags, stream)
+    job._raise_on_error(err, n_grp)              # the line-strength check, read once at the end
     return od, d_t, d_v
 
 

@@ -74,20 +74,25 @@ def run(n_train: int = 100_000, n_eval: int = 65_536, ood: float = 0.05, steps: 
         members: int = 4, batch: int = 4096, hidden: int = 1024, depth: int = 4, lr: float = 1e-3,
         strength_scale: float = 1e-4, n_lines: int = 200_000, gate: float = 1e-3, seed: int = 0,
         profiles_per_launch: int = 256, infer_batch: int = 0, n_calibrate: int = 8192, log=print,
-        dump: str = None) -> dict:
+        dump: str = None, train_widen: float = 1.0) -> dict:
     """The study; ``infer_batch`` > 0 also times surrogate-only inference on that many
     fresh profiles (features only, no engine reference)."""
     import torch
     problem = surrogate.SurrogateProblem()
     sd = line_list(n_lines, problem, strength_scale)
-    rep = {"problem": {"nu": [problem.nu_min, problem.nu_max], "step": problem.step,
+    rep = {"train_widen": train_widen,
+           "problem": {"nu": [problem.nu_min, problem.nu_max], "step": problem.step,
                        "channel_width": problem.channel_width, "n_channels": problem.n_channels,
                        "lines": int(sd.lines["nu0"].size), "strength_scale": strength_scale, "layers": 20},
            "network": {"inputs": 61, "hidden": [hidden] * depth, "outputs": problem.n_channels,
                        "members": members, "batch": batch, "steps": steps, "lr": lr}}
 
     # 1. training data from the engine
-    train = surrogate.sample_profiles(n_train, seed=seed)
+    # training profiles: the workload's distribution, or with its temperature and H2O
+    # spreads widened by train_widen so that its tails are better covered (evaluation and
+    # calibration always use the workload's own distribution)
+    train = surrogate.sample_profiles(n_train, seed=seed, t_sigma=5.0 * train_widen,
+                                      h2o_log_sigma=0.3 * train_widen)
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     y = surrogate.engine_channels(sd, train, problem, profiles_per_launch=profiles_per_launch)
@@ -245,6 +250,8 @@ def main(argv=None) -> None:
     ap.add_argument("--infer-batch", type=int, default=0)
     ap.add_argument("--calibrate", type=int, default=8192, help="calibration profiles for the gate (0: none)")
     ap.add_argument("--dump", default=None, help="write per-profile features, spreads and errors (.npz)")
+    ap.add_argument("--train-widen", type=float, default=1.0,
+                    help="factor on the training profiles' temperature and H2O spreads")
     ap.add_argument("--profiles-per-launch", type=int, default=256)
     ap.add_argument("--infer-only", action="store_true",
                     help="only time surrogate inference on --infer-batch profiles (random weights)")
@@ -256,7 +263,7 @@ def main(argv=None) -> None:
         return
     rep = run(a.train, a.eval, a.ood, a.steps, a.members, a.batch, a.hidden, a.depth, a.lr, a.strength_scale,
               a.lines, a.gate, a.seed, profiles_per_launch=a.profiles_per_launch, infer_batch=a.infer_batch,
-              n_calibrate=a.calibrate, dump=a.dump)
+              n_calibrate=a.calibrate, dump=a.dump, train_widen=a.train_widen)
     text = json.dumps(rep, indent=1)
     print(text)
     if a.out:
