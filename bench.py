@@ -352,7 +352,8 @@ def surrogate_timing():
     th, err = rep["throughput"], rep["errors"]
     return {"workload": "20-layer profiles, 650-1150 cm^-1 at 0.001, 2000 channels of 0.25 cm^-1, "
                         f"{rep['problem']['lines']} lines x {rep['problem']['strength_scale']:g} strength; "
-                        "100000 training spectra, 20000 steps/member, gate calibrated on 16384 profiles",
+                        "100000 training spectra (temperature and H2O spreads x 1.3), 20000 steps/member, gate calibrated "
+                        "on 16384 profiles of the workload's distribution",
             "blended_ceiling": "1 / (OOD share + flagged share): about 20x with 5 % OOD",
             "gate": rep["gate"], "calibration": rep.get("calibration"),
             "max_channel_err_accepted": err["accepted"],

@@ -273,10 +273,10 @@ __global__ void line_prep_f64_kernel(const LineIn* __restrict__ lines, const int
 // a line's record is read once and its layer-independent factors are formed once: the
 // stimulated-emission denominator -expm1(-c2 nu0 / 296), c2 E'' and 1/(nu0 * 3.581e-7).
 // Per (row, group) the CTA stages 1/T, 1/T - 1/296, 0.5 c2 / T, ln(296/T) and 1/sqrt(T/M)
-// in shared memory. The Boltzmann and stimulated-emission factors stay float64
-// (exp, expm1), the strength is divided by R(nuc, T) in float64 as in forward.py:277;
-// the Lorentz width's (296/T)^n_air is a float exponential (the record holds y in
-// float anyway). Same records and error word as before; the float64 engine's prep
+// in shared memory. The Boltzmann factor stays float64 (exp), the strength is divided by
+// R(nuc, T) in float64 as in forward.py:277 (through expm1); the stimulated-emission
+// factor (expm1f) and the Lorentz width's (296/T)^n_air (expf) are float, at the float
+// record's precision. Same records and error word as before; the float64 engine's prep
 // (line_prep_f64_kernel) keeps the reference's operation order.
 #ifndef LBL_PREP_ROWS
 #define LBL_PREP_ROWS 8
@@ -335,7 +335,11 @@ line_prep_f32_kernel(const LineIn* __restrict__ lines, const int* __restrict__ n
     LineF32 o = r;
     if (G.active) {
       const double nuc = L.nu0 + L.shift * G.p_air;             // forward.py:263
-      double S = sref_stim * G.col_q * exp(c2_elow * G.dinv) * -expm1(G.minus_c2_inv_t * L.nu0);
+      // Boltzmann factor in float64 (its argument reaches +-20 for large E''); the
+      // stimulated-emission factor 1 - exp(-c2 nu0 / T) by expm1f keeps float32 relative
+      // accuracy (no cancellation at any argument), which the float32 record needs
+      const double stim = -(double)expm1f((float)(G.minus_c2_inv_t * L.nu0));
+      double S = sref_stim * G.col_q * exp(c2_elow * G.dinv) * stim;
       // / R(nuc, T) = nuc tanh(v), v = c2 nuc / 2T (forward.py:277): with e = expm1(-2v),
       // tanh(v) = -e / (2 + e), so S / R = S (2 + e) / (-nuc e): one expm1, no tanh
       const double e = expm1(G.minus_c2_inv_t * nuc);

@@ -218,61 +218,43 @@ __device__ __forceinline__ void add3_line(float& s0, float& s1, float& s2, const
   s2 = fmaf(J.jv_u, v.u, fmaf(J.jv_y, v.uy, fmaf(-J.jv_x, v.ux, s2)));
 }
 
-// Node sums of one level-1 line at four mirrored node pairs: nodes KOFF + j (into f[q][j])
-// and K - 1 - (KOFF + j) (into f[q][4 + j]), j = 0..3, at +-xs[KOFF + j] from the centre.
-template <int K, int KOFF>
-__device__ __forceinline__ void jfar_line4(float (&f)[3][8], const float (&xs)[K / 2], const LineF32& L,
-                                           const LineJac& J, float xc, float y2, bool fast) {
+// Node sums of one level-1 line: nodes k and K-1-k sit at +xs[k] and -xs[k] from the chunk centre.
+template <int K>
+__device__ __forceinline__ void jfar_line(float (&f)[3][K], const float (&xs)[K / 2], const LineF32& L,
+                                          const LineJac& J, float xc, float y2, bool fast) {
   if (fast) {
 #pragma unroll
-    for (int j = 0; j < 4; ++j) {
-      const float xp = fmaf(xs[KOFF + j], L.a, xc), xm = fmaf(-xs[KOFF + j], L.a, xc);
-      add3_line(f[0][j], f[1][j], f[2][j], series2(xp, L.y, rcp_approx(fmaf(xp, xp, y2))), xp, L, J);
-      add3_line(f[0][4 + j], f[1][4 + j], f[2][4 + j], series2(xm, L.y, rcp_approx(fmaf(xm, xm, y2))), xm, L, J);
+    for (int k = 0; k < K / 2; ++k) {
+      const float xp = fmaf(xs[k], L.a, xc), xm = fmaf(-xs[k], L.a, xc);
+      add3_line(f[0][k], f[1][k], f[2][k], series2(xp, L.y, rcp_approx(fmaf(xp, xp, y2))), xp, L, J);
+      add3_line(f[0][K - 1 - k], f[1][K - 1 - k], f[2][K - 1 - k],
+                series2(xm, L.y, rcp_approx(fmaf(xm, xm, y2))), xm, L, J);
     }
   } else {
 #pragma unroll
-    for (int j = 0; j < 4; ++j) {
-      const float xp = fmaf(xs[KOFF + j], L.a, xc), xm = fmaf(-xs[KOFF + j], L.a, xc);
-      add3_line(f[0][j], f[1][j], f[2][j], jac_node_general(xp, L.y, y2), xp, L, J);
-      add3_line(f[0][4 + j], f[1][4 + j], f[2][4 + j], jac_node_general(xm, L.y, y2), xm, L, J);
+    for (int k = 0; k < K / 2; ++k) {
+      const float xp = fmaf(xs[k], L.a, xc), xm = fmaf(-xs[k], L.a, xc);
+      add3_line(f[0][k], f[1][k], f[2][k], jac_node_general(xp, L.y, y2), xp, L, J);
+      add3_line(f[0][K - 1 - k], f[1][K - 1 - k], f[2][K - 1 - k], jac_node_general(xm, L.y, y2), xm, L, J);
     }
   }
 }
 
-// Adds the lanes' float sums f[q][j] into the warp's float64 row at the nodes of
-// jfar_line4 (lane 0 owns the row) and clears them; every lane of the warp calls it.
-template <int K, int KOFF>
-__device__ __forceinline__ void jfar_flush(float (&f)[3][8], double* row, int lane) {
-#pragma unroll
-  for (int q = 0; q < 3; ++q)
-#pragma unroll
-    for (int j = 0; j < 8; ++j) {
-      double v = (double)f[q][j];
-#pragma unroll
-      for (int o = 16; o >= 1; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-      const int node = j < 4 ? KOFF + j : K - 1 - (KOFF + j - 4);
-      if (lane == 0) row[q * K + node] += v;
-      f[q][j] = 0.f;
-    }
-}
-
 // One pass of jac_far_kernel over the tile's candidate lines for the lines of one node
-// class (K = MJ_K: level-1 lines within six half-widths; K = MJ_KF: beyond) and four of
-// its mirrored node pairs (KOFF .. KOFF + 3); the warp's float64 sums go to
-// row[q * K + node]. The 16-node class takes two passes, so at most 3 x 8 accumulators
-// are live.
-template <int K, int KOFF>
+// class (K = MJ_K: level-1 lines within six half-widths; K = MJ_KF: beyond); the warp's
+// float64 sums of that class go to row[q * K + k]. Two passes keep 3 K accumulators live
+// instead of 3 (MJ_K + MJ_KF).
+template <int K>
 __device__ __forceinline__ void jfar_pass(JFarLine (*s_line)[MJF_THREADS], const LineF32* lp, const LineJac* jp,
                                           int2 rng, double wlo, double whi, long long c0, float H1,
                                           const float (&xs)[K / 2], double* row) {
   const int tid = threadIdx.x, lane = tid & 31;
   const float C1 = H1;
-  float f[3][8];
+  float f[3][K];
 #pragma unroll
   for (int q = 0; q < 3; ++q)
 #pragma unroll
-    for (int k = 0; k < 8; ++k) f[q][k] = 0.f;
+    for (int k = 0; k < K; ++k) f[q][k] = 0.f;
   // records of round r (line rng.x + r * MJF_THREADS + tid) go to stage r % 2, one round
   // ahead; each thread copies into and reads only its own slots
   const int n_rounds = rng.y > rng.x ? (rng.y - rng.x + MJF_THREADS - 1) / MJF_THREADS : 0;
@@ -307,21 +289,20 @@ __device__ __forceinline__ void jfar_pass(JFarLine (*s_line)[MJF_THREADS], const
       const float xc = fmaf(C1 - jf, R.l.a, -R.l.b);
       const float y2 = R.l.y * R.l.y;
       const float xm = fmaf(-H1 * c_jnode16[0], R.l.a, fabsf(xc));   // nearest node, as in tau_far_kernel
-      jfar_line4<K, KOFF>(f, xs, R.l, R.j, xc, y2, fmaf(xm, xm, y2) >= FAR_Z2);
+      jfar_line<K>(f, xs, R.l, R.j, xc, y2, fmaf(xm, xm, y2) >= FAR_Z2);
     }
     if (++rounds == MJF_FLUSH) {
       rounds = 0;
-      jfar_flush<K, KOFF>(f, row, lane);
+#pragma unroll
+      for (int q = 0; q < 3; ++q) flush_nodes(f[q], row + q * K, lane);
     }
   }
   cp_async_wait<0>();                                      // only empty groups remain
-  jfar_flush<K, KOFF>(f, row, lane);
+#pragma unroll
+  for (int q = 0; q < 3; ++q) flush_nodes(f[q], row + q * K, lane);
 }
 
-#ifndef LBL_JF_MIN_BLOCKS
-#define LBL_JF_MIN_BLOCKS 3
-#endif
-__global__ void __launch_bounds__(MJF_THREADS, LBL_JF_MIN_BLOCKS)
+__global__ void __launch_bounds__(MJF_THREADS, 2)
 jac_far_kernel(const LineF32* __restrict__ prep, const LineJac* __restrict__ jprep, int n_lines,
                const int2* __restrict__ ranges, const int2* __restrict__ near_ranges, double nu_min, double step,
                long long n_nu, int tile_samples, int chunks_per_tile, int chunk_pts, double cutoff,
@@ -359,9 +340,8 @@ jac_far_kernel(const LineF32* __restrict__ prep, const LineJac* __restrict__ jpr
     const int2 q = near_ranges[tile];
     rng16 = make_int2(max(rng.x, q.x), min(rng.y, q.y));
   }
-  jfar_pass<MJ_K, 0>(s_line, lp, jp, rng16, wlo, whi, c0, H1, xa, s_part[warp]);
-  jfar_pass<MJ_K, 4>(s_line, lp, jp, rng16, wlo, whi, c0, H1, xa, s_part[warp]);
-  jfar_pass<MJ_KF, 0>(s_line, lp, jp, rng, wlo, whi, c0, H1, xb, s_part[warp] + 3 * MJ_K);
+  jfar_pass<MJ_K>(s_line, lp, jp, rng16, wlo, whi, c0, H1, xa, s_part[warp]);
+  jfar_pass<MJ_KF>(s_line, lp, jp, rng, wlo, whi, c0, H1, xb, s_part[warp] + 3 * MJ_K);
   __syncthreads();
   if (tid < MJ_NCOEF) {                                    // column tid: only this thread touches it
     double v = 0.0;

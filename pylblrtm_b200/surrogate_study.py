@@ -74,7 +74,7 @@ def run(n_train: int = 100_000, n_eval: int = 65_536, ood: float = 0.05, steps: 
         members: int = 4, batch: int = 4096, hidden: int = 1024, depth: int = 4, lr: float = 1e-3,
         strength_scale: float = 1e-4, n_lines: int = 200_000, gate: float = 1e-3, seed: int = 0,
         profiles_per_launch: int = 256, infer_batch: int = 0, n_calibrate: int = 8192, log=print,
-        dump: str = None, train_widen: float = 1.0) -> dict:
+        dump: str = None, train_widen: float = 1.3) -> dict:
     """The study; ``infer_batch`` > 0 also times surrogate-only inference on that many
     fresh profiles (features only, no engine reference)."""
     import torch
@@ -88,9 +88,11 @@ def run(n_train: int = 100_000, n_eval: int = 65_536, ood: float = 0.05, steps: 
                        "members": members, "batch": batch, "steps": steps, "lr": lr}}
 
     # 1. training data from the engine
-    # training profiles: the workload's distribution, or with its temperature and H2O
-    # spreads widened by train_widen so that its tails are better covered (evaluation and
-    # calibration always use the workload's own distribution)
+    # training profiles: the workload's distribution with its temperature and H2O spreads
+    # widened by train_widen (1.3 by default), so that the tails of the workload's own
+    # distribution, where the network errs most, are better covered; calibration and
+    # evaluation always draw from the workload's own distribution (at train_widen = 1.3
+    # the in-distribution profiles above 1e-3 went from 1.2 % to 0.36 % of the 65,536)
     train = surrogate.sample_profiles(n_train, seed=seed, t_sigma=5.0 * train_widen,
                                       h2o_log_sigma=0.3 * train_widen)
     torch.cuda.synchronize()
@@ -250,7 +252,7 @@ def main(argv=None) -> None:
     ap.add_argument("--infer-batch", type=int, default=0)
     ap.add_argument("--calibrate", type=int, default=8192, help="calibration profiles for the gate (0: none)")
     ap.add_argument("--dump", default=None, help="write per-profile features, spreads and errors (.npz)")
-    ap.add_argument("--train-widen", type=float, default=1.0,
+    ap.add_argument("--train-widen", type=float, default=1.3,
                     help="factor on the training profiles' temperature and H2O spreads")
     ap.add_argument("--profiles-per-launch", type=int, default=256)
     ap.add_argument("--infer-only", action="store_true",
