@@ -518,14 +518,20 @@ tau_ml_kernel(const LineF32* __restrict__ prep, int n_lines, const int2* __restr
   unsigned long long n_pass = 0, n_nodes = 0, n_l3 = 0, n_near_items = 0;
 
   // register prefetch of the next round's line records
+  // Round r stages lines rng.x + k * n_rounds + r (k = thread): every round is an even
+  // sample of the whole inner range, so each warp's sub-chunk gets about the same share of
+  // level-3 and near-zone work in every round. With consecutive lines per round, the lines
+  // of a round lie next to one or two sub-chunks and the other warps wait at the barrier.
+  const int n_in = max(0, rng.y - rng.x);
+  const int n_rounds = (n_in + (int)blockDim.x - 1) / (int)blockDim.x;
   LineF32 nxt;
-  int li = rng.x + tid;
-  if (li < rng.y) nxt = lp[li];
+  if (tid * n_rounds < n_in) nxt = lp[rng.x + tid * n_rounds];
 
-  for (int base = rng.x; base < rng.y; base += blockDim.x) {
+  for (int r = 0; r < n_rounds; ++r) {
     const LineF32 L = nxt;
-    const bool have = base + tid < rng.y;
-    if (base + blockDim.x + tid < rng.y) nxt = lp[base + blockDim.x + tid];
+    const int k = tid * n_rounds + r;
+    const bool have = k < n_in;
+    if (r + 1 < n_rounds && k + 1 < n_in) nxt = lp[rng.x + k + 1];
     const bool pass = have && (L.nuc >= wlo) && (L.nuc <= whi);
     const float jf = (float)(L.j0 - c0i);           // |j0 - c0| < 1.5e9 (grid index span check)
     const float d1 = fabsf(jf - C1) - H1;

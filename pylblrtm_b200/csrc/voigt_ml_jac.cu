@@ -423,9 +423,14 @@ jac_ml_kernel(const LineF32* __restrict__ prep, const LineJac* __restrict__ jpre
     for (int m = 0; m < P; ++m) acc[q][m] = 0.f;
   float sum2[3] = {0.f, 0.f, 0.f}, comp2[3] = {0.f, 0.f, 0.f}, sum2f[3] = {0.f, 0.f, 0.f};
 
-  for (int base = rng.x; base < rng.y; base += blockDim.x) {
-    const int li = base + tid;
-    const bool have = li < rng.y;
+  // round r takes lines rng.x + k * n_rounds + r (k = thread): an even sample of the inner
+  // range per round, so the warps' level-3 and near-zone shares stay balanced round by round
+  const int n_in = max(0, rng.y - rng.x);
+  const int n_rounds = (n_in + (int)blockDim.x - 1) / (int)blockDim.x;
+  for (int r = 0; r < n_rounds; ++r) {
+    const int k = tid * n_rounds + r;
+    const int li = rng.x + k;
+    const bool have = k < n_in;
     LineF32 L;
     LineJac J;
     if (have) {

@@ -155,7 +155,10 @@ def test_jacobian_ranges_select_every_line(cuda, tile, monkeypatch):
     """Jacobians computed with the inner-line and near level-1 ranges equal, to float
     rounding, those of a scan of every candidate line (inner = near = NULL), with pressure
     shifts 40x the synthetic ones; tiles of one chunk, several chunks and below level 1's
-    minimum size. A line lost by a range would change whole line profiles."""
+    minimum size. A line lost by a range would change whole line profiles. The two scans
+    group lines into different rounds, so the float sums run in another order, and the
+    d/dT sums add terms of both signs: the bound is a few float roundings of the layer's
+    largest value."""
     from pylblrtm_b200 import _lib
     sd = synthetic.restrict(synthetic.three_gas_lines(20000, 1490.0, 1520.0, seed=4), 1490.0, 1520.0)
     lines = {k: v.copy() for k, v in sd.lines.items()}
@@ -178,4 +181,4 @@ def test_jacobian_ranges_select_every_line(cuda, tile, monkeypatch):
     every = job.jacobian("H2O", deterministic=True)
     for a, b in zip(with_ranges, every):
         scale = b.abs().amax(dim=-1, keepdim=True).clamp_min(1e-30)
-        assert ((a - b).abs() / scale).max().item() <= 1e-6
+        assert ((a - b).abs() / scale).max().item() <= 5e-6
