@@ -636,12 +636,14 @@ tau_ml_kernel(const LineF32* __restrict__ prep, int n_lines, const int2* __restr
     }
     if (lane == 0) n_nodes += (unsigned long long)n2w * ML_K + (unsigned long long)n2fw * ML_KF;
 
-    // ---- level 3: every point of the warp
+    // ---- level 3: every point of the warp. A sub-chunk of at most P points (the one-point
+    // tile at the end of a grid) lets each lane take its own lines at lane 0's points
+    // instead; the lanes' sums are added after the last round.
     const float xw_lo = (float)w0, xw_hi = (float)(w0 + n_w - 1);
-    for (int i = 0; i < n3w; ++i) {
+    auto level3_line = [&](int i, float pl0) {
       const int l = s_l3[warp][i];
       const float4 g = s_g[l], h = s_h[l];
-      const float x0 = fmaf(pf - g.x, g.y, -g.z);
+      const float x0 = fmaf(pl0 - g.x, g.y, -g.z);
       // |x| at the sub-chunk point nearest to the line centre (0 if it lies inside)
       const float xmin = fmaxf(fmaxf(fmaf(xw_lo - g.x, g.y, -g.z), -fmaf(xw_hi - g.x, g.y, -g.z)), 0.f);
       if (h.x >= 0.f && fmaf(xmin, xmin, h.y) >= FAR_Z2) {        // far from every point: two terms
@@ -656,6 +658,11 @@ tau_ml_kernel(const LineF32* __restrict__ prep, int n_lines, const int2* __restr
           acc[m] = fmaf(r, asym5_poly(r, g.w, p, q), acc[m]);
         }
       }
+    };
+    {
+      const bool few = n_w <= P;                      // warp-uniform
+      const float pl0 = few ? (float)w0 : pf;
+      for (int i = few ? lane : 0; i < n3w; i += few ? 32 : 1) level3_line(i, pl0);
     }
     if (lane == 0) n_l3 += (unsigned long long)n3w * n_w;
 
@@ -758,6 +765,12 @@ tau_ml_kernel(const LineF32* __restrict__ prep, int n_lines, const int2* __restr
     // barrier, which every warp reaches after finishing this round.
   }
   __syncthreads();                                  // s_c1 visible even when no round ran
+  if (n_w <= P) {                                   // lanes' level-3 sums at lane 0's points
+#pragma unroll
+    for (int m = 0; m < P; ++m)
+#pragma unroll
+      for (int o = 16; o >= 1; o >>= 1) acc[m] += __shfl_xor_sync(FULL_MASK, acc[m], o);
+  }
 
   // ---- one Chebyshev series per sub-chunk: level-2 node sums + the 8-node interpolant
   // + the level-1 series, at the 16 nodes, transformed back to coefficients

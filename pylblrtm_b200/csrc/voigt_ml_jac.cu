@@ -535,10 +535,12 @@ jac_ml_kernel(const LineF32* __restrict__ prep, const LineJac* __restrict__ jpre
     }
     // level 3, clamped loop (branch-free per line). A line whose nearest point of the
     // warp's sub-chunk has |z|^2 >= TIER3_Z2 (no near point here) takes the three-term
-    // series at every point; the choice is uniform across the warp.
-    for (int i = 0; i < n3w; ++i) {
+    // series at every point; the choice is uniform across the warp. A sub-chunk of at most
+    // P points (the one-point tile at the end of a grid) lets each lane take its own lines
+    // at lane 0's points; the lanes' sums are added after the last round.
+    auto level3_line = [&](int i, float pl0) {
       const JLine R = s2[s_l3[warp][i]];
-      const float x0 = fmaf(pf - R.g.x, R.g.y, -R.g.z);
+      const float x0 = fmaf(pl0 - R.g.x, R.g.y, -R.g.z);
       const float xl = fmaf((float)w0 - R.g.x, R.g.y, -R.g.z);       // x at the sub-chunk's first point
       const float xh = fmaf((float)(n_w - 1), R.g.y, xl);            // and at its last (x grows with p)
       const float xmin = xl > 0.f ? xl : (xh < 0.f ? -xh : 0.f);
@@ -565,6 +567,11 @@ jac_ml_kernel(const LineF32* __restrict__ prep, const LineJac* __restrict__ jpre
           acc[2][m] = a3[2];
         }
       }
+    };
+    {
+      const bool few = n_w <= P;                      // warp-uniform
+      const float pl0 = few ? (float)w0 : pf;
+      for (int i = few ? lane : 0; i < n3w; i += few ? 32 : 1) level3_line(i, pl0);
     }
     // level 3, near correction (accurate - clamped) of the warp's level-3 lines at the near
     // points inside its sub-chunk, 32 lines at a time: the middles (float64 core), then the
@@ -689,6 +696,14 @@ jac_ml_kernel(const LineF32* __restrict__ prep, const LineJac* __restrict__ jpre
     // barrier, which every warp reaches after finishing this round.
   }
   __syncthreads();
+  if (n_w <= P) {                                   // lanes' level-3 sums at lane 0's points
+#pragma unroll
+    for (int q = 0; q < 3; ++q)
+#pragma unroll
+      for (int m = 0; m < P; ++m)
+#pragma unroll
+        for (int o = 16; o >= 1; o >>= 1) acc[q][m] += __shfl_xor_sync(0xffffffffu, acc[q][m], o);
+  }
 
   // One Chebyshev series per sum and sub-chunk: the level-2 node sums (lanes j and j+16
   // hold halves of node j), the 8-node interpolant and the level-1 series evaluated at the
