@@ -428,15 +428,20 @@ __device__ __forceinline__ void level2_lines(float (&f)[K], const unsigned char*
 }
 
 // (accurate value - clamped loop value) of a level-3 line at chunk point p; x is
-// formed exactly as in the level-3 loop, so the clamped constant h.w cancels.
+// formed exactly as in the level-3 loop, so the clamped constant h.w cancels. Items of
+// a zone's middle (MID) take the float64 core at every point, the margin points with
+// |z|^2 >= CORE_Z2 included (28-term set: Re w within 8e-8 there too), so no lane of a
+// warp branches off to the continued fraction; tail items take the continued fraction.
+template <bool MID>
 __device__ __forceinline__ float near_correction(int p, const float4& g, const float4& h) {
   const float x0 = fmaf((float)(p & ~(ML_P - 1)) - g.x, g.y, -g.z);
   const float x = fmaf((float)(p & (ML_P - 1)), g.y, x0);
   const float z2 = fmaf(x, x, h.y);
   if (z2 >= MID_Z2) return 0.f;
   float v;
-  if (z2 >= CORE_Z2 && h.x >= 0.f) v = h.z * re_w_cf32(x, h.x, z2);
-  else v = (float)((double)h.z * weideman_re_f32((double)x, (double)h.x));
+  if (MID) v = (float)((double)h.z * weideman_re_f32((double)x, (double)h.x));
+  else if (z2 >= CORE_Z2 && h.x >= 0.f) v = h.z * re_w_cf32(x, h.x, z2);
+  else v = (float)((double)h.z * weideman_re_f32_compact((double)x, (double)h.x));
   return v - h.w;
 }
 
@@ -724,7 +729,8 @@ tau_ml_kernel(const LineF32* __restrict__ prep, int n_lines, const int2* __restr
             int p, sl;
             locate(mid, t, p, sl);
             if (it0 + lane < total) {
-              const float v = near_correction(p, s_g[sl], s_h[sl]);
+              const float v = mid ? near_correction<true>(p, s_g[sl], s_h[sl])
+                                  : near_correction<false>(p, s_g[sl], s_h[sl]);
               if (v != 0.f) atomicAdd(&s_core[p - p0], v);
             }
           }
@@ -741,7 +747,9 @@ tau_ml_kernel(const LineF32* __restrict__ prep, int n_lines, const int2* __restr
               const int t = min(it0 + lane, b1 - 1);
               int p, sl;
               locate(mid, t, p, sl);
-              if (it0 + lane < b1) s_nbuf[warp][t - b0] = near_correction(p, s_g[sl], s_h[sl]);
+              if (it0 + lane < b1)
+                s_nbuf[warp][t - b0] = mid ? near_correction<true>(p, s_g[sl], s_h[sl])
+                                           : near_correction<false>(p, s_g[sl], s_h[sl]);
             }
             __syncwarp();
             for (int jl = 0; jl < 32; ++jl) {

@@ -121,10 +121,12 @@ __device__ __forceinline__ U3 series3(float x, float y, float r) {
   return o;
 }
 
-// Accurate u, u_x, u_y for |z|^2 < MID_Z2 (continued fraction or Weideman).
-__device__ __noinline__ U3 near3(float x, float y, float z2) {
+// Accurate u, u_x, u_y for |z|^2 < MID_Z2 (continued fraction or Weideman). With core
+// set, Weideman's float64 form at any |z|^2 (the 28-term set stays within 8e-8 of Re w up
+// to MID_Z2), so the items of a zone's middle never branch off to the continued fraction.
+__device__ __noinline__ U3 near3(float x, float y, float z2, bool core = false) {
   double wr, wi;
-  if (z2 >= CORE_Z2 && y >= 0.f) {
+  if (!core && z2 >= CORE_Z2 && y >= 0.f) {
     const int depth = cf_depth<float>(z2);
     float rr = 0.f, ri = 0.f;
     for (int n = depth - 1; n >= 0; --n) {
@@ -618,14 +620,14 @@ jac_ml_kernel(const LineF32* __restrict__ prep, const LineJac* __restrict__ jpre
         sl = __shfl_sync(0xffffffffu, slot, o);
         p = mid ? m_lo + k : (k < t_ln ? t_lo + k : t_hi + (k - t_ln));
       };
-      auto correction = [&](int p, int sl, float (&d)[3]) {
+      auto correction = [&](bool mid, int p, int sl, float (&d)[3]) {
         d[0] = d[1] = d[2] = 0.f;
         const JLine R = s2[sl];
         const float x0 = fmaf((float)(p & ~(P - 1)) - R.g.x, R.g.y, -R.g.z);
         const float x = fmaf((float)(p & (P - 1)), R.g.y, x0);
         const float z2 = fmaf(x, x, R.h.y);
         if (z2 >= MID_Z2) return;
-        const U3 good = near3(x, R.h.x, z2);
+        const U3 good = near3(x, R.h.x, z2, mid);
         const U3 clamped = series5(x, R.h.x, rcp_approx(fmaxf(z2, MID_Z2)));
         float a[3] = {0.f, 0.f, 0.f}, b[3] = {0.f, 0.f, 0.f};
         add3(a, good, x, R);
@@ -646,7 +648,7 @@ jac_ml_kernel(const LineF32* __restrict__ prep, const LineJac* __restrict__ jpre
             locate(mid, t, p, sl);
             if (it0 + lane < total) {
               float d[3];
-              correction(p, sl, d);
+              correction(mid, p, sl, d);
               if (d[0] != 0.f || d[1] != 0.f || d[2] != 0.f) {
                 atomicAdd(&s_core[0][p], d[0]);
                 atomicAdd(&s_core[1][p], d[1]);
@@ -666,7 +668,7 @@ jac_ml_kernel(const LineF32* __restrict__ prep, const LineJac* __restrict__ jpre
               locate(mid, t, p, sl);
               if (it0 + lane < b1) {
                 float d[3];
-                correction(p, sl, d);
+                correction(mid, p, sl, d);
                 buf[t - b0] = d[0];
                 buf[MJ_NBW + t - b0] = d[1];
                 buf[2 * MJ_NBW + t - b0] = d[2];
