@@ -325,7 +325,7 @@ tau_far_kernel(const LineF32* __restrict__ prep, int n_lines, const int2* __rest
 //    and add (accurate value - clamped loop value) into the warp's part of s_core.
 // The epilogue folds the level-1 series and both level-2 interpolants into one
 // 16-term Chebyshev series per sub-chunk, so each point evaluates one series.
-constexpr int ML_NBW = 256;                    // near items buffered per warp (bit-reproducible mode)
+constexpr int ML_NBW = 128;                    // near items buffered per warp (bit-reproducible mode)
 constexpr unsigned FULL_MASK = 0xffffffffu;
 
 // Sum over the 32 lanes of f[16], transposed: afterwards lanes 2j and 2j+1 hold the
@@ -445,6 +445,17 @@ __device__ __forceinline__ float near_correction(int p, const float4& g, const f
   return v - h.w;
 }
 
+// One round's staged inner lines (slot = thread), in dynamic shared memory, two rounds deep.
+struct MlStage {
+  float4 g[ML_THREADS];            // jf, a, b, amp_far
+  float4 h[ML_THREADS];            // y, y^2, amp, clamped-loop value inside the near zone
+  float4 p[ML_THREADS];            // amp_far * (B_1 .. B_4)
+  float4 q[ML_THREADS];            // amp_far * (B_5 .. B_8)
+  short4 nr[ML_THREADS];           // near range (lo, n) and its middle (lo, n), chunk points
+  unsigned short cls[ML_THREADS];  // 2-bit class per warp: 0 -, 1 level 3, 2/3 level 2 (16/8)
+};
+constexpr size_t ML_STAGE_BYTES = 2 * sizeof(MlStage);
+
 #ifndef LBL_ML_CTA_SUBS
 #define LBL_ML_CTA_SUBS 8
 #endif
@@ -461,15 +472,10 @@ tau_ml_kernel(const LineF32* __restrict__ prep, int n_lines, const int2* __restr
   constexpr int P = ML_P;
   constexpr int NW = ML_CTA_SUBS;
   constexpr int ST = 32 * NW;                       // lines staged per round (one per thread)
-  __shared__ float4 s_g[ST];                // jf, a, b, amp_far of the round's inner lines
-  __shared__ float4 s_h[ST];                // y, y^2, amp, clamped-loop value inside the near zone
-  __shared__ float4 s_p[ST];                // amp_far * (B_1 .. B_4)
-  __shared__ float4 s_q[ST];                // amp_far * (B_5 .. B_8)
-  __shared__ short4 s_nr[ST];               // near range (lo, n) and its middle (lo, n), chunk points
-  __shared__ unsigned short s_cls[ST];      // 2-bit class per warp: 0 -, 1 level 3, 2/3 level 2 (16/8)
+  extern __shared__ __align__(16) unsigned char s_dyn[];
+  MlStage* const s_stage = reinterpret_cast<MlStage*>(s_dyn);   // two rounds' staging buffers
   __shared__ unsigned char s_l2[NW][ST];    // per-warp level-2 slots (16 nodes from the front, 8 from the back)
   __shared__ unsigned char s_l3[NW][ST];    // per-warp level-3 slots
-  __shared__ int s_cnt[NW];
   __shared__ float s_core[NW * ML_WARP_PTS];        // near-zone corrections (each warp owns its points)
   __shared__ double s_n2[NW][ML_K + ML_KF];         // level-2 node sums per warp
   __shared__ float s_c1[ML_K + ML_KF];              // level-1 coefficients from tau_far_kernel
@@ -533,6 +539,13 @@ tau_ml_kernel(const LineF32* __restrict__ prep, int n_lines, const int2* __restr
   if (tid * n_rounds < n_in) nxt = lp[rng.x + tid * n_rounds];
 
   for (int r = 0; r < n_rounds; ++r) {
+    MlStage& S = s_stage[r & 1];
+    float4* const s_g = S.g;
+    float4* const s_h = S.h;
+    float4* const s_p = S.p;
+    float4* const s_q = S.q;
+    short4* const s_nr = S.nr;
+    unsigned short* const s_cls = S.cls;
     const LineF32 L = nxt;
     const int k = tid * n_rounds + r;
     const bool have = k < n_in;
@@ -581,17 +594,12 @@ tau_ml_kernel(const LineF32* __restrict__ prep, int n_lines, const int2* __restr
         }
       }
     }
-    const unsigned b2 = __ballot_sync(FULL_MASK, inner);
-    if (lane == 0) s_cnt[warp] = __popc(b2);
-    __syncthreads();
-    int off2 = 0, n2 = 0;
-    for (int w = 0; w < n_warps; ++w) {
-      const int a2 = s_cnt[w];
-      off2 += (w < warp) ? a2 : 0;
-      n2 += a2;
-    }
+    // every thread owns slot tid of this round's buffer; a line that is not inner leaves
+    // class 0 there, so no warp lists it
+    const int n2 = blockDim.x;
+    s_cls[tid] = inner ? (unsigned short)cls : (unsigned short)0;
     if (inner) {
-      const int slot = off2 + __popc(b2 & ((1u << lane) - 1u));
+      const int slot = tid;
       float4 p, q;
       asym5_line_coeffs(y2, L.amp_far, p, q);
       const float rc = clamped_r(0.f, y2);                      // = rcp(MID_Z2) when y2 < MID_Z2
@@ -600,10 +608,11 @@ tau_ml_kernel(const LineF32* __restrict__ prep, int n_lines, const int2* __restr
       s_p[slot] = p;
       s_q[slot] = q;
       s_nr[slot] = make_short4((short)near_lo, (short)near_n, (short)mid_lo, (short)mid_n);
-      s_cls[slot] = (unsigned short)cls;
     }
+    // One barrier per round: this round's buffer was last read two rounds ago, and every
+    // warp finished that round before it reached the previous round's barrier.
     __syncthreads();
-    n_pass += (unsigned long long)n2;
+    n_pass += (unsigned long long)__popc(__ballot_sync(FULL_MASK, inner));   // this warp's lines
 
     // ---- this warp's lists: level 2 (16 nodes from the front, 8 from the back), level 3
     int n2w = 0, n2fw = 0, n3w = 0;
@@ -752,7 +761,9 @@ tau_ml_kernel(const LineF32* __restrict__ prep, int n_lines, const int2* __restr
                                            : near_correction<false>(p, s_g[sl], s_h[sl]);
             }
             __syncwarp();
-            for (int jl = 0; jl < 32; ++jl) {
+            // only the lines whose items fall in [b0, b1): from the owner of b0 to that of b1 - 1
+            const int j_hi = owner(mid ? mo : to, b1 - 1);
+            for (int jl = owner(mid ? mo : to, b0); jl <= j_hi; ++jl) {
               const int st = __shfl_sync(FULL_MASK, mid ? mo : to, jl), n = __shfl_sync(FULL_MASK, mid ? mn : tn, jl);
               const int m_lo = __shfl_sync(FULL_MASK, mlo, jl), t_lo = __shfl_sync(FULL_MASK, lo, jl);
               const int t_ln = __shfl_sync(FULL_MASK, ln, jl), t_hi = __shfl_sync(FULL_MASK, mhi, jl);
@@ -769,8 +780,7 @@ tau_ml_kernel(const LineF32* __restrict__ prep, int n_lines, const int2* __restr
       }
       if (lane == 0) n_near_items += (unsigned long long)(M + T);
     }
-    // No barrier here: the next round writes the staging arrays only after its first
-    // barrier, which every warp reaches after finishing this round.
+    // No barrier here: the next round stages into the other buffer.
   }
   __syncthreads();                                  // s_c1 visible even when no round ran
   if (n_w <= P) {                                   // lanes' level-3 sums at lane 0's points
@@ -834,7 +844,7 @@ tau_ml_kernel(const LineF32* __restrict__ prep, int n_lines, const int2* __restr
     }
   }
   if (bad) flag_error(err, row * (n_grp + 1) + n_grp);
-  if (tid == 0 && evals && n_pass)
+  if (lane == 0 && evals && n_pass)
     atomicAdd(evals, n_pass * (unsigned long long)(min(n_c, p0 + n_warps * ML_WARP_PTS) - p0));
   if (work) {   // work[0]: node evaluations, work[1]: level-3 loop evaluations, work[2]: near items
     if (n_nodes) atomicAdd(&work[0], n_nodes);
@@ -903,13 +913,24 @@ extern "C" int lbl_tau_tiles_ml_f32(const LineF32* prep, int n_lines, const int*
   tau_far_kernel<<<grid_far, MF_THREADS, 0, st>>>(prep, n_lines, (const int2*)ranges, nu_min, step, n_nu, tile_samples,
                                                    (int)chunks, cp, cutoff, l1_work, evals, work, tile_first);
   dim3 grid((unsigned)(n_tiles * chunks * parts), (unsigned)n_rows);
+  // the staging buffers take the kernel past 48 KB of shared memory: opt in (per call, so
+  // that every device and context the caller uses gets it; a host-side attribute write)
+  {
+    const void* fn = (flags & LBL_DETERMINISTIC) ? (const void*)tau_ml_kernel<true> : (const void*)tau_ml_kernel<false>;
+    cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ML_STAGE_BYTES);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(fn, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+    if (e != cudaSuccess) {
+      cudaGetLastError();
+      return lbl_set_error(LBL_ECUDA, "lbl_tau_tiles_ml_f32 (shared-memory attributes): %s", cudaGetErrorString(e));
+    }
+  }
   if (flags & LBL_DETERMINISTIC)
-    tau_ml_kernel<true><<<grid, cta_threads, 0, st>>>(prep, n_lines, (const int2*)ranges, (const int2*)inner, l1_work,
+    tau_ml_kernel<true><<<grid, cta_threads, ML_STAGE_BYTES, st>>>(prep, n_lines, (const int2*)ranges, (const int2*)inner, l1_work,
                                                       t_layer, nu_min, step, n_nu, tile_samples, (int)chunks, cp,
                                                       cutoff, n_grp, od, err, evals, work, tile_first, out_first,
                                                       out_end - out_first);
   else
-    tau_ml_kernel<false><<<grid, cta_threads, 0, st>>>(prep, n_lines, (const int2*)ranges, (const int2*)inner, l1_work,
+    tau_ml_kernel<false><<<grid, cta_threads, ML_STAGE_BYTES, st>>>(prep, n_lines, (const int2*)ranges, (const int2*)inner, l1_work,
                                                        t_layer, nu_min, step, n_nu, tile_samples, (int)chunks, cp,
                                                        cutoff, n_grp, od, err, evals, work, tile_first, out_first,
                                                        out_end - out_first);
