@@ -608,12 +608,17 @@ jac_ml_kernel(const LineF32* __restrict__ prep, const LineJac* __restrict__ jpre
       const int M = __shfl_sync(0xffffffffu, mo, 31), T = __shfl_sync(0xffffffffu, to, 31);
       mo -= mn;
       to -= tn;
-      auto locate = [&](bool mid, int t, int& p, int& sl) {
-        const int off = mid ? mo : to;
+      // item t of a space lies in the run of the last lane whose offset is <= t
+      auto owner = [&](int off, int t) {
         int o = 0;
 #pragma unroll
         for (int st = 16; st >= 1; st >>= 1)
           if (__shfl_sync(0xffffffffu, off, o + st) <= t) o += st;
+        return o;
+      };
+      auto locate = [&](bool mid, int t, int& p, int& sl) {
+        const int off = mid ? mo : to;
+        const int o = owner(off, t);
         const int k = t - __shfl_sync(0xffffffffu, off, o);
         const int m_lo = __shfl_sync(0xffffffffu, mlo, o), t_lo = __shfl_sync(0xffffffffu, lo, o);
         const int t_ln = __shfl_sync(0xffffffffu, ln, o), t_hi = __shfl_sync(0xffffffffu, mhi, o);
@@ -675,7 +680,9 @@ jac_ml_kernel(const LineF32* __restrict__ prep, const LineJac* __restrict__ jpre
               }
             }
             __syncwarp();
-            for (int jl = 0; jl < 32; ++jl) {
+            // only the lines whose items fall in [b0, b1): from the owner of b0 to that of b1 - 1
+            const int j_hi = owner(mid ? mo : to, b1 - 1);
+            for (int jl = owner(mid ? mo : to, b0); jl <= j_hi; ++jl) {
               const int st = __shfl_sync(0xffffffffu, mid ? mo : to, jl);
               const int n = __shfl_sync(0xffffffffu, mid ? mn : tn, jl);
               const int m_lo = __shfl_sync(0xffffffffu, mlo, jl), t_lo = __shfl_sync(0xffffffffu, lo, jl);
