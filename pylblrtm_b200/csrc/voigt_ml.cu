@@ -10,11 +10,12 @@
 //           analytic on a Bernstein ellipse with rho >= 2 + sqrt(3) around the
 //           chunk, so it is evaluated at K1 = 16 Chebyshev nodes and interpolated
 //           (interpolation error ~rho^-16 ~ 1e-9 of the level-1 sum; lines more than
-//           six half-widths out use 8 nodes). A separate kernel (tau_far_kernel)
-//           computes this level and hands its coefficients over through od;
+//           four half-widths out use 8 nodes, rho >= 7.87: ~7e-8 of their sum). A
+//           separate kernel (tau_far_kernel) computes this level and hands its
+//           coefficients over through a workspace;
 //  level 2  the other lines farther than one sub-chunk half-width from a warp's
 //           256-point sub-chunk: 16 Chebyshev nodes per sub-chunk, same geometry
-//           (8 beyond six sub-chunk half-widths);
+//           (8 beyond four sub-chunk half-widths);
 //  level 3  the remaining lines: direct evaluation at every point. The warp's
 //           loop is branch-free: it evaluates the five-term asymptotic form with
 //           |z|^2 clamped to >= MID_Z2 = 64, so every point inside a line's near
@@ -42,7 +43,7 @@ constexpr int ML_THREADS = 256;                // max threads per CTA = lines st
 constexpr int ML_CHUNK = ML_THREADS * ML_P;    // max points per CTA
 constexpr int ML_K = 16;                       // Chebyshev nodes per level
 constexpr int ML_KF = 8;                       // nodes for level-1 lines far from the chunk
-constexpr float ML_FAR1 = 5.f;                 // "far": more than (1 + ML_FAR1) half-widths from the centre
+constexpr float ML_FAR1 = 3.f;                 // "far": more than (1 + ML_FAR1) half-widths from the centre
 constexpr float ML_MIN_H1 = 32.f;              // smallest chunk half-width (points) using level 1
 constexpr float ML_MIN_H2 = 16.f;              // smallest sub-chunk half-width using level 2
 
