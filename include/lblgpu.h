@@ -173,7 +173,7 @@ int lbl_ml_inner_ranges(const LineIn* lines, const int* n_kept, double nu_min, d
 /* Same contract as lbl_tau_tiles_f32, multi-level float32 summation (the
  * default float32 engine): per chunk (<= 2048 points of one reference tile),
  * lines farther than a chunk half-width contribute through 16 Chebyshev nodes over
- * the chunk (8 beyond six half-widths; a line-per-thread kernel that runs first and
+ * the chunk (8 beyond four half-widths; a line-per-thread kernel that runs first and
  * leaves the chunk's coefficients in l1_work), the remaining lines farther than a
  * 256-point sub-chunk half-width through 16 nodes over that sub-chunk, the rest
  * directly; one warp per sub-chunk does levels 2 and 3. inner (nullable; from
@@ -214,7 +214,7 @@ long long lbl_ml_work_floats(int n_rows, int tile_samples, int tile_count);
  * coefficients in l1_work (lbl_jacobian_ml_work_floats floats, required); inner
  * (nullable) are the ranges of lbl_ml_inner_ranges for the same grid, a superset of
  * the inner lines of this kernel's smaller chunks; near (nullable) those of
- * lbl_jac_near_ranges, which limit the level-1 pass over lines within six chunk
+ * lbl_jac_near_ranges, which limit the level-1 pass over lines within four chunk
  * half-widths. NULL scans every candidate (same results, slower). */
 int lbl_jacobian_ml_f32(const LineF32* prep, const LineJac* jprep, int n_lines, const int* ranges, const int* inner,
                         const int* near, const double* t_layer, int n_rows, int n_lay, double nu_min, double step, long long n_nu,
@@ -222,7 +222,7 @@ int lbl_jacobian_ml_f32(const LineF32* prep, const LineJac* jprep, int n_lines, 
                         const double* g_tau, double* vjp_t, double* vjp_v, int flags, void* stream);
 
 /* Per-tile candidate range [near[2t], near[2t+1]) of the level-1 lines of
- * lbl_jacobian_ml_f32 that lie within six chunk half-widths of a chunk (same search as
+ * lbl_jacobian_ml_f32 that lie within four chunk half-widths of a chunk (same search as
  * lbl_tile_ranges, pad as there). No reference counterpart: an index of the summation. */
 int lbl_jac_near_ranges(const LineIn* lines, const int* n_kept, double nu_min, double step, long long n_nu,
                         int tile_samples, double pad, int n_tiles, int* near, void* stream);

@@ -41,8 +41,8 @@ constexpr int MJ_NBW = 128;                        // near items buffered per wa
 // Chebyshev node offsets (fractions of the half-width) and DCT weights, row-major [k][j]
 static __constant__ float c_jnode16[MJ_K] = {LBL_CHEB16_NODES};
 static __constant__ double c_jdct16[MJ_K * MJ_K] = {LBL_DCT16};
-constexpr int MJ_KF = 8;                           // nodes for level-1 lines beyond six half-widths
-constexpr float MJ_FAR1 = 5.f;                     // "far": more than (1 + MJ_FAR1) half-widths from the centre
+constexpr int MJ_KF = 8;                           // nodes for level-1 lines beyond four half-widths
+constexpr float MJ_FAR1 = 3.f;                     // "far": more than (1 + MJ_FAR1) half-widths from the centre
 constexpr int MJ_NCOEF = 3 * (MJ_K + MJ_KF);       // level-1 coefficients per (chunk, row)
 constexpr int MJF_THREADS = 256;                   // lines per round of jac_far_kernel
 constexpr int MJF_STAGES = 2;                      // rounds of line records in flight per thread
@@ -197,7 +197,7 @@ __device__ __forceinline__ float clenshaw_k(const float* c, float t) {
 // ---------------------------------------------------------------------------
 // Level 1 of the Jacobian sums as its own kernel (as tau_far_kernel for the optical
 // depth): one thread takes one level-1 line and evaluates u, u_x, u_y at all of the
-// chunk's Chebyshev nodes (16; 8 beyond six half-widths), adding the three weighted sums
+// chunk's Chebyshev nodes (16; 8 beyond four half-widths), adding the three weighted sums
 // in registers. It writes the chunk's 3 x (16 + 8) Chebyshev coefficients to l1_coef
 // ([row][chunk of the launch][MJ_NCOEF]), which jac_ml_kernel reads.
 struct JFarLine {
@@ -243,7 +243,7 @@ __device__ __forceinline__ void jfar_line(float (&f)[3][K], const float (&xs)[K 
 }
 
 // One pass of jac_far_kernel over the tile's candidate lines for the lines of one node
-// class (K = MJ_K: level-1 lines within six half-widths; K = MJ_KF: beyond); the warp's
+// class (K = MJ_K: level-1 lines within four half-widths; K = MJ_KF: beyond); the warp's
 // float64 sums of that class go to row[q * K + k]. Two passes keep 3 K accumulators live
 // instead of 3 (MJ_K + MJ_KF).
 template <int K>
@@ -335,7 +335,7 @@ jac_far_kernel(const LineF32* __restrict__ prep, const LineJac* __restrict__ jpr
   for (int k = 0; k < MJ_K / 2; ++k) xa[k] = H1 * c_jnode16[k];
 #pragma unroll
   for (int k = 0; k < MJ_KF / 2; ++k) xb[k] = H1 * c_jnode8[k];
-  // the 16-node class lies within six half-widths of the chunk: its pass reads only the
+  // the 16-node class lies within four half-widths of the chunk: its pass reads only the
   // tile's near range (lbl_jac_near_ranges) when one is given
   int2 rng16 = rng;
   if (near_ranges) {
@@ -495,7 +495,7 @@ jac_ml_kernel(const LineF32* __restrict__ prep, const LineJac* __restrict__ jpre
     }
     __syncthreads();
 
-    // per-warp split of the inner lines into level 2 (16 nodes; 8 beyond six sub-chunk
+    // per-warp split of the inner lines into level 2 (16 nodes; 8 beyond four sub-chunk
     // half-widths, listed from the back of s_l2) and level 3
     int n2w = 0, n2fw = 0, n3w = 0;
     for (int k = 0; k < n2; k += 32) {
@@ -825,14 +825,14 @@ extern "C" int lbl_jac_near_ranges(const LineIn* lines, const int* n_kept, doubl
                                    int tile_samples, double pad, int n_tiles, int* near, void* stream) {
   if (tile_samples < 1 || !(step > 0) || n_nu < 1)
     return lbl_set_error(LBL_EINVAL, "lbl_jac_near_ranges: bad arguments");
-  // A 16-node level-1 line of a chunk (half-width H) has |j0 - centre| <= 6H, so its centre
-  // lies within 5H + 1.5 grid steps of the chunk; chunks lie inside their tile and have at
-  // most min(tile_samples, chunk size) points. Two further steps absorb rounding.
+  // A 16-node level-1 line of a chunk (half-width H) has |j0 - centre| <= (1 + MJ_FAR1) H, so
+  // its centre lies within MJ_FAR1 H + 1.5 grid steps of the chunk; chunks lie inside their tile
+  // and have at most min(tile_samples, chunk size) points. Two further steps absorb rounding.
   int threads, cp;
   long long n_all, chunks;
   jac_geometry(tile_samples, n_nu, &threads, &cp, &n_all, &chunks);
   const int n_c_max = tile_samples < cp ? tile_samples : cp;
-  const double reach = (2.5 * (n_c_max - 1) + 3.5) * step;
+  const double reach = (0.5 * MJ_FAR1 * (n_c_max - 1) + 3.5) * step;
   return lbl_tile_ranges(lines, n_kept, nu_min, step, n_nu, tile_samples, reach, pad, n_tiles, near, stream);
 }
 
