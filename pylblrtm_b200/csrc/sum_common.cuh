@@ -6,6 +6,20 @@
 
 namespace lbl {
 
+// Points [c0, c0 + n_c) of chunk `chunk` of the tile [t0, t1): a tile of n points is cut
+// into ceil(n / chunk_max) chunks of near-equal size, none longer than chunk_max, so no
+// chunk is a sliver too short for the far-field levels (a 1,050-point tile gives 525 + 525,
+// not 1,024 + 26). Returns false for a chunk index the tile does not have.
+__device__ __forceinline__ bool tile_chunk(long long t0, long long t1, int chunk, int chunk_max, long long& c0,
+                                           int& n_c) {
+  const long long n = t1 - t0;
+  const long long nch = (n + chunk_max - 1) / chunk_max;
+  if (chunk >= nch) return false;
+  c0 = t0 + chunk * n / nch;
+  n_c = (int)(t0 + (chunk + 1) * n / nch - c0);
+  return true;
+}
+
 __device__ __forceinline__ float rcp_approx(float v) {
   float r;
   asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(v));

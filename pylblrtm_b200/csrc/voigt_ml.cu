@@ -194,9 +194,9 @@ tau_far_kernel(const LineF32* __restrict__ prep, int n_lines, const int2* __rest
   const int tile = tile_first + (int)(blockIdx.x / chunks_per_tile), chunk = blockIdx.x % chunks_per_tile;
   const long long t0 = (long long)tile * tile_samples;
   const long long t1 = min(t0 + (long long)tile_samples, n_nu);
-  const long long c0 = t0 + (long long)chunk * chunk_pts;
-  if (c0 >= t1) return;
-  const int n_c = (int)(min(c0 + (long long)chunk_pts, t1) - c0);
+  long long c0;
+  int n_c;
+  if (!tile_chunk(t0, t1, chunk, chunk_pts, c0, n_c)) return;
   const float H1 = 0.5f * (float)(n_c - 1), C1 = H1;      // same chunk geometry as tau_ml_kernel
   if (!(H1 >= ML_MIN_H1)) return;                         // no level 1: tau_ml_kernel takes every line
   const int c0i = (int)c0;
@@ -489,9 +489,9 @@ tau_ml_kernel(const LineF32* __restrict__ prep, int n_lines, const int2* __restr
   const int tile = tile_first + chunk_id / chunks_per_tile, chunk = chunk_id % chunks_per_tile;
   const long long t0 = (long long)tile * tile_samples;
   const long long t1 = min(t0 + (long long)tile_samples, n_nu);
-  const long long c0 = t0 + (long long)chunk * chunk_pts;
-  if (c0 >= t1) return;
-  const int n_c = (int)(min(c0 + (long long)chunk_pts, t1) - c0);
+  long long c0;
+  int n_c;
+  if (!tile_chunk(t0, t1, chunk, chunk_pts, c0, n_c)) return;
   const int first_sub = part * NW, p0 = first_sub * ML_WARP_PTS;   // this CTA's first sub-chunk and point
   if (p0 >= n_c) return;
   const int c0i = (int)c0;

@@ -316,9 +316,9 @@ jac_far_kernel(const LineF32* __restrict__ prep, const LineJac* __restrict__ jpr
   const int tile = blockIdx.x / chunks_per_tile, chunk = blockIdx.x % chunks_per_tile;
   const long long t0 = (long long)tile * tile_samples;
   const long long t1 = min(t0 + (long long)tile_samples, n_nu);
-  const long long c0 = t0 + (long long)chunk * chunk_pts;
-  if (c0 >= t1) return;
-  const int n_c = (int)(min(c0 + (long long)chunk_pts, t1) - c0);
+  long long c0;
+  int n_c;
+  if (!tile_chunk(t0, t1, chunk, chunk_pts, c0, n_c)) return;
   const float H1 = 0.5f * (float)(n_c - 1);               // same chunk geometry as jac_ml_kernel
   if (!(H1 >= MJ_MIN_H1)) return;                         // no level 1: jac_ml_kernel takes every line
   const double wlo = __dsub_rn(grid_nu(nu_min, step, t0), cutoff);
@@ -390,9 +390,9 @@ jac_ml_kernel(const LineF32* __restrict__ prep, const LineJac* __restrict__ jpre
   const int tile = blockIdx.x / chunks_per_tile, chunk = blockIdx.x % chunks_per_tile;
   const long long t0 = (long long)tile * tile_samples;
   const long long t1 = min(t0 + (long long)tile_samples, n_nu);
-  const long long c0 = t0 + (long long)chunk * (blockDim.x * P);
-  if (c0 >= t1) return;
-  const int n_c = (int)(min(c0 + (long long)(blockDim.x * P), t1) - c0);
+  long long c0;
+  int n_c;
+  if (!tile_chunk(t0, t1, chunk, blockDim.x * P, c0, n_c)) return;
   const double wlo = __dsub_rn(grid_nu(nu_min, step, t0), cutoff);
   const double whi = __dadd_rn(grid_nu(nu_min, step, t1 - 1), cutoff);
   const LineF32* lp = prep + (long long)row * n_lines;

@@ -686,7 +686,7 @@ def _jacobian_impl(job: Job, gas: str, g_tau=None, deterministic: bool = False):
     inner = torch.empty_like(ranges)
     _lib.call("lbl_ml_inner_ranges", lines.data_ptr(), job._kept.data_ptr(), grid.nu_min, grid.step, n_nu,
               grid.tile_samples, job.pad, ranges.shape[0], inner.data_ptr(), stream)
-    near = torch.empty_like(ranges)         # level-1 lines within six chunk half-widths
+    near = torch.empty_like(ranges)         # level-1 lines within four chunk half-widths
     _lib.call("lbl_jac_near_ranges", lines.data_ptr(), job._kept.data_ptr(), grid.nu_min, grid.step, n_nu,
               grid.tile_samples, job.pad, ranges.shape[0], near.data_ptr(), stream)
     l1_work = torch.empty((_lib.load().lbl_jacobian_ml_work_floats(n_rows, n_nu, grid.tile_samples),),
