@@ -444,9 +444,12 @@ def main():
     else:
         job = engine.Job(sd, engine.layer_input_from_profile(prof), grid, 25.0)
 
+    # Steps are queued back to back: each call returns once its stages are queued and its
+    # error word is checked after the timed region (Job.run(defer_errors=True)), so the
+    # next step's small stages queue behind this one's summation instead of waiting for it.
     def step(timer=None, count_evals=False):
         r = job.run(a.precision, mu=[0.8], want_od=False, want_trans=True, timer=timer, count_evals=count_evals,
-                    tiles=tiles)
+                    tiles=tiles, defer_errors=not count_evals)
         if mode == "wavenumber" and world > 1:       # the exchange: every rank gets the whole spectrum
             piece[: r.trans.shape[1]].copy_(r.trans[0])
             dist.all_gather_into_tensor(gathered, piece)
@@ -473,16 +476,17 @@ def main():
         torch.cuda.synchronize()
 
     for _ in range(a.warmup):
-        step()
+        step().check()
     timer = {}
     barrier()
     with ClockSampler(local) as clocks:
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record()
-        for _ in range(a.steps):
-            step(timer=timer)
+        done = [step(timer=timer) for _ in range(a.steps)]
         e1.record()
         barrier()
+    for r in done:
+        r.check()                                    # every step's error word, after the timing
     ms = e0.elapsed_time(e1)
     tau_ms = [b.elapsed_time(c) for b, c in timer["tau_events"]]
     if world > 1:

@@ -260,6 +260,14 @@ class EngineResult:
     work: int = 0                  # Faddeeva evaluations actually performed (multi-level engine)
     work_split: tuple = ()         # (node evaluations, level-3 loop evaluations, near-zone points)
     groups: List[Group] = field(default_factory=list)
+    pending: object = None         # the deferred error check of Job.run(defer_errors=True)
+
+    def check(self) -> None:
+        """Raise the device error of a run made with ``defer_errors=True`` (waits for that run's
+        device work); a no-op for other results and after the first call."""
+        if self.pending is not None:
+            f, self.pending = self.pending, None
+            f()
 
 
 _GRID_POOL = None
@@ -519,8 +527,14 @@ class Job:
     def run(self, precision: str = "fp32", mu: Optional[Sequence[float]] = None, want_od: bool = True,
             want_tau: bool = False, want_trans: bool = False, count_evals: bool = False,
             timer: Optional[dict] = None, channels: Optional[Tuple[int, int]] = None,
-            deterministic: bool = False, tiles: Optional[Tuple[int, int]] = None) -> EngineResult:
+            deterministic: bool = False, tiles: Optional[Tuple[int, int]] = None,
+            defer_errors: bool = False) -> EngineResult:
         """All device stages; ``timer`` (dict) receives CUDA-event times of the summation kernel.
+
+        The device error word (non-finite or negative line strengths, non-finite optical
+        depths) is read at the end, which waits for the device. ``defer_errors=True`` skips
+        that wait: the call returns once every stage is queued and ``result.check()`` raises
+        the error later, so a caller can queue the next call while this one runs.
 
         ``channels = (width_points, n_channels)`` adds channel-mean transmittances
         over consecutive half-open blocks of ``width_points`` grid points.
@@ -633,7 +647,10 @@ class Job:
             timer.setdefault("tau_events", []).append((e0, e1))
         self.launches += 2
         finish(od)                          # queue the layer sums before the error word is read
-        self._raise_on_error(err, n_grp)
+        if defer_errors and evals is None:
+            res.pending = lambda: self._raise_on_error(err, n_grp)
+        else:
+            self._raise_on_error(err, n_grp)
         if evals is not None:
             ev = evals.cpu().tolist()
             res.evals = int(ev[0])

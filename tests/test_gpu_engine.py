@@ -157,6 +157,29 @@ def test_nonfinite_or_negative_strength_raises(cuda, precision):
                                       precision=precision)
 
 
+def test_deferred_error_check_raises_later(cuda):
+    """Job.run(defer_errors=True) queues every stage and returns; result.check() then raises
+    the same error the blocking call raises, and a clean run's check() passes."""
+    sd, prof, prm, _ = golden_case("edge_mix")
+    lines = {k: v.copy() for k, v in sd.lines.items()}
+    co2 = np.flatnonzero((lines["mol_id"] == 2) & (lines["iso_id"] == 1) & (lines["nu0"] > 700.5))
+    lines["Sref"][co2[0]] = np.nan
+    grid = engine.make_grid(prm["nu_min"], prm["nu_max"], prm["step"], prm["tile"])
+    with warnings.catch_warnings():
+        warnings.simplefilter("ignore")
+        good = engine.Job(sd, engine.layer_input_from_profile(prof), grid, prm["cutoff"])
+        bad = engine.Job(SpectralData(lines, sd.tips, sd.molar_masses), engine.layer_input_from_profile(prof), grid,
+                         prm["cutoff"])
+    rb = bad.run("fp32", mu=[1.0], want_od=False, want_trans=True, defer_errors=True)
+    rg = good.run("fp32", mu=[1.0], want_od=False, want_trans=True, defer_errors=True)
+    rg.check()
+    with pytest.raises(FloatingPointError, match=r"^Layer 0, gas 'CO2': non-finite or negative line strength$"):
+        rb.check()
+    rb.check()                                      # raised once; the check is then spent
+    ref = good.run("fp32", mu=[1.0], want_od=False, want_trans=True)
+    assert torch.allclose(rg.trans, ref.trans, rtol=1e-6, atol=0)
+
+
 def test_missing_tips_raises_keyerror(cuda):
     sd, prof, prm, _ = golden_case("tile2.0")
     with pytest.raises(KeyError, match="No TIPS data"):
