@@ -28,6 +28,10 @@ void lbl_host_faddeeva_f32(const float* x, const float* y, long long n, float* r
       re[i] = lbl::faddeeva_re_f32(x[i], y[i]);
       continue;
     }
+    if (mode == 2) {                       // the near-zone tails' eight-term series (36 <= |z|^2 < 64)
+      re[i] = lbl::re_w_asym8(y[i], x[i] * x[i] + y[i] * y[i]);
+      continue;
+    }
     const lbl::cpx<float> w = lbl::faddeeva<float>(x[i], y[i]);
     re[i] = w.re;
     im[i] = w.im;

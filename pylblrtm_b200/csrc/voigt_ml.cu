@@ -20,8 +20,8 @@
 //           loop is branch-free: it evaluates the five-term asymptotic form with
 //           |z|^2 clamped to >= MID_Z2 = 64, so every point inside a line's near
 //           zone receives the same constant. A CTA-wide near pass then gives each
-//           near point (accurate value - that constant): float continued fraction
-//           for 36 <= |z|^2 < 64, Weideman's float64 approximation below.
+//           near point (accurate value - that constant): eight terms of the float
+//           asymptotic series for 36 <= |z|^2 < 64, Weideman's float64 approximation below.
 //
 // Inside a reference tile the set of lines is fixed, so every level-1/2 sum is
 // smooth over its interval; the window test keeps the reference's truncation.
@@ -432,7 +432,7 @@ __device__ __forceinline__ void level2_lines(float (&f)[K], const unsigned char*
 // formed exactly as in the level-3 loop, so the clamped constant h.w cancels. Items of
 // a zone's middle (MID) take the float64 core at every point, the margin points with
 // |z|^2 >= CORE_Z2 included (28-term set: Re w within 8e-8 there too), so no lane of a
-// warp branches off to the continued fraction; tail items take the continued fraction.
+// warp branches off to another form; tail items take the eight-term asymptotic series.
 template <bool MID>
 __device__ __forceinline__ float near_correction(int p, const float4& g, const float4& h) {
   const float x0 = fmaf((float)(p & ~(ML_P - 1)) - g.x, g.y, -g.z);
@@ -441,7 +441,7 @@ __device__ __forceinline__ float near_correction(int p, const float4& g, const f
   if (z2 >= MID_Z2) return 0.f;
   float v;
   if (MID) v = (float)((double)h.z * weideman_re_f32((double)x, (double)h.x));
-  else if (z2 >= CORE_Z2 && h.x >= 0.f) v = h.z * re_w_cf32(x, h.x, z2);
+  else if (z2 >= CORE_Z2 && h.x >= 0.f) v = h.z * re_w_asym8(h.x, z2);
   else v = (float)((double)h.z * weideman_re_f32_compact((double)x, (double)h.x));
   return v - h.w;
 }
