@@ -49,11 +49,11 @@ CPU_SAMPLE = (1000.0, 1000.5)  # sub-window timed on the host (all 60 layers)
 
 # DRAM traffic of one lbl_tau_tiles_ml_f32 call on the default workload (200k lines, 60
 # layers, 600-2500 cm^-1), from a single-pass ncu capture of its two launches
-# (profiles/launches_three_gas_200k_fp32_ml.md): tau_far_kernel 384.15 MB read + 7.83 MB
-# written, tau_ml_kernel 394.40 MB read + 471.57 MB written. Each kernel reads the 384 MB
-# of line records once; tau_ml_kernel writes the 456 MB optical depth (471.6 MB written
-# in all).
-TAU_ML_DRAM_BYTES = 384.146176e6 + 7.834624e6 + 394.399232e6 + 471.572992e6
+# (profiles/launches_three_gas_200k_fp32_ml.md): tau_far_kernel 384.53 MB read + 7.91 MB
+# written, tau_ml_kernel 391.63 MB read + 451.51 MB written. Each kernel reads the 384 MB
+# of line records once; tau_ml_kernel writes the 456 MB optical depth (part of it still in
+# L2 when the launch ends).
+TAU_ML_DRAM_BYTES = 384.532480e6 + 7.905280e6 + 391.629568e6 + 451.512064e6
 
 
 def parse():
