@@ -121,25 +121,49 @@ __device__ __forceinline__ U3 series3(float x, float y, float r) {
   return o;
 }
 
-// Accurate u, u_x, u_y for |z|^2 < MID_Z2 (continued fraction or Weideman). With core
-// set, Weideman's float64 form at any |z|^2 (the 28-term set stays within 8e-8 of Re w up
-// to MID_Z2), so the items of a zone's middle never branch off to the continued fraction.
+// u, u_x, u_y from eight terms of the asymptotic series in its real-part form (as re_w_asym8
+// in faddeeva.cuh): u = (y/sqrt(pi)) r S with S = 1 + sum_{k=1..7} r^k A_k(q), r = 1/|z|^2,
+// q = y^2 r, and by Cauchy-Riemann (u_x = Re w', u_y = -Im w' are the x and y derivatives of u)
+//   u_x = -(2xy/sqrt(pi)) r^2 (S + r S_r + q S_q),
+//   u_y = (r/sqrt(pi)) (S - 2q S - 2q r S_r + 2q (1 - q) S_q),
+// with S_r, S_q the partial derivatives of S. For CORE_Z2 <= |z|^2 < MID_Z2 all three stay within
+// 6.3e-8 of |w| and |w'| (float64 evaluation, against scipy.special.wofz). Forming w' =
+// -2zw + 2i/sqrt(pi) from the float continued fraction's w there cancels ~70x of w's rounding.
+__device__ __forceinline__ U3 asym8_u3(float x, float y, float z2) {
+  const float r = __fdividef(1.0f, z2), q = y * y * r;
+  const float a1 = fmaf(-2.0f, q, 1.5f);
+  const float d1 = -2.0f;
+  const float a2 = fmaf(fmaf(12.0f, q, -15.0f), q, 3.75f);
+  const float d2 = fmaf(24.0f, q, -15.0f);
+  const float a3 = fmaf(fmaf(fmaf(-120.0f, q, 210.0f), q, -105.0f), q, 13.125f);
+  const float d3 = fmaf(fmaf(-360.0f, q, 420.0f), q, -105.0f);
+  const float a4 = fmaf(fmaf(fmaf(fmaf(1680.0f, q, -3780.0f), q, 2835.0f), q, -787.5f), q, 59.0625f);
+  const float d4 = fmaf(fmaf(fmaf(6720.0f, q, -11340.0f), q, 5670.0f), q, -787.5f);
+  const float a5 = fmaf(fmaf(fmaf(fmaf(fmaf(-30240.0f, q, 83160.0f), q, -83160.0f), q, 36382.5f), q, -6496.875f), q, 324.84375f);
+  const float d5 = fmaf(fmaf(fmaf(fmaf(-151200.0f, q, 332640.0f), q, -249480.0f), q, 72765.0f), q, -6496.875f);
+  const float a6 = fmaf(fmaf(fmaf(fmaf(fmaf(fmaf(665280.0f, q, -2162160.0f), q, 2702700.0f), q, -1621620.0f), q, 472972.5f), q, -59121.5625f), q, 2111.484375f);
+  const float d6 = fmaf(fmaf(fmaf(fmaf(fmaf(3991680.0f, q, -10810800.0f), q, 10810800.0f), q, -4864860.0f), q, 945945.0f), q, -59121.5625f);
+  const float a7 = fmaf(fmaf(fmaf(fmaf(fmaf(fmaf(fmaf(-17297280.0f, q, 64864800.0f), q, -97297200.0f), q, 74324250.0f), q, -30405375.0f), q, 6385128.75f), q, -591215.625f), q, 15836.1328125f);
+  const float d7 = fmaf(fmaf(fmaf(fmaf(fmaf(fmaf(-121080960.0f, q, 389188800.0f), q, -486486000.0f), q, 297297000.0f), q, -91216125.0f), q, 12770257.5f), q, -591215.625f);
+  const float s = fmaf(fmaf(fmaf(fmaf(fmaf(fmaf(a7, r, a6), r, a5), r, a4), r, a3), r, a2), r, a1) * r + 1.0f;
+  const float sr = fmaf(fmaf(fmaf(fmaf(fmaf(fmaf(7.0f * a7, r, 6.0f * a6), r, 5.0f * a5), r, 4.0f * a4), r, 3.0f * a3), r,
+                        2.0f * a2), r, a1);
+  const float sq = fmaf(fmaf(fmaf(fmaf(fmaf(fmaf(d7, r, d6), r, d5), r, d4), r, d3), r, d2), r, d1) * r;
+  const float k = float(INV_SQRT_PI);
+  U3 o;
+  o.u = k * y * r * s;
+  o.ux = -2.0f * k * x * y * r * r * fmaf(q, sq, fmaf(r, sr, s));
+  o.uy = k * r * fmaf(2.0f * q * (1.0f - q), sq, fmaf(-2.0f * q * r, sr, fmaf(-2.0f * q, s, s)));
+  return o;
+}
+
+// Accurate u, u_x, u_y for |z|^2 < MID_Z2 (the eight-term series above CORE_Z2, Weideman
+// below). With core set, Weideman's float64 form at any |z|^2 (the 28-term set stays within
+// 8e-8 of Re w up to MID_Z2), so the items of a zone's middle never branch off.
 __device__ __noinline__ U3 near3(float x, float y, float z2, bool core = false) {
   double wr, wi;
-  if (!core && z2 >= CORE_Z2 && y >= 0.f) {
-    const int depth = cf_depth<float>(z2);
-    float rr = 0.f, ri = 0.f;
-    for (int n = depth - 1; n >= 0; --n) {
-      const float cr = y + float(n + 1) * rr;
-      const float ci = -x + float(n + 1) * ri;
-      const float inv = __fdividef(0.5f, cr * cr + ci * ci);
-      rr = cr * inv;
-      ri = -ci * inv;
-    }
-    wr = TWO_INV_SQRT_PI * rr;
-    wi = TWO_INV_SQRT_PI * ri;
-    if (y < 0.1f) wr += exp(fmin((double)y * y - (double)x * x, 0.0)) * cos(2.0 * x * y);
-  } else if (y >= 0.f) {
+  if (!core && z2 >= CORE_Z2 && y >= 0.f) return asym8_u3(x, y, z2);
+  if (y >= 0.f) {
     const cpx<double> w = weideman_upper_n<LBL_WEIDEMAN28_N>(x, y);
     wr = w.re;
     wi = w.im;
