@@ -274,6 +274,35 @@ def test_channel_mean_matches_host_box_average(cuda):
     np.testing.assert_allclose(centres, nu[:5000].reshape(20, 250).mean(axis=1), rtol=0, atol=1e-9)
 
 
+def test_channel_means_against_oracle(cuda):
+    """Device channel means (box averages of T over 200 grid points) against the oracle's
+    float64 transmittance averaged on the host, per profile and view cosine."""
+    lo, hi, cutoff, step = 1500.0, 1503.0, 3.0, 0.001
+    sd = synthetic.restrict(synthetic.three_gas_lines(4000, lo - cutoff - 1, hi + cutoff + 1, seed=21),
+                            lo - cutoff - 1, hi + cutoff + 1)
+    lv = synthetic.perturbed_levels(synthetic.logp_levels(7), 2, seed=8)
+    for g in ("H2O", "CO2", "O3"):                         # thin the column to optical depths of order 1
+        lv[g] = lv[g] * 2e-5
+    mu = np.array([0.9, 0.6])
+    nu = restate.grid(lo, hi, step)
+    width = 200
+    n_ch = nu.size // width
+    ref = np.empty((2, n_ch))
+    for i in range(2):
+        inp = oracle_inputs(sd, synthetic.profile_from_levels(lv, i))
+        od = restate.optical_depth(nu, inp["lines"], inp["tips"], inp["masses"], inp["p_atm"], inp["t_layer"],
+                                   inp["vmr_layer"], inp["col"], cutoff, 2.0)
+        ref[i] = restate.transmittance(nu, od, mu[i])[: n_ch * width].reshape(n_ch, width).mean(axis=1)
+    assert 0.01 < ref.min() and ref.max() < 0.95             # neither saturated nor transparent
+    for precision in ("fp64", "fp32"):
+        centres, ch = lbl.transmittance_batch(sd, lv["p"], lv["t"], {g: lv[g] for g in ("H2O", "CO2", "O3")},
+                                              lo, hi, step_cm1=step, line_cutoff_cm1=cutoff, mu_view=mu,
+                                              precision=precision, channel_width_cm1=width * step)
+        assert ch.shape == (2, n_ch)
+        assert np.max(np.abs(ch - ref)) <= TOL[precision]["dT"], precision
+        np.testing.assert_allclose(centres, nu[: n_ch * width].reshape(n_ch, width).mean(axis=1), rtol=0, atol=1e-9)
+
+
 def test_fp32_bitwise_reproducible_with_overlapping_near_zones(cuda):
     """300 lines per cm^-1 (near zones overlap): repeated launches and a batch of
     profiles give the same float32 optical depth bit for bit, for both precisions."""
