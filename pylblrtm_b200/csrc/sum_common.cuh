@@ -72,6 +72,37 @@ __device__ __forceinline__ void cp_async_wait() {
   asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
 }
 
+// Line records staged in shared memory as 16-byte planes, plane[k][slot] holding bytes
+// 16k..16k+15 of slot's record: a thread reading its own slot then reads 16 consecutive
+// bytes per thread per plane, so the eight threads of each quarter-warp phase of a
+// 128-bit load hit eight different 16-byte bank groups (a 32- or 64-byte record read
+// whole from an array of records puts them on 4 or 2 groups). The records are put
+// back together field by field (little-endian byte order of the device).
+static_assert(sizeof(LineF32) == 32 && sizeof(LineJac) == 32, "line records are two 16-byte planes");
+__device__ __forceinline__ LineF32 line_f32_from_planes(const float4& p0, const float4& p1) {
+  LineF32 L;
+  L.nuc = __hiloint2double(__float_as_int(p0.y), __float_as_int(p0.x));   // bytes 0-7
+  L.j0 = __float_as_int(p0.z);                                             // bytes 8-11
+  L.b = p0.w;
+  L.a = p1.x;
+  L.y = p1.y;
+  L.amp = p1.z;
+  L.amp_far = p1.w;
+  return L;
+}
+__device__ __forceinline__ LineJac line_jac_from_planes(const float4& p0, const float4& p1) {
+  LineJac J;
+  J.jT_u = p0.x;
+  J.jT_x = p0.y;
+  J.jT_y = p0.z;
+  J.jv_u = p0.w;
+  J.jv_y = p1.x;
+  J.jv_x = p1.y;
+  J.pad0 = p1.z;
+  J.pad1 = p1.w;
+  return J;
+}
+
 // Adds the lanes' float node sums into the warp's float64 sums (lane 0 owns the row)
 // and clears them; every lane of the warp calls it.
 template <int K>

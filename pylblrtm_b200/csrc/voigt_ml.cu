@@ -135,9 +135,10 @@ __device__ __forceinline__ float clenshaw16(const float* c, float t) {
 // ---------------------------------------------------------------------------
 // Level 1 as its own kernel. Nine in ten lines of a chunk's window are level-1
 // lines; each contributes only through the chunk's Chebyshev nodes, so one thread
-// takes one line and evaluates it at all nodes from registers (no shared-memory
-// staging, no barriers). The kernel leaves the chunk's 16 + 8 Chebyshev coefficients
-// in l1_work ([row][chunk of the launch][24]), which tau_ml_kernel reads.
+// takes one line and evaluates it at all nodes from registers (each thread copies its
+// own records through a cp.async ring; no barriers). The kernel leaves the chunk's
+// 16 + 8 Chebyshev coefficients in l1_work ([row][chunk of the launch][24]), which
+// tau_ml_kernel reads.
 constexpr int MF_THREADS = 256;                // lines per round
 constexpr int MF_FLUSH = 32;                   // rounds summed in float before the double sums
 
@@ -185,6 +186,9 @@ __global__ void __launch_bounds__(MF_THREADS, 4)
 tau_far_kernel(const LineF32* __restrict__ prep, int n_lines, const int2* __restrict__ ranges, double nu_min,
                double step, long long n_nu, int tile_samples, int chunks_per_tile, int chunk_pts, double cutoff,
                float* __restrict__ l1_work, unsigned long long* evals, unsigned long long* work, int tile_first) {
+  // Whole 32-B records: read back by their own thread they meet 2-way bank conflicts, but
+  // the 16-B planes that jac_far_kernel stages its records in (no conflicts) made this
+  // kernel slower (summation call 10.40 -> 11.06 ms, with more spilled registers).
   __shared__ __align__(16) LineF32 s_line[MF_STAGES][MF_THREADS];   // records are 32 B, 16-B aligned
   __shared__ double s_part[MF_THREADS / 32][ML_K + ML_KF];
   __shared__ float s_coef[ML_K + ML_KF];

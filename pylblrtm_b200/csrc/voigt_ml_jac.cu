@@ -271,7 +271,7 @@ __device__ __forceinline__ void jfar_line(float (&f)[3][K], const float (&xs)[K 
 // float64 sums of that class go to row[q * K + k]. Two passes keep 3 K accumulators live
 // instead of 3 (MJ_K + MJ_KF).
 template <int K>
-__device__ __forceinline__ void jfar_pass(JFarLine (*s_line)[MJF_THREADS], const LineF32* lp, const LineJac* jp,
+__device__ __forceinline__ void jfar_pass(float4 (*s_line)[4][MJF_THREADS], const LineF32* lp, const LineJac* jp,
                                           int2 rng, double wlo, double whi, long long c0, float H1,
                                           const float (&xs)[K / 2], double* row) {
   const int tid = threadIdx.x, lane = tid & 31;
@@ -289,11 +289,10 @@ __device__ __forceinline__ void jfar_pass(JFarLine (*s_line)[MJF_THREADS], const
     if (li < rng.y) {   // 32-B records in 256-B aligned allocations
       const float4* g = reinterpret_cast<const float4*>(lp + li);
       const float4* h = reinterpret_cast<const float4*>(jp + li);
-      float4* d = reinterpret_cast<float4*>(&s_line[stage][tid]);
-      cp_async16(d, g);
-      cp_async16(d + 1, g + 1);
-      cp_async16(d + 2, h);
-      cp_async16(d + 3, h + 1);
+      cp_async16(&s_line[stage][0][tid], g);
+      cp_async16(&s_line[stage][1][tid], g + 1);
+      cp_async16(&s_line[stage][2][tid], h);
+      cp_async16(&s_line[stage][3][tid], h + 1);
     }
     cp_async_commit();
   };
@@ -305,7 +304,10 @@ __device__ __forceinline__ void jfar_pass(JFarLine (*s_line)[MJF_THREADS], const
     cp_async_wait<1>();
     const bool have = rng.x + r * MJF_THREADS + tid < rng.y;
     JFarLine R;
-    if (have) R = s_line[stage][tid];
+    if (have) {
+      R.l = line_f32_from_planes(s_line[stage][0][tid], s_line[stage][1][tid]);
+      R.j = line_jac_from_planes(s_line[stage][2][tid], s_line[stage][3][tid]);
+    }
     // the level-1 test of jac_ml_kernel, expression for expression, then the node class
     const bool pass = have && (R.l.nuc >= wlo) && (R.l.nuc <= whi);
     const float jf = (float)((long long)R.l.j0 - c0);
@@ -333,7 +335,7 @@ jac_far_kernel(const LineF32* __restrict__ prep, const LineJac* __restrict__ jpr
                const int2* __restrict__ ranges, const int2* __restrict__ near_ranges, double nu_min, double step,
                long long n_nu, int tile_samples, int chunks_per_tile, int chunk_pts, double cutoff,
                float* __restrict__ l1_coef) {
-  __shared__ __align__(16) JFarLine s_line[MJF_STAGES][MJF_THREADS];   // records 64 B, 16-B aligned
+  __shared__ __align__(16) float4 s_line[MJF_STAGES][4][MJF_THREADS];  // 64-B records as four 16-B planes
   __shared__ double s_part[MJF_THREADS / 32][MJ_NCOEF];                 // [q][16] then [q][8] per warp
 
   const int row = blockIdx.y;
