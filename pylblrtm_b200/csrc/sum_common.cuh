@@ -1,6 +1,8 @@
 // Device helpers shared by the summation kernels (voigt.cu, voigt_ml.cu, voigt_ml_jac.cu).
 #pragma once
 
+#include <stddef.h>
+
 #include "faddeeva.cuh"
 #include "lbl_common.cuh"
 
@@ -79,6 +81,13 @@ __device__ __forceinline__ void cp_async_wait() {
 // whole from an array of records puts them on 4 or 2 groups). The records are put
 // back together field by field (little-endian byte order of the device).
 static_assert(sizeof(LineF32) == 32 && sizeof(LineJac) == 32, "line records are two 16-byte planes");
+static_assert(offsetof(LineF32, nuc) == 0 && offsetof(LineF32, j0) == 8 && offsetof(LineF32, b) == 12 &&
+                  offsetof(LineF32, a) == 16 && offsetof(LineF32, y) == 20 && offsetof(LineF32, amp) == 24 &&
+                  offsetof(LineF32, amp_far) == 28,
+              "LineF32 field offsets assumed by line_f32_from_planes");
+static_assert(offsetof(LineJac, jT_u) == 0 && offsetof(LineJac, jv_u) == 12 && offsetof(LineJac, jv_y) == 16 &&
+                  offsetof(LineJac, pad1) == 28,
+              "LineJac field offsets assumed by line_jac_from_planes");
 __device__ __forceinline__ LineF32 line_f32_from_planes(const float4& p0, const float4& p1) {
   LineF32 L;
   L.nuc = __hiloint2double(__float_as_int(p0.y), __float_as_int(p0.x));   // bytes 0-7
